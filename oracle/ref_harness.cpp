@@ -1,0 +1,281 @@
+// Oracle harness around the reference solver's own code (TEST INFRASTRUCTURE
+// ONLY -- never part of the product path).
+//
+// Built by oracle/Makefile from the reference sources where they lie, twice:
+//   ref_f32  : the sources as shipped (FP32, Eigen::MatrixXf),
+//   ref_f64  : a float->double mechanical promotion of a scratch copy.
+// Outputs go to oracle/_ref/ only.
+//
+// The harness constructs the reference's `SIMPLE` object (SIMPLE.cpp:18-29; it
+// reads ExportFiles/fluid_params.txt and geometry_fluid.txt from the working
+// directory, which this harness writes first), sets the public configuration
+// members the way SIMPLE.h documents them (SIMPLE.h:68-358), overwrites the
+// geometry fields, and then drives the reference's own
+// `SIMPLE::calculateStep` (iterations.cpp:82-526) in the loop that
+// `runIterations` would run (SIMPLE.cpp:299-318) minus file I/O and printing.
+//
+// Jacobi sweep counts: calculateStep discards the count returned by
+// solveU/VMomentumImplicit (iterations.cpp:125).  momentum_solver.cpp is
+// compiled with -DsolveMomentumJacobi=harness_solveMomentumJacobi so that its
+// call (momentum_solver.cpp:313) lands in the wrapper below, which calls the
+// reference's unmodified solvers::cpu::solveMomentumJacobi
+// (jacobi_solver.cpp:20-75) and records what it returns.
+//
+// I/O: a record file (see oracle/casefile.py): each record is a 16-byte
+// NUL-padded name, a 1-byte type ('d' = float64, 'i' = int32), a little-endian
+// int64 count, then the payload.  Grids are row-major (i-major) float64.
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "SIMPLE.h"
+#include "Utilities/solvers/cpu/jacobi_solver.h"
+
+typedef decltype(SIMPLE::hx) real;                 // float as shipped, double when promoted
+typedef decltype(SIMPLE::u) Matrix;                // Eigen::MatrixXf / MatrixXd
+
+static std::vector<int> g_sweep_counts;
+
+namespace solvers {
+namespace cpu {
+int harness_solveMomentumJacobi(int n, const std::vector<int>& row_ptr, const std::vector<int>& col_idx,
+                                const std::vector<real>& values, const std::vector<real>& b,
+                                std::vector<real>& x, const std::vector<int>& diagOffset, real tol,
+                                int maxIter) {
+  int it = solveMomentumJacobi(n, row_ptr, col_idx, values, b, x, diagOffset, tol, maxIter);
+  g_sweep_counts.push_back(it);
+  return it;
+}
+}  // namespace cpu
+}  // namespace solvers
+
+namespace {
+
+struct Record {
+  char type;
+  std::vector<double> d;
+  std::vector<int32_t> i;
+};
+
+std::map<std::string, Record> read_records(const char* path) {
+  std::map<std::string, Record> recs;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) throw std::runtime_error(std::string("cannot open ") + path);
+  for (;;) {
+    char name[17] = {0};
+    if (std::fread(name, 1, 16, f) != 16) break;
+    Record r;
+    int64_t count = 0;
+    if (std::fread(&r.type, 1, 1, f) != 1 || std::fread(&count, 8, 1, f) != 1) throw std::runtime_error("truncated");
+    if (r.type == 'd') {
+      r.d.resize(count);
+      if (count && std::fread(r.d.data(), 8, count, f) != (size_t)count) throw std::runtime_error("truncated");
+    } else if (r.type == 'i') {
+      r.i.resize(count);
+      if (count && std::fread(r.i.data(), 4, count, f) != (size_t)count) throw std::runtime_error("truncated");
+    } else {
+      throw std::runtime_error("bad record type");
+    }
+    recs[name] = std::move(r);
+  }
+  std::fclose(f);
+  return recs;
+}
+
+struct Writer {
+  FILE* f;
+  explicit Writer(const char* path) : f(std::fopen(path, "wb")) {
+    if (!f) throw std::runtime_error(std::string("cannot write ") + path);
+  }
+  ~Writer() { std::fclose(f); }
+  void head(const char* name, char type, int64_t count) {
+    char buf[16] = {0};
+    std::strncpy(buf, name, 16);
+    std::fwrite(buf, 1, 16, f);
+    std::fwrite(&type, 1, 1, f);
+    std::fwrite(&count, 8, 1, f);
+  }
+  void d(const char* name, const std::vector<double>& v) { head(name, 'd', v.size()); std::fwrite(v.data(), 8, v.size(), f); }
+  void i(const char* name, const std::vector<int32_t>& v) { head(name, 'i', v.size()); std::fwrite(v.data(), 4, v.size(), f); }
+  void matrix(const char* name, const Matrix& m) {
+    std::vector<double> v(static_cast<size_t>(m.rows() * m.cols()));
+    for (long r = 0; r < m.rows(); ++r)
+      for (long c = 0; c < m.cols(); ++c) v[r * m.cols() + c] = static_cast<double>(m(r, c));
+    d(name, v);
+  }
+};
+
+double getd(std::map<std::string, Record>& recs, const char* key) {
+  auto it = recs.find(key);
+  if (it == recs.end() || it->second.d.empty()) throw std::runtime_error(std::string("missing ") + key);
+  return it->second.d[0];
+}
+int geti(std::map<std::string, Record>& recs, const char* key) {
+  auto it = recs.find(key);
+  if (it == recs.end() || it->second.i.empty()) throw std::runtime_error(std::string("missing ") + key);
+  return it->second.i[0];
+}
+
+void load_grid(std::map<std::string, Record>& recs, const char* key, Matrix& m) {
+  auto it = recs.find(key);
+  if (it == recs.end()) throw std::runtime_error(std::string("missing ") + key);
+  const std::vector<double>& v = it->second.d;
+  if ((long)v.size() != m.rows() * m.cols()) throw std::runtime_error(std::string("bad size for ") + key);
+  for (long r = 0; r < m.rows(); ++r)
+    for (long c = 0; c < m.cols(); ++c) m(r, c) = static_cast<real>(v[r * m.cols() + c]);
+}
+
+// Mass imbalance restricted to the pressure unknowns (i=1..M-1, j=1..N-2),
+// evaluated with the reference's own expression (pressure_solver.cpp:476-480).
+real mass_residual_dof(const SIMPLE& s) {
+  real out = 0;
+  for (int i = 1; i < s.M; ++i)
+    for (int j = 1; j < s.N - 1; ++j) {
+      real massE = s.rho * s.uStar(i, j) * s.hy;
+      real massW = s.rho * s.uStar(i, j - 1) * s.hy;
+      real massN = s.rho * s.vStar(i, j) * s.hx;
+      real massS = s.rho * s.vStar(i - 1, j) * s.hx;
+      real b = std::abs(massW - massE + massS - massN);
+      if (b > out) out = b;
+    }
+  return out;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  if (argc != 3) {
+    std::fprintf(stderr, "usage: %s case.bin out.bin   (run inside a scratch directory)\n", argv[0]);
+    return 2;
+  }
+  try {
+    auto recs = read_records(argv[1]);
+    const int M = geti(recs, "M"), N = geti(recs, "N");
+    const int mode = geti(recs, "mode");  // 0 = iterate, 1 = build alpha from gamma only
+    // The constructor reads these two files from ./ExportFiles (SIMPLE.cpp:19-21).
+    mkdir("ExportFiles", 0755);
+    {
+      FILE* f = std::fopen("ExportFiles/fluid_params.txt", "w");
+      std::fprintf(f, "%d %d %.17g %.17g %.17g 0 0 %.17g\n", M, N, getd(recs, "hy"), getd(recs, "hx"),
+                   getd(recs, "U_in"), getd(recs, "Ht"));
+      std::fclose(f);
+      f = std::fopen("ExportFiles/geometry_fluid.txt", "w");
+      for (int i = 0; i < M; ++i) {
+        for (int j = 0; j < N; ++j) std::fputs(j ? " 0" : "0", f);
+        std::fputc('\n', f);
+      }
+      std::fclose(f);
+    }
+    SIMPLE s;
+    omp_set_num_threads(geti(recs, "threads"));  // SIMPLE.cpp:89 forces numThreads=8
+
+    s.hx = static_cast<real>(getd(recs, "hx"));
+    s.hy = static_cast<real>(getd(recs, "hy"));
+    s.rho = static_cast<real>(getd(recs, "rho"));
+    s.eta = static_cast<real>(getd(recs, "eta"));
+    s.brinkmanKMin = static_cast<real>(getd(recs, "kmin"));
+    s.brinkmanQ = static_cast<real>(getd(recs, "q"));
+    s.brinkmanAlphaMax = s.eta / std::max(s.brinkmanKMin, static_cast<real>(1e-20));  // SIMPLE.cpp:65-66
+
+    Writer w(argv[2]);
+    if (mode == 1) {
+      load_grid(recs, "gamma", s.gamma);
+      s.buildAlphaFromDensity();  // SIMPLE.cpp:589-630
+      w.matrix("alpha", s.alpha);
+      w.matrix("gamma", s.gamma);
+      return 0;
+    }
+
+    s.targetVel = static_cast<real>(getd(recs, "U_in"));
+    s.inletVelocity = s.targetVel;
+    s.convectionScheme = geti(recs, "conv");
+    s.enableTwoPointFiveD = geti(recs, "twoFiveD") != 0;
+    s.enableConvectionScaling = geti(recs, "convScale") != 0;
+    s.Ht_channel = static_cast<real>(getd(recs, "Ht"));
+    s.twoPointFiveDSinkMultiplier = static_cast<real>(getd(recs, "sinkMult"));
+    s.uvAlpha = static_cast<real>(getd(recs, "uvAlpha"));
+    s.pAlpha = static_cast<real>(getd(recs, "pAlpha"));
+    s.pTol = static_cast<real>(getd(recs, "pTol"));
+    s.maxPressureIter = geti(recs, "maxPIter");
+    s.momentumTol = static_cast<real>(getd(recs, "momTol"));
+    s.maxMomentumIter = geti(recs, "maxMomIter");
+    s.pressureSolverType = 1;           // Parallel CG (pressure_solver.cpp:759)
+    s.momentumSolverType = 1;           // implicit Jacobi (iterations.cpp:109)
+    s.enablePseudoTimeStepping = false; // SIMPLE.h:262 default
+    s.usePressureDropConvergence = false;
+    s.saveStateInterval = 0;
+
+    load_grid(recs, "alpha", s.alpha);
+    load_grid(recs, "gamma", s.gamma);
+    if (recs.count("u0")) {
+      load_grid(recs, "u0", s.u);
+      load_grid(recs, "v0", s.v);
+      load_grid(recs, "p0", s.p);
+    }
+
+    const int maxOuter = geti(recs, "maxOuter");
+    const int stopOnConv = geti(recs, "stopOnConv");
+    const double eps = getd(recs, "eps");
+    std::vector<double> hU, hV, hMass, hMassDof, hErr;
+    std::vector<int32_t> hP, hJu, hJv;
+    double elapsed = 0.0;
+    for (int it = 0; it < maxOuter; ++it) {
+      s.inletVelocity = s.targetVel;  // SIMPLE.cpp:303-307 with the inlet ramp off
+      g_sweep_counts.clear();
+      int pIt = 0;
+      auto t0 = std::chrono::steady_clock::now();
+      real err = s.calculateStep(pIt);
+      elapsed += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      real massDof = mass_residual_dof(s);
+      hU.push_back(s.residU);
+      hV.push_back(s.residV);
+      hMass.push_back(s.residMass);
+      hMassDof.push_back(massDof);
+      hErr.push_back(err);
+      hP.push_back(pIt);
+      hJu.push_back(g_sweep_counts.size() > 0 ? g_sweep_counts[0] : -1);
+      hJv.push_back(g_sweep_counts.size() > 1 ? g_sweep_counts[1] : -1);
+      double conv = std::max({(double)s.residU, (double)s.residV, (double)massDof});
+      if (stopOnConv && conv <= eps) break;
+    }
+    w.d("residU", hU);
+    w.d("residV", hV);
+    w.d("residMass", hMass);
+    w.d("residMassDof", hMassDof);
+    w.d("err", hErr);
+    w.i("pIters", hP);
+    w.i("uSweeps", hJu);
+    w.i("vSweeps", hJv);
+    w.d("elapsed", {elapsed});
+    w.matrix("u", s.u);
+    w.matrix("v", s.v);
+    w.matrix("p", s.p);
+    w.matrix("pStar", s.pStar);
+    w.matrix("uStar", s.uStar);
+    w.matrix("vStar", s.vStar);
+    w.matrix("dE", s.dE);
+    w.matrix("dN", s.dN);
+    // Plane sampling with the reference's samplePlaneAtX (postprocessing.cpp:97-230):
+    // full inlet/outlet (SIMPLE.cpp:256-257) and the two core planes.
+    const double xs[4] = {0.0, static_cast<double>(N * s.hx), getd(recs, "xCoreIn"), getd(recs, "xCoreOut")};
+    std::vector<double> planes;
+    for (double x : xs) {
+      PlaneMetrics m = samplePlaneAtX(s, static_cast<real>(x));
+      planes.insert(planes.end(), {m.flowArea, m.massFlux, m.avgStatic, m.avgDynamic, m.avgTotal, m.valid ? 1.0 : 0.0});
+    }
+    w.d("planes", planes);
+  } catch (const std::exception& e) {
+    std::fprintf(stderr, "ref_harness: %s\n", e.what());
+    return 1;
+  }
+  return 0;
+}

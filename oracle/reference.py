@@ -1,0 +1,89 @@
+"""Runner for the reference solver's own code, compiled from its sources by
+oracle/Makefile into oracle/_ref/ref_f32 and oracle/_ref/ref_f64 (TEST
+INFRASTRUCTURE ONLY).
+
+Each call runs the harness in a scratch directory (the reference's
+constructor reads ExportFiles/ from the working directory) and returns its
+records: the per-iteration residual history, the inner iteration counts, the
+final fields (row-major, reference index space) and four sampled planes.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import tempfile
+from typing import Dict, Optional
+
+import numpy as np
+
+from . import casefile
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(_HERE, "_ref")
+
+
+def binary(precision: str) -> str:
+    return os.path.join(REF_DIR, "ref_f64" if precision == "f64" else "ref_f32")
+
+
+def available(precision: str = "f64") -> bool:
+    return os.access(binary(precision), os.X_OK)
+
+
+def case_records(design, max_outer: int, eps: float = 1e-6, stop_on_conv: bool = False, threads: int = 1,
+                 init: Optional[Dict[str, np.ndarray]] = None, mode: int = 0, x_core=(0.01, 0.05)) -> dict:
+    rec = {
+        "M": [design.M], "N": [design.N], "mode": [mode], "threads": [threads],
+        "hx": [design.hx], "hy": [design.hy], "U_in": [design.inletVelocity], "Ht": [design.Ht_channel],
+        "rho": [design.rho], "eta": [design.eta], "kmin": [1e-14], "q": [1.0], "conv": [design.convectionScheme], "twoFiveD": [int(design.enableTwoPointFiveD)],
+        "convScale": [int(design.enableConvectionScaling)], "sinkMult": [design.twoPointFiveDSinkMultiplier],
+        "uvAlpha": [design.uvAlpha], "pAlpha": [design.pAlpha], "pTol": [design.pTol],
+        "maxPIter": [design.maxPressureIter], "momTol": [design.momentumTol],
+        "maxMomIter": [design.maxMomentumIter], "maxOuter": [max_outer], "stopOnConv": [int(stop_on_conv)],
+        "eps": [eps], "xCoreIn": [x_core[0]], "xCoreOut": [x_core[1]],
+        "alpha": design.alpha, "gamma": design.gamma,
+    }
+    if init is not None:
+        rec["u0"], rec["v0"], rec["p0"] = init["u"], init["v"], init["p"]
+    return rec
+
+
+def run(design, max_outer: int, precision: str = "f64", eps: float = 1e-6, stop_on_conv: bool = False,
+        threads: int = 1, init: Optional[Dict[str, np.ndarray]] = None, timeout: float = 3600) -> Dict[str, np.ndarray]:
+    """Run the reference's calculateStep loop on ``design``; fields come back
+    reshaped to the reference's shapes."""
+    if not available(precision):
+        raise FileNotFoundError(f"{binary(precision)} not built (make -C oracle ref)")
+    with tempfile.TemporaryDirectory(prefix="cps_ref_") as tmp:
+        cpath, opath = os.path.join(tmp, "case.bin"), os.path.join(tmp, "out.bin")
+        casefile.write_records(cpath, case_records(design, max_outer, eps, stop_on_conv, threads, init))
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        proc = subprocess.run([binary(precision), cpath, opath], cwd=tmp, env=env, stdout=subprocess.DEVNULL,
+                              stderr=subprocess.PIPE, timeout=timeout)
+        if proc.returncode != 0:
+            raise RuntimeError(f"reference harness failed: {proc.stderr.decode()[-2000:]}")
+        out = casefile.read_records(opath)
+    M, N = design.M, design.N
+    shapes = {"u": (M + 1, N), "v": (M, N + 1), "p": (M + 1, N + 1), "pStar": (M + 1, N + 1),
+              "uStar": (M + 1, N), "vStar": (M, N + 1), "dE": (M + 1, N), "dN": (M, N + 1)}
+    for k, s in shapes.items():
+        out[k] = out[k].reshape(s)
+    out["planes"] = out["planes"].reshape(4, 6)
+    return out
+
+
+def build_alpha(gamma: np.ndarray, kmin: float = 1e-14, q: float = 1.0, precision: str = "f64", eta: float = 0.00089):
+    """The reference's own buildAlphaFromDensity (SIMPLE.cpp:589-630) on
+    ``gamma`` with alpha_max = eta / kmin (SIMPLE.cpp:65-66); returns (alpha, gamma)."""
+    M, N = gamma.shape
+    with tempfile.TemporaryDirectory(prefix="cps_ref_") as tmp:
+        cpath, opath = os.path.join(tmp, "case.bin"), os.path.join(tmp, "out.bin")
+        casefile.write_records(cpath, {"M": [M], "N": [N], "mode": [1], "threads": [1], "hx": [1e-5], "hy": [1e-5],
+                                       "U_in": [0.1], "Ht": [0.0], "rho": [997.0], "eta": [eta],
+                                       "kmin": [kmin], "q": [q], "gamma": gamma})
+        proc = subprocess.run([binary(precision), cpath, opath], cwd=tmp, stdout=subprocess.DEVNULL,
+                              stderr=subprocess.PIPE, timeout=600)
+        if proc.returncode != 0:
+            raise RuntimeError(proc.stderr.decode()[-2000:])
+        out = casefile.read_records(opath)
+    return out["alpha"].reshape(M, N), out["gamma"].reshape(M, N)

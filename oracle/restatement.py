@@ -1,0 +1,125 @@
+"""ctypes binding of the oracle's C restatement, oracle/liboracle.so (TEST
+INFRASTRUCTURE ONLY).
+
+``precision="f64"`` is the reference promoted to double (the parity judge),
+``"f32"`` the reference as shipped.  Fields are row-major numpy arrays in the
+reference's index space: u/uStar/dE (M+1, N), v/vStar/dN (M, N+1), p/pStar
+(M+1, N+1).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from typing import Dict, Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+FIELD_NAMES = ("u", "v", "p", "pStar", "uStar", "vStar", "dE", "dN")
+DIAG_NAMES = ("residU", "residV", "residMass", "residMassDof", "err", "pIters", "uSweeps", "vSweeps")
+
+
+def build() -> str:
+    """Compile liboracle.so with the recipe in oracle/Makefile."""
+    subprocess.run(["make", "-s", "-C", _HERE, "restatement"], check=True)
+    return _LIB_PATH
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(_LIB_PATH)
+    return _lib
+
+
+def field_shapes(M: int, N: int) -> Dict[str, tuple]:
+    return {"u": (M + 1, N), "v": (M, N + 1), "p": (M + 1, N + 1), "pStar": (M + 1, N + 1),
+            "uStar": (M + 1, N), "vStar": (M, N + 1), "dE": (M + 1, N), "dN": (M, N + 1)}
+
+
+def new_fields(design, precision: str = "f64") -> Dict[str, np.ndarray]:
+    """All fields zero, as SIMPLE::initializeMemory leaves them (SIMPLE.cpp:184-197)."""
+    dt = np.float64 if precision == "f64" else np.float32
+    return {k: np.zeros(s, dtype=dt) for k, s in field_shapes(design.M, design.N).items()}
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _check(fields: Dict[str, np.ndarray], design, dt) -> None:
+    for k, s in field_shapes(design.M, design.N).items():
+        a = fields[k]
+        if a.shape != s or a.dtype != dt or not a.flags.c_contiguous:
+            raise ValueError(f"field {k}: expected {s} {dt} C-contiguous, got {a.shape} {a.dtype}")
+
+
+def step(design, fields: Dict[str, np.ndarray], precision: str = "f64", stop_after: int = 3) -> Dict[str, float]:
+    """One outer iteration in place (iterations.cpp:82-526)."""
+    dt = np.float64 if precision == "f64" else np.float32
+    _check(fields, design, dt)
+    alpha = np.ascontiguousarray(design.alpha, dtype=dt)
+    gamma = np.ascontiguousarray(design.gamma, dtype=dt)
+    diag = np.zeros(8, dtype=np.float64)
+    fn = lib().orc64_step if precision == "f64" else lib().orc32_step
+    rc = fn(_ptr(design.int_params()), _ptr(design.real_params()), ctypes.c_int(stop_after),
+            *[_ptr(fields[k]) for k in FIELD_NAMES], _ptr(alpha), _ptr(gamma), _ptr(diag))
+    if rc != 0:
+        raise RuntimeError(f"oracle step failed ({rc})")
+    return dict(zip(DIAG_NAMES, diag.tolist()))
+
+
+def solve(design, fields: Dict[str, np.ndarray], max_outer: int, eps: float = 1e-6, stop_on_conv: bool = True,
+          precision: str = "f64") -> np.ndarray:
+    """Outer iterations until max(residU, residV, residMassDof) <= eps (or
+    ``max_outer``); returns the (steps, 8) diagnostic history."""
+    dt = np.float64 if precision == "f64" else np.float32
+    _check(fields, design, dt)
+    alpha = np.ascontiguousarray(design.alpha, dtype=dt)
+    gamma = np.ascontiguousarray(design.gamma, dtype=dt)
+    hist = np.zeros((max_outer, 8), dtype=np.float64)
+    fn = lib().orc64_solve if precision == "f64" else lib().orc32_solve
+    n = fn(_ptr(design.int_params()), _ptr(design.real_params()), ctypes.c_int(max_outer), ctypes.c_double(eps),
+           ctypes.c_int(int(stop_on_conv)), *[_ptr(fields[k]) for k in FIELD_NAMES], _ptr(alpha), _ptr(gamma),
+           _ptr(hist))
+    if n < 0:
+        raise RuntimeError("oracle solve failed")
+    return hist[:n]
+
+
+def sample_plane(design, fields: Dict[str, np.ndarray], x: float, precision: str = "f64") -> np.ndarray:
+    """postprocessing.cpp:97-230; returns flowArea, massFlux, avgStatic,
+    avgDynamic, avgTotal, valid."""
+    dt = np.float64 if precision == "f64" else np.float32
+    out = np.zeros(6, dtype=np.float64)
+    gamma = np.ascontiguousarray(design.gamma, dtype=dt)
+    fn = lib().orc64_sample_plane if precision == "f64" else lib().orc32_sample_plane
+    fn(ctypes.c_int(design.M), ctypes.c_int(design.N), ctypes.c_double(design.hx), ctypes.c_double(design.hy),
+       ctypes.c_double(design.rho), ctypes.c_double(x), _ptr(np.ascontiguousarray(fields["u"], dtype=dt)),
+       _ptr(np.ascontiguousarray(fields["v"], dtype=dt)), _ptr(np.ascontiguousarray(fields["p"], dtype=dt)),
+       _ptr(gamma), _ptr(out))
+    return out
+
+
+def full_dp(design, fields: Dict[str, np.ndarray], precision: str = "f64") -> float:
+    """Full inlet-outlet total-pressure drop (SIMPLE.cpp:256-257, 349)."""
+    a = sample_plane(design, fields, 0.0, precision)
+    b = sample_plane(design, fields, design.N * design.hx, precision)
+    return float(a[4] - b[4])
+
+
+def build_alpha(gamma: np.ndarray, alpha_max: float, q: float, precision: str = "f64"):
+    """SIMPLE.cpp:589-630; returns (alpha, gamma_after_wall_forcing)."""
+    dt = np.float64 if precision == "f64" else np.float32
+    g = np.array(gamma, dtype=dt, copy=True, order="C")
+    a = np.zeros_like(g)
+    fn = lib().orc64_build_alpha if precision == "f64" else lib().orc32_build_alpha
+    fn(ctypes.c_int(g.shape[0]), ctypes.c_int(g.shape[1]), ctypes.c_double(alpha_max), ctypes.c_double(q),
+       _ptr(g), _ptr(a))
+    return a, g
