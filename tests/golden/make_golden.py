@@ -1,0 +1,65 @@
+"""Generate the golden fixtures in this directory from the reference solver's
+own code (oracle/_ref/ref_f64 = the reference promoted to double, ref_f32 =
+as shipped), run with one OpenMP thread so every reduction is sequential.
+
+Run from the repository root where the reference sources are available:
+    make -C oracle ref && python tests/golden/make_golden.py
+The fixtures are committed; tests read them without the reference present.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from coldplate_solver_b200 import geometry as g  # noqa: E402
+from oracle import reference  # noqa: E402
+
+DESIGN_KEYS = ("M", "N", "hx", "hy", "inletVelocity", "convectionScheme", "enableTwoPointFiveD",
+               "enableConvectionScaling", "Ht_channel", "twoPointFiveDSinkMultiplier", "uvAlpha", "pAlpha", "rho",
+               "eta", "pTol", "maxPressureIter", "momentumTol", "maxMomentumIter")
+
+
+def cases():
+    yield "straight_11x13", g.straight_channel(M=11, N=13, band=(3, 8)), 40, None
+    yield "network_30x48_sou25d", g.channel_network(M=30, N=48, h=20e-6, wmin=3, wmax=6, seed=3), 25, None
+    yield "density_13x27_sou", g.density_field(Nx=27, seed=9, sigma=2.0, plenum=3, twoFiveD=False), 25, None
+    d = g.density_field(Nx=40, seed=5, sigma=3.0, plenum=4)
+    rng = np.random.default_rng(11)
+    init = {"u": rng.normal(0, 0.05, (d.M + 1, d.N)), "v": rng.normal(0, 0.02, (d.M, d.N + 1)),
+            "p": rng.normal(0, 10.0, (d.M + 1, d.N + 1))}
+    yield "density_20x40_random_state", d, 3, init
+    yield "minimal_3x3", g.straight_channel(M=3, N=3, band=(1, 2)), 5, None
+    d = g.straight_channel(M=9, N=17, band=(2, 7)).replace(maxMomentumIter=3, maxPressureIter=2, pTol=1e-12,
+                                                            momentumTol=1e-12)
+    yield "capped_9x17", d, 6, None
+
+
+def main() -> None:
+    for name, d, n, init in cases():
+        rec = {k: np.asarray(getattr(d, k)) for k in DESIGN_KEYS}
+        rec.update(gamma=d.gamma, alpha=d.alpha, n_outer=np.asarray(n))
+        if init is not None:
+            rec.update(u0=init["u"], v0=init["v"], p0=init["p"])
+        for prec in ("f64", "f32"):
+            out = reference.run(d, n, precision=prec, threads=1, init=init)
+            for k in ("residU", "residV", "residMass", "residMassDof", "err", "pIters", "uSweeps", "vSweeps",
+                      "u", "v", "p", "pStar", "uStar", "vStar", "dE", "dN", "planes"):
+                rec[f"{prec}_{k}"] = out[k]
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **rec)
+        print("wrote", name)
+    gm = np.random.default_rng(0).random((17, 23))
+    rec = {"gamma_in": gm}
+    for prec in ("f64", "f32"):
+        a, gg = reference.build_alpha(gm, 1e-14, 1.0, precision=prec)
+        rec[f"{prec}_alpha"], rec[f"{prec}_gamma"] = a, gg
+    np.savez_compressed(os.path.join(HERE, "alpha_ramp_17x23.npz"), **rec)
+    print("wrote alpha_ramp_17x23")
+
+
+if __name__ == "__main__":
+    main()

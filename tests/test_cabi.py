@@ -1,0 +1,75 @@
+"""libcps.so loads, exports every entry point include/cps.h declares, and its
+structs have the layout the ctypes binding assumes.  No GPU calls."""
+import ctypes
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from conftest import REPO
+from coldplate_solver_b200 import cps
+
+HEADERS = [os.path.join(REPO, "include", f) for f in os.listdir(os.path.join(REPO, "include")) if f.endswith(".h")]
+
+
+def declared_functions():
+    names = []
+    for h in HEADERS:
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names += re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(cps_\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = cps.load_library()
+    names = declared_functions()
+    assert len(names) >= 10
+    for n in names:
+        assert hasattr(lib, n), n
+        assert n in cps.SIGNATURES, f"{n} has no ctypes signature"
+    out = subprocess.run(["nm", "-D", "--defined-only", cps.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (cps_\w+)", out))
+    assert set(names) <= exported
+
+
+def test_struct_layout_matches_c():
+    src = r'''
+#include <stdio.h>
+#include <stddef.h>
+#include "cps.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(cps_desc), offsetof(cps_desc, precision), offsetof(cps_desc, alpha),
+         offsetof(cps_desc, grid_ctas), sizeof(cps_step_out), offsetof(cps_step_out, vSweeps), sizeof(cps_plane));
+  return 0;
+}'''
+    with tempfile.TemporaryDirectory() as t:
+        c, exe = os.path.join(t, "l.c"), os.path.join(t, "l")
+        open(c, "w").write(src)
+        subprocess.run(["/usr/bin/gcc", "-I", os.path.join(REPO, "include"), c, "-o", exe], check=True)
+        vals = list(map(int, subprocess.run([exe], capture_output=True, text=True).stdout.split()))
+    py = [ctypes.sizeof(cps.CpsDesc), cps.CpsDesc.precision.offset, cps.CpsDesc.alpha.offset,
+          cps.CpsDesc.grid_ctas.offset, ctypes.sizeof(cps.CpsStepOut), cps.CpsStepOut.vSweeps.offset,
+          ctypes.sizeof(cps.CpsPlane)]
+    assert vals == py
+
+
+def test_argument_validation_without_gpu():
+    lib = cps.load_library()
+    from coldplate_solver_b200 import geometry
+    d = geometry.straight_channel(M=10, N=12, band=(3, 7))
+    desc, keep = cps.make_desc(d)
+    out = ctypes.c_ulonglong()
+    assert lib.cps_footprint(ctypes.byref(desc), ctypes.byref(out)) == cps.CPS_OK
+    assert out.value > 33 * 11 * 32 * 8
+    bad, keep2 = cps.make_desc(d)
+    bad.M = 2
+    assert lib.cps_footprint(ctypes.byref(bad), ctypes.byref(out)) == cps.CPS_ERR_ARG
+    assert b"too small" in lib.cps_last_error(None)
+    bad.M, bad.hx = 10, -1.0
+    assert lib.cps_footprint(ctypes.byref(bad), ctypes.byref(out)) == cps.CPS_ERR_ARG
+    assert lib.cps_create(None, None) == cps.CPS_ERR_ARG
+    assert lib.cps_step(None, None, None) == cps.CPS_ERR_ARG
+    assert lib.cps_version().startswith(b"cps")
