@@ -1,0 +1,393 @@
+#!/usr/bin/env python
+"""Benchmark: converged SIMPLE solves per second on one B200 (and N GPUs).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload network|straight|density|mix] [--precision fp64|mixed]
+
+A step is one converged solve (outer residual max(residU, residV,
+residMassDof) <= 1e-6) of the workload's design(s), started from the zero
+state.  ``value`` is converged solves/s over all ranks with the inputs
+resident in HBM (device time from CUDA events on the library's stream, L2
+flushed between steps); ``e2e`` is the same metric through the public C ABI
+with host buffers: geometry and initial fields uploaded, the solve run, and
+u, v, p downloaded, every step (wall clock).
+
+Multi-GPU (torchrun, one rank per GPU): every rank solves its own copy of the
+workload (independent designs, no collective on the data path; weak scaling);
+the timed region is bracketed by barriers and the max over ranks is taken.
+
+--impl reference times the reference solver's own CPU implementation
+(oracle/_ref/ref_f64: its sources promoted to FP64, all host threads) on the
+same workload: each step runs a bounded sample of outer iterations and the
+solves/s figure is extrapolated with the iteration count of a converged solve.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "converged solves/s (1e-6 outer residual)"
+EPS = 1e-6
+MAX_OUTER = 200000
+L2_FLUSH_BYTES = 512 << 20  # > 126 MB L2
+
+
+def workload(name: str):
+    from coldplate_solver_b200 import geometry as g
+    if name == "network":
+        d = g.channel_network()
+        cfg = {"workload": "channel_network_500x250_sou_2.5d", "grid": "500x250", "dx_um": 20,
+               "convection": "SOU", "two_point_five_d": True}
+    elif name == "straight":
+        d = g.straight_channel()
+        cfg = {"workload": "straight_channel_200x100_fou", "grid": "200x100", "dx_um": 50, "convection": "FOU"}
+    elif name == "density":
+        d = g.density_field(Nx=1000)
+        cfg = {"workload": "density_field_1000x500_sou_2.5d", "grid": "1000x500", "dx_um": 10, "convection": "SOU"}
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    cfg.update(uvAlpha=d.uvAlpha, pAlpha=d.pAlpha, eps=EPS)
+    return d, cfg
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes (per outer iteration, FP64: 8-byte elements)
+# ---------------------------------------------------------------------------
+def algorithmic_bytes(design, hist: np.ndarray, s: int = 8) -> float:
+    """Minimal single-pass DRAM streams of one outer iteration:
+    momentum set-up 6(nU+nV), Jacobi 6(Ku nU + Kv nV), mass residual 3 nP,
+    PCG 12 Kp nP, correction 9 M N elements (s bytes each)."""
+    nU, nV, nP, MN = design.nU, design.nV, design.nP, design.M * design.N
+    ku, kv = hist[:, 6], hist[:, 7]
+    kp = np.where(hist[:, 5] < design.maxPressureIter, hist[:, 5] + 1, design.maxPressureIter)
+    per = 6 * (nU + nV) + 6 * (ku * nU + kv * nV) + 3 * nP + 12 * kp * nP + 9 * MN
+    return float(s * per.sum())
+
+
+# ---------------------------------------------------------------------------
+# clocks sampling
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except OSError:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        loaded = [x for x in sm if mx and x > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_init(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return rank, local, world
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int, local: int) -> float:
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own code (oracle/_ref/ref_f64), all host cores
+# ---------------------------------------------------------------------------
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline(design, iters_per_solve: int, starts, sample_iters: int, threads: int) -> dict:
+    """Time the reference's calculateStep loop on ``sample_iters`` outer
+    iterations from each start state; extrapolate converged solves/s."""
+    from oracle import reference
+    kind = "reference"
+    per_it = []
+    if reference.available("f64"):
+        for st in starts:
+            out = reference.run(design, sample_iters, precision="f64", threads=threads, init=st)
+            per_it.append(float(out["elapsed"][0]) / len(out["err"]))
+    else:  # the oracle restatement (single thread) when the reference binary is absent
+        from oracle import restatement as rs
+        kind, threads = "port", 1
+        for st in starts:
+            f = rs.new_fields(design)
+            if st is not None:
+                for k in ("u", "v", "p"):
+                    f[k][...] = st[k]
+            t = time.perf_counter()
+            rs.solve(design, f, sample_iters, stop_on_conv=False)
+            per_it.append((time.perf_counter() - t) / sample_iters)
+    s_per_it = float(np.mean(per_it))
+    return {"value": 1.0 / (s_per_it * iters_per_solve), "unit": "solves/s", "cores": threads, "kind": kind,
+            "ms_per_outer_iteration": 1e3 * s_per_it,
+            "sample": f"{sample_iters} outer iterations from each of {len(starts)} states along the FP64 trajectory "
+                      f"of this design, extrapolated to a converged solve of {iters_per_solve} outer iterations"}
+
+
+# ---------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------
+def run_b200(args) -> None:
+    rank, local, world = dist_init(args.gpus)
+    import torch
+
+    from coldplate_solver_b200 import cps
+    device = local
+    torch.cuda.set_device(device)
+    design, cfg = workload(args.workload)
+    precision = cps.CPS_MIXED if args.precision == "mixed" else cps.CPS_FP64
+    solver = cps.Solver(design, precision=precision, device=device)
+    stream = torch.cuda.ExternalStream(solver.stream, device=device)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+
+    def one_solve():
+        solver.reset_fields()
+        return solver.solve(MAX_OUTER, eps=EPS)
+
+    hist = None
+    for _ in range(args.warmup):
+        hist = one_solve()
+    iters_per_solve = len(hist)
+    converged = bool(max(hist[-1, 0], hist[-1, 1], hist[-1, 3]) <= EPS)
+
+    # ---- device-resident timing ----
+    barrier(world)
+    torch.cuda.synchronize(device)
+    solver.kernel_timing(reset=True)
+    step_ms, alg_bytes, iters = [], 0.0, []
+    with ClockSampler(device) as clocks:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)  # evict the previous step's working set from L2
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            h = one_solve()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            alg_bytes += algorithmic_bytes(design, h)
+            iters.append(len(h))
+    torch.cuda.synchronize(device)
+    barrier(world)
+    kernel_ms, launches, outer_done = solver.kernel_timing(reset=True)
+    total_s = max_over_ranks(sum(step_ms) / 1e3, world, local)
+    value = world * args.steps / total_s
+
+    # ---- end to end through the C ABI with host buffers ----
+    M, N = design.M, design.N
+    host_in = {k: torch.zeros(s, dtype=torch.float64).pin_memory().numpy()
+               for k, s in (("u", (M + 1, N)), ("v", (M, N + 1)), ("p", (M + 1, N + 1)))}
+    alpha = torch.from_numpy(design.alpha).pin_memory().numpy()
+    gamma = torch.from_numpy(design.gamma).pin_memory().numpy()
+    h2d = (alpha.nbytes + gamma.nbytes + sum(a.nbytes for a in host_in.values()))
+    d2h = sum(a.nbytes for a in host_in.values()) + 8 * 8 * iters_per_solve
+    e2e_steps = max(1, min(args.steps, 5))
+    barrier(world)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        solver.upload_geometry(alpha, gamma)
+        solver.upload_fields(host_in["u"], host_in["v"], host_in["p"])
+        solver.solve(MAX_OUTER, eps=EPS)
+        solver.download()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, local)
+    barrier(world)
+
+    # ---- CPU baseline (rank 0, N = 1 only) ----
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        starts = [None]
+        for frac in (0.25, 0.5, 0.75):
+            solver.reset_fields()
+            solver.solve(max(1, int(frac * iters_per_solve)), eps=0.0)
+            f = solver.download()
+            starts.append({k: f[k] for k in ("u", "v", "p")})
+        cpu = cpu_baseline(design, iters_per_solve, starts, args.cpu_sample_iters, host_cores())
+
+    solver.close()
+    if rank != 0:
+        return
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    kernel_s = kernel_ms / 1e3
+    achieved = alg_bytes / kernel_s / 1e9 if kernel_s > 0 else None
+    lat = sorted(step_ms)
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == cps.CPS_FP64 else "f32+f64",
+        "data": "synthetic (seeded generator)", "impl": "b200",
+        "config": dict(cfg, l2="flushed between steps (512 MiB write)", precision=args.precision,
+                       outer_iterations_per_solve=iters_per_solve, converged=converged,
+                       parallelism=f"replicas x{world}"),
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "cell_updates_per_s": world * design.M * design.N * sum(iters) / total_s,
+        "e2e": {"value": world * e2e_steps / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s",
+                     "kernel": "cps_grid_kernel", "kernel_ms_per_launch": kernel_ms / max(1, launches),
+                     "algorithmic_bytes_per_launch": alg_bytes / max(1, launches)},
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
+def run_reference(args) -> None:
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import reference
+    design, cfg = workload(args.workload)
+    if not reference.available("f64"):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_f64 is not built (make -C oracle ref)"}))
+        return
+    iters_per_solve = REFERENCE_ITERS.get(args.workload)
+    threads = host_cores()
+    for _ in range(args.warmup):
+        reference.run(design, max(1, args.ref_sample_iters // 4), precision="f64", threads=threads)
+    per_it = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        out = reference.run(design, args.ref_sample_iters, precision="f64", threads=threads)
+        per_it.append(float(out["elapsed"][0]) / len(out["err"]))
+    wall = time.perf_counter() - t0
+    s_per_it = float(np.mean(per_it))
+    value = 1.0 / (s_per_it * iters_per_solve)
+    sample = (f"first {args.ref_sample_iters} outer iterations from the zero state per step, extrapolated to a "
+              f"converged solve of {iters_per_solve} outer iterations (count from the FP64 oracle)")
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)", "impl": "reference",
+        "config": dict(cfg, outer_iterations_per_solve=iters_per_solve, ms_per_outer_iteration=1e3 * s_per_it),
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+# Outer iterations of a converged FP64 solve of each workload, measured by the
+# bit-exact FP64 oracle (the reference's own arithmetic).
+REFERENCE_ITERS = {"straight": 5564}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="straight", choices=["straight", "network", "density"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--cpu-sample-iters", type=int, default=200)
+    ap.add_argument("--ref-sample-iters", type=int, default=300)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

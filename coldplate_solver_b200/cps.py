@@ -64,6 +64,16 @@ class CpsPlane(ctypes.Structure):
                 ("avgDynamic", ctypes.c_double), ("avgTotal", ctypes.c_double), ("valid", ctypes.c_int)]
 
 
+class CpsBatchOpts(ctypes.Structure):
+    _fields_ = [("cluster_ctas", ctypes.c_int), ("max_clusters", ctypes.c_int), ("max_outer", ctypes.c_int),
+                ("eps", ctypes.c_double), ("order_by_size", ctypes.c_int)]
+
+
+class CpsBatchResult(ctypes.Structure):
+    _fields_ = [("n_done", ctypes.c_int), ("converged", ctypes.c_int), ("status", ctypes.c_int),
+                ("last", CpsStepOut)]
+
+
 # Every symbol include/cps.h declares, with its ctypes signature.
 _P = ctypes.c_void_p
 _D = ctypes.POINTER(ctypes.c_double)
@@ -77,6 +87,14 @@ SIGNATURES = {
     "cps_sample_plane": (ctypes.c_int, [_P, ctypes.c_double, ctypes.POINTER(CpsPlane)]),
     "cps_download_fields": (ctypes.c_int, [_P, _D, _D, _D, _D, _D, _D, _D, _D, ctypes.c_int]),
     "cps_footprint": (ctypes.c_int, [ctypes.POINTER(CpsDesc), ctypes.POINTER(ctypes.c_ulonglong)]),
+    "cps_upload_geometry": (ctypes.c_int, [_P, _D, _D, ctypes.c_int]),
+    "cps_reset_fields": (ctypes.c_int, [_P]),
+    "cps_get_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
+    "cps_kernel_timing": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
+                                         ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]),
+    "cps_batch_solve": (ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_int, _D, ctypes.POINTER(CpsBatchOpts),
+                                       ctypes.POINTER(CpsBatchResult), _D]),
+    "cps_get_history": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(CpsStepOut)]),
     "cps_last_error": (ctypes.c_char_p, [_P]),
     "cps_version": (ctypes.c_char_p, []),
 }
@@ -191,6 +209,30 @@ class Solver:
                 arrs.append(a)
         self._check(self.lib.cps_upload_fields(self.ctx, *[_dptr(a) for a in arrs], CPS_ROW_MAJOR))
 
+    def upload_geometry(self, alpha: np.ndarray, gamma: np.ndarray) -> None:
+        M, N = self.design.M, self.design.N
+        a = np.ascontiguousarray(alpha, dtype=np.float64)
+        g = np.ascontiguousarray(gamma, dtype=np.float64)
+        if a.shape != (M, N) or g.shape != (M, N):
+            raise ValueError("alpha and gamma must be (M, N)")
+        self._check(self.lib.cps_upload_geometry(self.ctx, _dptr(a), _dptr(g), CPS_ROW_MAJOR))
+
+    def reset_fields(self) -> None:
+        self._check(self.lib.cps_reset_fields(self.ctx))
+
+    @property
+    def stream(self) -> int:
+        s = _P()
+        self._check(self.lib.cps_get_stream(self.ctx, ctypes.byref(s)))
+        return int(s.value or 0)
+
+    def kernel_timing(self, reset: bool = False):
+        """(kernel_ms, launches, outer_iterations) since the last reset."""
+        ms, n, it = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(self.lib.cps_kernel_timing(self.ctx, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(it),
+                                               int(reset)))
+        return ms.value, n.value, it.value
+
     def step(self, inletVelocity: Optional[float] = None) -> Dict[str, float]:
         out = CpsStepOut()
         sin = CpsStepIn(self.inletVelocity if inletVelocity is None else inletVelocity)
@@ -228,3 +270,47 @@ class Solver:
                                                             ("u", "v", "p", "pStar", "uStar", "vStar", "dE", "dN")],
                                                  CPS_ROW_MAJOR))
         return out
+
+
+def history_to_array(hist, n: int) -> np.ndarray:
+    out = np.zeros((n, 8))
+    for k in range(n):
+        h = hist[k]
+        out[k] = (h.residU, h.residV, h.residMass, h.residMassDof, h.err, h.pIters, h.uSweeps, h.vSweeps)
+    return out
+
+
+def batch_solve(solvers, max_outer: int, eps: float = 1e-6, cluster_ctas: int = 8, max_clusters: int = 0,
+                order_by_size: bool = True, inlet_velocities=None):
+    """Run many resident designs in one persistent cluster launch
+    (cps_batch_solve).  Returns (results, kernel_ms); results[k] is a dict with
+    n_done, converged, status and the last step's diagnostics."""
+    if not solvers:
+        return [], 0.0
+    lib = solvers[0].lib
+    n = len(solvers)
+    ctxs = (_P * n)(*[s.ctx for s in solvers])
+    uin = np.ascontiguousarray([s.inletVelocity if inlet_velocities is None else inlet_velocities[k]
+                                for k, s in enumerate(solvers)], dtype=np.float64)
+    opts = CpsBatchOpts(cluster_ctas=cluster_ctas, max_clusters=max_clusters, max_outer=max_outer, eps=eps,
+                        order_by_size=int(order_by_size))
+    res = (CpsBatchResult * n)()
+    ms = ctypes.c_double(0.0)
+    st = lib.cps_batch_solve(ctxs, n, _dptr(uin), ctypes.byref(opts), res, ctypes.byref(ms))
+    if st not in (CPS_OK, CPS_ERR_DIVERGED):
+        raise CpsError(st, lib.cps_last_error(None).decode())
+    out = []
+    for k in range(n):
+        r = res[k]
+        last = r.last
+        out.append({"n_done": r.n_done, "converged": bool(r.converged), "status": r.status,
+                    "last": (last.residU, last.residV, last.residMass, last.residMassDof, last.err, last.pIters,
+                             last.uSweeps, last.vSweeps)})
+    return out, ms.value
+
+
+def get_history(solver: "Solver", n: int) -> np.ndarray:
+    """The first n (<= 4096) diagnostics of the solver's last launch chunk or batch visit."""
+    hist = (CpsStepOut * max(1, n))()
+    solver._check(solver.lib.cps_get_history(solver.ctx, n, hist))
+    return history_to_array(hist, n)

@@ -1,23 +1,31 @@
 // Host side of libcps.so: contexts, device memory, launches and the C ABI
 // declared in include/cps.h.
 //
-// Memory: one cudaMalloc'd slab per context holds every field as a pitched
-// row-major plane of (M+1) rows x P doubles, P = round_up(N+1, 32), plus the
-// grid barrier, the reduction ring and the history buffer.  The fields stay
-// resident between calls; per outer iteration only the 8 diagnostics of each
-// step travel to the host (batched per cps_solve call).
+// Memory: one cudaMalloc'd slab per context.  The ten FP64 field planes (u, v,
+// p, p', u*, v*, dE, dN, alpha, gamma) come first, each (M+1) rows x P
+// doubles, P = round_up(N+1, 32); then the 25 inner-solve planes in the
+// context's storage type (double for CPS_FP64, float for CPS_MIXED); then the
+// grid barrier, flags, reduction ring and history buffer.  The fields stay
+// resident between calls; per outer iteration only the 8 diagnostics travel
+// to the host (batched per call).
 //
-// Launch: the outer iterations run in one persistent kernel launched
-// cooperatively (all CTAs co-resident), synchronised by a software grid
-// barrier whose waits are bounded (2 s) and report CPS_ERR_TIMEOUT instead of
-// hanging.
+// Launch, one design: the outer iterations run in one persistent kernel
+// launched cooperatively (all CTAs co-resident), synchronised by a software
+// grid barrier whose waits are bounded (2 s) and report CPS_ERR_TIMEOUT
+// instead of hanging.
+//
+// Launch, many designs (cps_batch_solve): one thread-block cluster per design
+// at a time; clusters take designs from a device work queue, synchronise with
+// the hardware cluster barrier and reduce through distributed shared memory.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
+#include <numeric>
 #include <string>
 #include <vector>
 
@@ -29,15 +37,11 @@ namespace {
 thread_local std::string g_create_error;
 
 constexpr int kHistChunk = 4096;  // outer iterations per launch inside cps_solve
+constexpr int kFieldPlanes = 10;  // FP64 planes: u v p pc us vs dE dN alpha gamma
+constexpr int kInnerPlanes = 25;  // cU x5, cV x5, bU bV xU0 xU1 xV0 xV1 px pr pz pp0 pp1 pAp pdiag cx cy
+constexpr int kMaxGridCtas = 2048;
 
-// Field planes held by a context, in slab order.
-enum Plane {
-  kU, kV, kP, kPc, kUs, kVs, kDE, kDN, kAlpha, kGamma,
-  kCU0, kCU1, kCU2, kCU3, kCU4, kCV0, kCV1, kCV2, kCV3, kCV4,
-  kBU, kBV, kXU0, kXU1, kXV0, kXV1,
-  kPx, kPr, kPz, kPp0, kPp1, kPAp, kPdiag,
-  kNumPlanes
-};
+enum FieldPlane { kU, kV, kP, kPc, kUs, kVs, kDE, kDN, kAlpha, kGamma };
 
 size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -46,9 +50,8 @@ size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 struct cps_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
-  int M = 0, N = 0, P = 0, R = 0;
+  int M = 0, N = 0, P = 0;
   int precision = CPS_FP64;
-  double momTol = 0.0;
   cps::DesignView view{};
   char* slab = nullptr;
   size_t slab_bytes = 0;
@@ -63,16 +66,20 @@ struct cps_ctx {
   double* hhist = nullptr;   // pinned, kHistChunk * 8
   int* hflags = nullptr;     // pinned: status, n_done
   int grid = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double kernel_ms = 0.0;
+  long long launches = 0, outer_done = 0;
   std::string err;
 };
 
-__global__ void __launch_bounds__(cps::kThreads) cps_grid_kernel(cps::DesignView d, cps::RunControl rc,
+template <typename T>
+__global__ void __launch_bounds__(cps::kThreads, 2) cps_grid_kernel(cps::DesignView d, cps::RunControl rc,
                                                                 cps::GridBarrier* bar, double* red) {
   __shared__ double smem[cps::kRedWidth * 8];
-  cps::GridGroup g{bar, red, rc.status, blockIdx.x, gridDim.x, 0u};
+  cps::GridGroup g{bar, red, rc.status, blockIdx.x, gridDim.x, 0u, 0ull};
   for (int it = 0; it < rc.n_outer; ++it) {
     double out[8];
-    const int r = cps::outer_iteration(d, g, smem, out, it + 1 == rc.n_outer, rc.stop_on_conv != 0, rc.eps);
+    const int r = cps::outer_iteration<T>(d, g, smem, out, it + 1 == rc.n_outer, rc.stop_on_conv != 0, rc.eps);
     if (r < 0) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       for (int k = 0; k < 8; ++k) rc.hist[(size_t)it * 8 + k] = out[k];
@@ -80,6 +87,54 @@ __global__ void __launch_bounds__(cps::kThreads) cps_grid_kernel(cps::DesignView
     }
     if (r == 1) return;
   }
+}
+
+// Batched solves: each cluster takes the next design from the queue and runs
+// its outer iterations to convergence or to the item's budget.
+template <typename T>
+__global__ void __launch_bounds__(cps::kThreads) cps_cluster_kernel(const cps::BatchItem* __restrict__ items,
+                                                                   const int* __restrict__ order, int n_items,
+                                                                   int* queue, cps::BatchResult* results) {
+  __shared__ double smem[cps::kRedWidth * 8];
+  __shared__ double redbuf[2 * cps::kRedWidth];
+  __shared__ __align__(16) cps::BatchItem s_item;
+  __shared__ int s_next;
+  cps::cg::cluster_group cl = cps::cg::this_cluster();
+  cps::ClusterGroup g{redbuf, nullptr, cl.block_rank(), cl.num_blocks(), 0u};
+  for (;;) {
+    if (g.rank == 0 && threadIdx.x == 0) s_next = atomicAdd(queue, 1);
+    cl.sync();
+    const int idx = *cl.map_shared_rank(&s_next, 0);
+    if (idx >= n_items) break;
+    const int id = order[idx];
+    {
+      const int* src = reinterpret_cast<const int*>(items + id);
+      int* dst = reinterpret_cast<int*>(&s_item);
+      for (int k = threadIdx.x; k < (int)(sizeof(cps::BatchItem) / sizeof(int)); k += blockDim.x) dst[k] = src[k];
+    }
+    __syncthreads();
+    const cps::BatchItem& item = s_item;
+    cps::BatchResult* res = results + id;
+    g.status = &res->status;
+    double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int done = 0;
+    for (int it = 0; it < item.n_outer; ++it) {
+      const int r = cps::outer_iteration<T>(item.view, g, smem, out, it + 1 == item.n_outer, item.stop_on_conv != 0,
+                                            item.eps);
+      done = it + 1;
+      if (g.rank == 0 && threadIdx.x == 0 && item.hist && it < item.hist_cap)
+        for (int k = 0; k < 8; ++k) item.hist[(size_t)it * 8 + k] = out[k];
+      if (r != 0) break;
+    }
+    if (g.rank == 0 && threadIdx.x == 0) {
+      res->n_done = done;
+      const double conv = cps::maxd(cps::maxd(out[0], out[1]), out[3]);
+      res->converged = (done > 0 && conv <= item.eps) ? 1 : 0;
+      for (int k = 0; k < 8; ++k) res->last[k] = out[k];
+    }
+    cl.sync();  // s_item, s_next and the reduction ring are reused next round
+  }
+  cl.sync();    // no CTA leaves while another may still read its shared memory
 }
 
 // samplePlaneAtX (postprocessing.cpp:62-230) for one plane, one CTA: every row's
@@ -152,15 +207,18 @@ cps_status fail(cps_ctx* ctx, cps_status s, const std::string& msg) {
   return s;
 }
 
-size_t footprint_bytes(int M, int N, size_t* plane_elems_out, int* P_out) {
+size_t elem_bytes(int precision) { return precision == CPS_MIXED ? sizeof(float) : sizeof(double); }
+
+size_t footprint_bytes(int M, int N, int precision, size_t* plane_elems_out, int* P_out) {
   const int P = (int)round_up((size_t)N + 1, 32);
   const size_t plane = (size_t)(M + 1) * P;
   if (plane_elems_out) *plane_elems_out = plane;
   if (P_out) *P_out = P;
-  size_t bytes = plane * sizeof(double) * kNumPlanes;
-  bytes += 256;                                                // barrier + flags
-  bytes += (size_t)cps::kRedSlots * 2048 * cps::kRedWidth * 8; // reduction ring (<= 2048 CTAs)
-  bytes += (size_t)kHistChunk * 8 * 8 + 64;                    // history + plane metrics
+  size_t bytes = plane * sizeof(double) * kFieldPlanes;
+  bytes += round_up(plane * elem_bytes(precision) * kInnerPlanes, 256);
+  bytes += 256;                                                           // barrier + flags
+  bytes += (size_t)cps::kRedSlots * kMaxGridCtas * cps::kRedWidth * 8;    // reduction ring
+  bytes += (size_t)kHistChunk * 8 * 8 + 64;                               // history + plane metrics
   return round_up(bytes, 256);
 }
 
@@ -175,21 +233,19 @@ cps_status validate(const cps_desc* d) {
   if (d->precision != CPS_FP64 && d->precision != CPS_MIXED) return fail(nullptr, CPS_ERR_ARG, "bad precision");
   if (d->layout != CPS_ROW_MAJOR && d->layout != CPS_COL_MAJOR) return fail(nullptr, CPS_ERR_ARG, "bad layout");
   if (!d->alpha || !d->gamma) return fail(nullptr, CPS_ERR_ARG, "alpha and gamma are required");
+  if (d->grid_ctas < 0) return fail(nullptr, CPS_ERR_ARG, "grid_ctas < 0");
   return CPS_OK;
 }
 
 // Copy a host rows x cols matrix (row- or column-major) into a pitched device plane.
 bool upload_plane(cps_ctx* c, double* dst, const double* src, int rows, int cols, int layout) {
-  const double* rowmajor = src;
   if (layout == CPS_COL_MAJOR) {
     for (int i = 0; i < rows; ++i)
       for (int j = 0; j < cols; ++j) c->hstage[(size_t)i * cols + j] = src[(size_t)j * rows + i];
-    rowmajor = c->hstage;
   } else {
     std::memcpy(c->hstage, src, sizeof(double) * (size_t)rows * cols);
-    rowmajor = c->hstage;
   }
-  if (!cuda_ok(c, cudaMemcpy2DAsync(dst, (size_t)c->P * 8, rowmajor, (size_t)cols * 8, (size_t)cols * 8, rows,
+  if (!cuda_ok(c, cudaMemcpy2DAsync(dst, (size_t)c->P * 8, c->hstage, (size_t)cols * 8, (size_t)cols * 8, rows,
                                     cudaMemcpyHostToDevice, c->stream), "upload"))
     return false;
   return cuda_ok(c, cudaStreamSynchronize(c->stream), "upload sync");
@@ -210,11 +266,31 @@ bool download_plane(cps_ctx* c, double* dst, const double* src, int rows, int co
   return true;
 }
 
-double* plane_ptr(cps_ctx* c, int k) { return reinterpret_cast<double*>(c->slab) + (size_t)k * c->plane_elems; }
+double* field_ptr(cps_ctx* c, int k) { return reinterpret_cast<double*>(c->slab) + (size_t)k * c->plane_elems; }
+
+template <typename T>
+void bind_inner(cps_ctx* c, cps::Inner<T>& w) {
+  T* base = reinterpret_cast<T*>(c->slab + c->plane_elems * sizeof(double) * kFieldPlanes);
+  auto pl = [&](int k) { return base + (size_t)k * c->plane_elems; };
+  w.cU = pl(0); w.cV = pl(5);
+  w.bU = pl(10); w.bV = pl(11);
+  w.xU0 = pl(12); w.xU1 = pl(13); w.xV0 = pl(14); w.xV1 = pl(15);
+  w.px = pl(16); w.pr = pl(17); w.pz = pl(18); w.pp0 = pl(19); w.pp1 = pl(20); w.pAp = pl(21);
+  w.pdiag = pl(22); w.cx = pl(23); w.cy = pl(24);
+}
 
 void set_step_inputs(cps_ctx* c, double Uin) {
   c->view.Uin = Uin;
   c->view.maxVel = 3.0 * std::max(std::fabs(Uin), 0.1);  // iterations.cpp:104
+}
+
+const void* grid_kernel_for(int precision) {
+  return precision == CPS_MIXED ? (const void*)cps_grid_kernel<float> : (const void*)cps_grid_kernel<double>;
+}
+
+void to_step_out(const double* h, cps_step_out* o) {
+  o->residU = h[0]; o->residV = h[1]; o->residMass = h[2]; o->residMassDof = h[3]; o->err = h[4];
+  o->pIters = (int)h[5]; o->uSweeps = (int)h[6]; o->vSweeps = (int)h[7];
 }
 
 cps_status run(cps_ctx* c, int n_outer, int stop_on_conv, double eps, cps_step_out* hist, int* n_done) {
@@ -222,11 +298,15 @@ cps_status run(cps_ctx* c, int n_outer, int stop_on_conv, double eps, cps_step_o
   while (done_total < n_outer) {
     const int chunk = std::min(kHistChunk, n_outer - done_total);
     cps::RunControl rc{chunk, stop_on_conv, eps, c->dhist, c->dndone, c->dstatus};
-    if (!cuda_ok(c, cudaMemsetAsync(c->dndone, 0, sizeof(int), c->stream), "memset")) return CPS_ERR_CUDA;
-    void* args[] = {&c->view, &rc, &c->bar, &c->red};
-    if (!cuda_ok(c, cudaLaunchCooperativeKernel((const void*)cps_grid_kernel, dim3(c->grid), dim3(cps::kThreads), args,
-                                                0, c->stream), "cooperative launch"))
+    if (!cuda_ok(c, cudaMemsetAsync(c->dndone, 0, sizeof(int), c->stream), "memset") ||
+        !cuda_ok(c, cudaMemsetAsync(c->bar, 0, sizeof(cps::GridBarrier), c->stream), "memset"))
       return CPS_ERR_CUDA;
+    void* args[] = {&c->view, &rc, &c->bar, &c->red};
+    if (!cuda_ok(c, cudaEventRecord(c->ev0, c->stream), "event")) return CPS_ERR_CUDA;
+    if (!cuda_ok(c, cudaLaunchCooperativeKernel(grid_kernel_for(c->precision), dim3(c->grid), dim3(cps::kThreads),
+                                                args, 0, c->stream), "cooperative launch"))
+      return CPS_ERR_CUDA;
+    if (!cuda_ok(c, cudaEventRecord(c->ev1, c->stream), "event")) return CPS_ERR_CUDA;
     if (!cuda_ok(c, cudaMemcpyAsync(c->hflags, c->dstatus, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream), "d2h"))
       return CPS_ERR_CUDA;
     if (!cuda_ok(c, cudaMemcpyAsync(c->hhist, c->dhist, sizeof(double) * 8 * chunk, cudaMemcpyDeviceToHost, c->stream),
@@ -234,14 +314,12 @@ cps_status run(cps_ctx* c, int n_outer, int stop_on_conv, double eps, cps_step_o
       return CPS_ERR_CUDA;
     if (!cuda_ok(c, cudaStreamSynchronize(c->stream), "kernel")) return CPS_ERR_CUDA;
     const int status = c->hflags[0], nd = c->hflags[1];
-    if (hist) {
-      for (int k = 0; k < nd; ++k) {
-        const double* h = c->hhist + (size_t)8 * k;
-        cps_step_out& o = hist[done_total + k];
-        o.residU = h[0]; o.residV = h[1]; o.residMass = h[2]; o.residMassDof = h[3]; o.err = h[4];
-        o.pIters = (int)h[5]; o.uSweeps = (int)h[6]; o.vSweeps = (int)h[7];
-      }
-    }
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, c->ev0, c->ev1) == cudaSuccess) c->kernel_ms += ms;
+    c->launches += 1;
+    c->outer_done += nd;
+    if (hist)
+      for (int k = 0; k < nd; ++k) to_step_out(c->hhist + (size_t)8 * k, &hist[done_total + k]);
     done_total += nd;
     if (n_done) *n_done = done_total;
     if (status != cps::kStatusOk) {
@@ -257,11 +335,61 @@ cps_status run(cps_ctx* c, int n_outer, int stop_on_conv, double eps, cps_step_o
   return CPS_OK;
 }
 
+// Per-device scratch of cps_batch_solve, grown on demand and reused.
+struct BatchWorkspace {
+  int device = -1;
+  size_t cap = 0;
+  cps::BatchItem* items = nullptr;
+  int* order = nullptr;
+  int* queue = nullptr;
+  cps::BatchResult* results = nullptr;
+  cps::BatchItem* h_items = nullptr;
+  int* h_order = nullptr;
+  cps::BatchResult* h_results = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+std::mutex g_batch_mutex;
+std::vector<BatchWorkspace> g_batch_ws;
+
+BatchWorkspace* batch_workspace(int device, size_t n, std::string& err) {
+  BatchWorkspace* ws = nullptr;
+  for (auto& w : g_batch_ws)
+    if (w.device == device) ws = &w;
+  if (!ws) {
+    g_batch_ws.emplace_back();
+    ws = &g_batch_ws.back();
+    ws->device = device;
+    if (cudaEventCreate(&ws->ev0) != cudaSuccess || cudaEventCreate(&ws->ev1) != cudaSuccess) {
+      err = "event create failed";
+      return nullptr;
+    }
+  }
+  if (ws->cap < n) {
+    cudaFree(ws->items); cudaFree(ws->order); cudaFree(ws->queue); cudaFree(ws->results);
+    cudaFreeHost(ws->h_items); cudaFreeHost(ws->h_order); cudaFreeHost(ws->h_results);
+    ws->items = nullptr; ws->order = nullptr; ws->queue = nullptr; ws->results = nullptr;
+    ws->h_items = nullptr; ws->h_order = nullptr; ws->h_results = nullptr;
+    ws->cap = 0;
+    const size_t cap = std::max<size_t>(n, 64);
+    if (cudaMalloc(&ws->items, cap * sizeof(cps::BatchItem)) != cudaSuccess ||
+        cudaMalloc(&ws->order, cap * sizeof(int)) != cudaSuccess || cudaMalloc(&ws->queue, 256) != cudaSuccess ||
+        cudaMalloc(&ws->results, cap * sizeof(cps::BatchResult)) != cudaSuccess ||
+        cudaMallocHost(&ws->h_items, cap * sizeof(cps::BatchItem)) != cudaSuccess ||
+        cudaMallocHost(&ws->h_order, cap * sizeof(int)) != cudaSuccess ||
+        cudaMallocHost(&ws->h_results, cap * sizeof(cps::BatchResult)) != cudaSuccess) {
+      err = "batch workspace allocation failed";
+      return nullptr;
+    }
+    ws->cap = cap;
+  }
+  return ws;
+}
+
 }  // namespace
 
 extern "C" {
 
-const char* cps_version(void) { return "cps 0.1 (sm_100a)"; }
+const char* cps_version(void) { return "cps 0.2 (sm_100a)"; }
 
 const char* cps_last_error(const cps_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
 
@@ -269,7 +397,7 @@ cps_status cps_footprint(const cps_desc* desc, unsigned long long* bytes) {
   cps_status s = validate(desc);
   if (s != CPS_OK) return s;
   if (!bytes) return fail(nullptr, CPS_ERR_ARG, "bytes is NULL");
-  *bytes = footprint_bytes(desc->M, desc->N, nullptr, nullptr);
+  *bytes = footprint_bytes(desc->M, desc->N, desc->precision, nullptr, nullptr);
   return CPS_OK;
 }
 
@@ -278,14 +406,13 @@ cps_status cps_create(const cps_desc* d, cps_ctx** out) {
   *out = nullptr;
   cps_status s = validate(d);
   if (s != CPS_OK) return s;
-  if (d->precision != CPS_FP64) return fail(nullptr, CPS_ERR_ARG, "this entry point builds FP64 contexts only");
   cps_ctx* c = new (std::nothrow) cps_ctx();
   if (!c) return fail(nullptr, CPS_ERR_OOM, "host allocation failed");
   c->device = d->device;
   c->M = d->M;
   c->N = d->N;
-  c->slab_bytes = footprint_bytes(d->M, d->N, &c->plane_elems, &c->P);
-  c->R = d->M + 1;
+  c->precision = d->precision;
+  c->slab_bytes = footprint_bytes(d->M, d->N, d->precision, &c->plane_elems, &c->P);
   auto bail = [&](cps_status st) {
     g_create_error = c->err;
     cps_destroy(c);
@@ -299,18 +426,21 @@ cps_status cps_create(const cps_desc* d, cps_ctx** out) {
     return bail(CPS_ERR_OOM);
   }
   if (!cuda_ok(c, cudaMemsetAsync(c->slab, 0, c->slab_bytes, c->stream), "memset")) return bail(CPS_ERR_CUDA);
+  if (!cuda_ok(c, cudaEventCreate(&c->ev0), "event") || !cuda_ok(c, cudaEventCreate(&c->ev1), "event"))
+    return bail(CPS_ERR_CUDA);
   const size_t stage = (size_t)(d->M + 1) * (d->N + 1);
   if (!cuda_ok(c, cudaMallocHost(&c->hstage, stage * sizeof(double)), "pinned alloc") ||
       !cuda_ok(c, cudaMallocHost(&c->hhist, (size_t)kHistChunk * 8 * sizeof(double)), "pinned alloc") ||
       !cuda_ok(c, cudaMallocHost(&c->hflags, 4 * sizeof(int)), "pinned alloc"))
     return bail(CPS_ERR_OOM);
 
-  char* tail = c->slab + c->plane_elems * sizeof(double) * kNumPlanes;
+  char* tail = c->slab + c->plane_elems * sizeof(double) * kFieldPlanes +
+               round_up(c->plane_elems * elem_bytes(d->precision) * kInnerPlanes, 256);
   c->bar = reinterpret_cast<cps::GridBarrier*>(tail);
   c->dstatus = reinterpret_cast<int*>(tail + 64);  // [0] status, [1] n_done
   c->dndone = c->dstatus + 1;
   c->red = reinterpret_cast<double*>(tail + 256);
-  c->dhist = c->red + (size_t)cps::kRedSlots * 2048 * cps::kRedWidth;
+  c->dhist = c->red + (size_t)cps::kRedSlots * kMaxGridCtas * cps::kRedWidth;
   c->dplane = c->dhist + (size_t)kHistChunk * 8;
 
   cps::DesignView& v = c->view;
@@ -333,15 +463,13 @@ cps_status cps_create(const cps_desc* d, cps_ctx** out) {
   const double tolsq = d->momentumTol * d->momentumTol;
   v.thrU = tolsq * (double)((d->M - 1) * (d->N - 2));
   v.thrV = tolsq * (double)((d->M - 2) * (d->N - 1));
-  v.u = plane_ptr(c, kU); v.v = plane_ptr(c, kV); v.p = plane_ptr(c, kP); v.pc = plane_ptr(c, kPc);
-  v.us = plane_ptr(c, kUs); v.vs = plane_ptr(c, kVs); v.dE = plane_ptr(c, kDE); v.dN = plane_ptr(c, kDN);
-  v.alpha = plane_ptr(c, kAlpha); v.gamma = plane_ptr(c, kGamma);
-  v.cU = plane_ptr(c, kCU0); v.cV = plane_ptr(c, kCV0);
+  v.u = field_ptr(c, kU); v.v = field_ptr(c, kV); v.p = field_ptr(c, kP); v.pc = field_ptr(c, kPc);
+  v.us = field_ptr(c, kUs); v.vs = field_ptr(c, kVs); v.dE = field_ptr(c, kDE); v.dN = field_ptr(c, kDN);
+  v.alpha = field_ptr(c, kAlpha); v.gamma = field_ptr(c, kGamma);
   v.planeStride = (long long)c->plane_elems;
-  v.bU = plane_ptr(c, kBU); v.bV = plane_ptr(c, kBV);
-  v.xU0 = plane_ptr(c, kXU0); v.xU1 = plane_ptr(c, kXU1); v.xV0 = plane_ptr(c, kXV0); v.xV1 = plane_ptr(c, kXV1);
-  v.px = plane_ptr(c, kPx); v.pr = plane_ptr(c, kPr); v.pz = plane_ptr(c, kPz); v.pp0 = plane_ptr(c, kPp0);
-  v.pp1 = plane_ptr(c, kPp1); v.pAp = plane_ptr(c, kPAp); v.pdiag = plane_ptr(c, kPdiag);
+  std::memset(&v.f64, 0, sizeof(v.f64));
+  std::memset(&v.f32, 0, sizeof(v.f32));
+  if (d->precision == CPS_MIXED) bind_inner<float>(c, v.f32); else bind_inner<double>(c, v.f64);
   set_step_inputs(c, 0.0);
 
   if (!upload_plane(c, v.alpha, d->alpha, d->M, d->N, d->layout) ||
@@ -350,17 +478,16 @@ cps_status cps_create(const cps_desc* d, cps_ctx** out) {
 
   // Persistent grid: co-resident CTAs, at most one per tile of the design.
   int per_sm = 0, sms = 0;
-  if (!cuda_ok(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cps_grid_kernel, cps::kThreads, 0),
-               "occupancy") ||
+  if (!cuda_ok(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_kernel_for(d->precision),
+                                                                cps::kThreads, 0), "occupancy") ||
       !cuda_ok(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->device), "attribute"))
     return bail(CPS_ERR_CUDA);
   if (per_sm < 1) return bail(fail(c, CPS_ERR_CUDA, "persistent kernel does not fit on an SM"));
   const int tiles = ((d->M - 1 + cps::kTileI - 1) / cps::kTileI) * ((d->N - 1 + cps::kTileJ - 1) / cps::kTileJ);
-  int grid = d->grid_ctas > 0 ? d->grid_ctas : std::min(sms * per_sm, std::max(1, (tiles + 1) / 2));
-  grid = std::min(std::min(grid, sms * per_sm), 2048);
+  int grid = d->grid_ctas > 0 ? d->grid_ctas : std::min(sms, std::max(1, (tiles + 1) / 2));
+  grid = std::min(std::min(grid, sms * per_sm), kMaxGridCtas);
   grid = std::max(1, std::min(grid, tiles));
   c->grid = grid;
-  c->precision = d->precision;
   *out = c;
   return CPS_OK;
 }
@@ -372,8 +499,45 @@ void cps_destroy(cps_ctx* c) {
   if (c->hstage) cudaFreeHost(c->hstage);
   if (c->hhist) cudaFreeHost(c->hhist);
   if (c->hflags) cudaFreeHost(c->hflags);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
+}
+
+cps_status cps_upload_geometry(cps_ctx* c, const double* alpha, const double* gamma, int layout) {
+  if (!c || !alpha || !gamma) return fail(c, CPS_ERR_ARG, "ctx, alpha and gamma are required");
+  if (layout != CPS_ROW_MAJOR && layout != CPS_COL_MAJOR) return fail(c, CPS_ERR_ARG, "bad layout");
+  if (!cuda_ok(c, cudaSetDevice(c->device), "cudaSetDevice")) return CPS_ERR_CUDA;
+  if (!upload_plane(c, c->view.alpha, alpha, c->M, c->N, layout) ||
+      !upload_plane(c, c->view.gamma, gamma, c->M, c->N, layout))
+    return CPS_ERR_CUDA;
+  return CPS_OK;
+}
+
+cps_status cps_reset_fields(cps_ctx* c) {
+  if (!c) return fail(nullptr, CPS_ERR_ARG, "ctx is NULL");
+  if (!cuda_ok(c, cudaSetDevice(c->device), "cudaSetDevice")) return CPS_ERR_CUDA;
+  // Planes u .. dN are contiguous at the start of the slab.
+  if (!cuda_ok(c, cudaMemsetAsync(c->slab, 0, c->plane_elems * sizeof(double) * (kDN + 1), c->stream), "memset"))
+    return CPS_ERR_CUDA;
+  return CPS_OK;
+}
+
+cps_status cps_get_stream(cps_ctx* c, void** stream) {
+  if (!c || !stream) return fail(c, CPS_ERR_ARG, "ctx and stream are required");
+  *stream = (void*)c->stream;
+  return CPS_OK;
+}
+
+cps_status cps_kernel_timing(cps_ctx* c, double* kernel_ms, long long* launches, long long* outer_iterations,
+                             int reset) {
+  if (!c) return fail(nullptr, CPS_ERR_ARG, "ctx is NULL");
+  if (kernel_ms) *kernel_ms = c->kernel_ms;
+  if (launches) *launches = c->launches;
+  if (outer_iterations) *outer_iterations = c->outer_done;
+  if (reset) { c->kernel_ms = 0.0; c->launches = 0; c->outer_done = 0; }
+  return CPS_OK;
 }
 
 cps_status cps_upload_fields(cps_ctx* c, const double* u, const double* v, const double* p, int layout) {
@@ -392,8 +556,7 @@ cps_status cps_step(cps_ctx* c, const cps_step_in* in, cps_step_out* out) {
   set_step_inputs(c, in->inletVelocity);
   int nd = 0;
   cps_step_out tmp;
-  cps_status s = run(c, 1, 0, 0.0, out ? out : &tmp, &nd);
-  return s;
+  return run(c, 1, 0, 0.0, out ? out : &tmp, &nd);
 }
 
 cps_status cps_solve(cps_ctx* c, double inletVelocity, int max_outer, double eps, cps_step_out* history,
@@ -405,6 +568,118 @@ cps_status cps_solve(cps_ctx* c, double inletVelocity, int max_outer, double eps
   if (!cuda_ok(c, cudaSetDevice(c->device), "cudaSetDevice")) return CPS_ERR_CUDA;
   set_step_inputs(c, inletVelocity);
   return run(c, max_outer, eps > 0.0 ? 1 : 0, eps, history, n_done);
+}
+
+cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVelocity, const cps_batch_opts* opts,
+                           cps_batch_result* results, double* kernel_ms) {
+  if (!ctxs || n <= 0 || !opts || !results) return fail(nullptr, CPS_ERR_ARG, "ctxs, n > 0, opts and results required");
+  if (opts->max_outer < 0) return fail(nullptr, CPS_ERR_ARG, "max_outer < 0");
+  const int cl = opts->cluster_ctas > 0 ? opts->cluster_ctas : 8;
+  if (cl > 16) return fail(nullptr, CPS_ERR_ARG, "cluster_ctas must be <= 16");
+  cps_ctx* c0 = ctxs[0];
+  for (int k = 0; k < n; ++k) {
+    if (!ctxs[k]) return fail(nullptr, CPS_ERR_ARG, "NULL context in batch");
+    if (ctxs[k]->device != c0->device || ctxs[k]->precision != c0->precision)
+      return fail(nullptr, CPS_ERR_ARG, "a batch needs one device and one precision");
+  }
+  std::lock_guard<std::mutex> lock(g_batch_mutex);
+  if (!cuda_ok(c0, cudaSetDevice(c0->device), "cudaSetDevice")) return CPS_ERR_CUDA;
+  std::string err;
+  BatchWorkspace* ws = batch_workspace(c0->device, (size_t)n, err);
+  if (!ws) return fail(c0, CPS_ERR_OOM, err);
+  for (int k = 0; k < n; ++k) {
+    cps_ctx* c = ctxs[k];
+    set_step_inputs(c, inletVelocity ? inletVelocity[k] : c->view.Uin);
+    cps::BatchItem& it = ws->h_items[k];
+    std::memset(&it, 0, sizeof(it));
+    it.view = c->view;
+    it.n_outer = opts->max_outer;
+    it.stop_on_conv = opts->eps > 0.0 ? 1 : 0;
+    it.eps = opts->eps;
+    it.hist = c->dhist;
+    it.hist_cap = kHistChunk;
+  }
+  std::vector<int> ord(n);
+  std::iota(ord.begin(), ord.end(), 0);
+  if (opts->order_by_size)
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
+      return (long long)ctxs[a]->M * ctxs[a]->N > (long long)ctxs[b]->M * ctxs[b]->N;
+    });
+  std::copy(ord.begin(), ord.end(), ws->h_order);
+  cudaStream_t st = c0->stream;
+  if (!cuda_ok(c0, cudaMemcpyAsync(ws->items, ws->h_items, sizeof(cps::BatchItem) * n, cudaMemcpyHostToDevice, st),
+               "h2d") ||
+      !cuda_ok(c0, cudaMemcpyAsync(ws->order, ws->h_order, sizeof(int) * n, cudaMemcpyHostToDevice, st), "h2d") ||
+      !cuda_ok(c0, cudaMemsetAsync(ws->queue, 0, sizeof(int), st), "memset") ||
+      !cuda_ok(c0, cudaMemsetAsync(ws->results, 0, sizeof(cps::BatchResult) * n, st), "memset"))
+    return CPS_ERR_CUDA;
+  using KernFn = void (*)(const cps::BatchItem*, const int*, int, int*, cps::BatchResult*);
+  KernFn kern = c0->precision == CPS_MIXED ? (KernFn)cps_cluster_kernel<float> : (KernFn)cps_cluster_kernel<double>;
+  if (cl > 8 &&
+      !cuda_ok(c0, cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1), "attr"))
+    return CPS_ERR_CUDA;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cl;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim = dim3(cps::kThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cfg.gridDim = dim3(cl * 64);
+  int max_clusters = 0;
+  if (!cuda_ok(c0, cudaOccupancyMaxActiveClusters(&max_clusters, (const void*)kern, &cfg), "cluster occupancy"))
+    return CPS_ERR_CUDA;
+  if (max_clusters < 1) return fail(c0, CPS_ERR_CUDA, "cluster configuration does not fit");
+  int clusters = std::min(max_clusters, n);
+  if (opts->max_clusters > 0) clusters = std::min(clusters, opts->max_clusters);
+  cfg.gridDim = dim3(cl * clusters);
+  const cps::BatchItem* items = ws->items;
+  const int* order = ws->order;
+  int* queue = ws->queue;
+  cps::BatchResult* res = ws->results;
+  if (!cuda_ok(c0, cudaEventRecord(ws->ev0, st), "event")) return CPS_ERR_CUDA;
+  if (!cuda_ok(c0, cudaLaunchKernelEx(&cfg, kern, items, order, n, queue, res), "cluster launch")) return CPS_ERR_CUDA;
+  if (!cuda_ok(c0, cudaEventRecord(ws->ev1, st), "event") ||
+      !cuda_ok(c0, cudaMemcpyAsync(ws->h_results, ws->results, sizeof(cps::BatchResult) * n, cudaMemcpyDeviceToHost,
+                                   st), "d2h") ||
+      !cuda_ok(c0, cudaStreamSynchronize(st), "batch kernel"))
+    return CPS_ERR_CUDA;
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, ws->ev0, ws->ev1);
+  if (kernel_ms) *kernel_ms = ms;
+  cps_status status = CPS_OK;
+  for (int k = 0; k < n; ++k) {
+    const cps::BatchResult& r = ws->h_results[k];
+    results[k].n_done = r.n_done;
+    results[k].converged = r.converged;
+    results[k].status = r.status == cps::kStatusOk ? CPS_OK : CPS_ERR_DIVERGED;
+    to_step_out(r.last, &results[k].last);
+    ctxs[k]->outer_done += r.n_done;
+    if (r.status != cps::kStatusOk) {
+      status = CPS_ERR_DIVERGED;
+      ctxs[k]->err = "residual is not finite (solution diverged)";
+    }
+  }
+  c0->kernel_ms += ms;
+  c0->launches += 1;
+  if (status != CPS_OK) g_create_error = "at least one design diverged; see results[k].status";
+  return status;
+}
+
+cps_status cps_get_history(cps_ctx* c, int n, cps_step_out* history) {
+  if (!c || !history || n < 0 || n > kHistChunk) return fail(c, CPS_ERR_ARG, "bad history request");
+  if (!cuda_ok(c, cudaSetDevice(c->device), "cudaSetDevice")) return CPS_ERR_CUDA;
+  if (n == 0) return CPS_OK;
+  if (!cuda_ok(c, cudaMemcpyAsync(c->hhist, c->dhist, sizeof(double) * 8 * n, cudaMemcpyDeviceToHost, c->stream),
+               "d2h") ||
+      !cuda_ok(c, cudaStreamSynchronize(c->stream), "sync"))
+    return CPS_ERR_CUDA;
+  for (int k = 0; k < n; ++k) to_step_out(c->hhist + (size_t)8 * k, &history[k]);
+  return CPS_OK;
 }
 
 cps_status cps_sample_plane(cps_ctx* c, double x, cps_plane* out) {

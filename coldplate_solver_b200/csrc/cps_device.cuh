@@ -22,15 +22,30 @@
 //
 // Matrix-free: no CSR is built.  The momentum coefficients of each unknown are
 // stored once per outer iteration (5 per unknown) because the Jacobi sweeps
-// reuse them; the pressure coefficients are rebuilt on the fly from dE, dN.
-// Every product/sum that feeds a stored value is evaluated in the reference's
-// order, and this translation unit is compiled with --fmad=false, so per-point
-// values equal the FP64 reference's; only the grid-wide sums (Jacobi RMS, PCG
-// dots) are summed in a different (fixed, deterministic) order.
+// reuse them; the pressure matrix is held as its two face-conductance planes
+// (east and north faces) and its diagonal.
 //
-// Layout: one pitched row-major array per field in the reference's (i, j)
+// Two arithmetic modes share this code through the storage type T of the
+// inner-solve arrays:
+//   T = double (plain FP64, the drop-in judge).  Every product/sum that feeds
+//     a stored value is evaluated in the reference's order and the unit is
+//     compiled with --fmad=false, so per-point values equal the FP64
+//     reference's; only the grid-wide sums (Jacobi RMS, PCG dots) are added
+//     in a different (fixed, deterministic) order.
+//   T = float (mixed).  Fields, momentum coefficients, the momentum defect
+//     r0 = b - A u, the mass imbalance and every dot product / norm are FP64;
+//     the Jacobi iterate is the correction delta (A delta = r0) and the PCG
+//     vectors are stored in FP32.  Each outer iteration is one FP64 defect-
+//     correction step, so the converged state is the FP64 fixed point.
+//
+// Two groups of CTAs can run a design: the whole grid (cooperative launch,
+// software barrier with bounded waits) or one thread-block cluster (hardware
+// cluster barrier, DSMEM reductions; used by the batched kernel).
+//
+// Layout: one pitched row-major plane per field in the reference's (i, j)
 // index space; element (i, j) at base[i * P + j] with P >= N + 1 a multiple of
-// 32 doubles, so a warp's 32 consecutive j are one 256-byte segment.
+// 32 elements, so a warp's 32 consecutive j are one 256-byte (FP64) or
+// 128-byte (FP32) segment.
 #pragma once
 #include <cuda_runtime.h>
 #include <cooperative_groups.h>
@@ -44,10 +59,25 @@ constexpr int kThreads = 256;   // 8 warps
 constexpr int kTileI = 8;       // tile rows (one warp per row)
 constexpr int kTileJ = 32;      // tile columns (one lane per column)
 constexpr int kRedWidth = 8;    // doubles per CTA per reduction
-constexpr int kRedSlots = 4;    // ring of reduction slots
+constexpr int kRedSlots = 4;    // ring of reduction slots (grid group)
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
 
 enum DeviceStatus : int { kStatusOk = 0, kStatusTimeout = 1, kStatusDiverged = 2 };
+
+// Inner-solve arrays of one design in storage type T.
+template <typename T>
+struct Inner {
+  T* cU;            // 5 planes (E, W, N, S, P) of U-momentum coefficients, stride planeStride
+  T* cV;            // same for V
+  T* bU;            // FP64 mode: source b; mixed: defect r0 = b - A u
+  T* bV;
+  T* xU0; T* xU1;   // Jacobi iterates (FP64: x; mixed: the correction delta)
+  T* xV0; T* xV1;
+  T* px; T* pr; T* pz; T* pp0; T* pp1; T* pAp;  // PCG vectors
+  T* pdiag;         // pressure diagonal aP
+  T* cx;            // rho dE hy: conductance of the east face of P-cell (i, j)
+  T* cy;            // rho dN hx: conductance of the north face of P-cell (i, j)
+};
 
 // Device view of one design's grid, parameters and arrays.
 struct DesignView {
@@ -58,14 +88,16 @@ struct DesignView {
   double thrU, thrV;                              // momTol^2 * nU, momTol^2 * nV
   double Uin, maxVel;
   double *u, *v, *p, *pc, *us, *vs, *dE, *dN, *alpha, *gamma;
-  double *cU, *cV;          // 5 planes each (E, W, N, S, P), plane stride = planeStride
-  double *bU, *bV;
-  double *xU0, *xU1, *xV0, *xV1;
-  double *px, *pr, *pz, *pp0, *pp1, *pAp, *pdiag;
-  long long planeStride;    // elements between coefficient planes
+  long long planeStride;                          // elements between coefficient planes
+  Inner<double> f64;
+  Inner<float> f32;
 };
 
-// Per-launch control shared by all CTAs.
+template <typename T> __device__ __forceinline__ const Inner<T>& inner(const DesignView& d);
+template <> __device__ __forceinline__ const Inner<double>& inner<double>(const DesignView& d) { return d.f64; }
+template <> __device__ __forceinline__ const Inner<float>& inner<float>(const DesignView& d) { return d.f32; }
+
+// Per-launch control of the single-design (grid) kernel.
 struct RunControl {
   int n_outer;        // outer iterations to run
   int stop_on_conv;   // stop once max(residU, residV, residMassDof) <= eps
@@ -75,9 +107,27 @@ struct RunControl {
   int* status;        // DeviceStatus
 };
 
+// One entry of the batched (cluster) kernel's work list.
+struct BatchItem {
+  DesignView view;
+  int n_outer;        // outer-iteration budget of this visit
+  int stop_on_conv;
+  double eps;
+  double* hist;       // hist_cap x 8 (the first hist_cap iterations of the visit), may be null
+  int hist_cap;
+  int pad;
+};
+struct BatchResult {
+  int n_done;         // outer iterations run in this visit
+  int status;         // DeviceStatus
+  int converged;
+  int pad;
+  double last[8];     // diagnostics of the last iteration
+};
+
+// Monotonic arrival counter of the grid barrier; zeroed before every launch.
 struct GridBarrier {
-  unsigned int count;
-  unsigned int gen;
+  unsigned long long count;
 };
 
 // ---------------------------------------------------------------------------
@@ -87,13 +137,15 @@ __device__ __forceinline__ double maxd(double a, double b) { return (a < b) ? b 
 __device__ __forceinline__ double mind(double a, double b) { return (b < a) ? b : a; }
 __device__ __forceinline__ double clampd(double v, double lo, double hi) { return (v < lo) ? lo : (hi < v) ? hi : v; }
 
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ unsigned long long atom_add_acq_rel_u64(unsigned long long* p, unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+  return old;
 }
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
   unsigned long long t;
@@ -141,24 +193,25 @@ struct GridGroup {
   int* status;
   unsigned rank, nblk;
   unsigned redCount;  // reductions issued so far (same in every CTA)
+  unsigned long long epoch;  // barriers passed in this launch
 
-  // Returns false (and the CTA must return) on timeout or on an error raised elsewhere.
+  // Arrive (release) and wait (acquire) for all nblk CTAs: barrier k is
+  // complete once the counter reaches k * nblk.  The CTA's writes are ordered
+  // before thread 0's release by __syncthreads (cumulativity), and thread 0's
+  // acquire before the other threads' reads by the trailing __syncthreads.
+  // Returns false (the CTA must return) on timeout or on an error raised elsewhere.
   __device__ bool sync() {
     __shared__ int s_ok;
     __syncthreads();
+    ++epoch;
     if (threadIdx.x == 0) {
       int ok = 1;
-      __threadfence();
-      const unsigned g = ld_acquire_u32(&bar->gen);
-      const unsigned arrived = atomicAdd(&bar->count, 1u);
-      if (arrived == nblk - 1) {
-        atomicExch(&bar->count, 0u);
-        __threadfence();
-        st_release_u32(&bar->gen, g + 1);
-      } else {
+      const unsigned long long target = epoch * nblk;
+      const unsigned long long old = atom_add_acq_rel_u64(&bar->count, 1ull);
+      if (old + 1 < target) {
         const unsigned long long t0 = globaltimer_ns();
         unsigned spins = 0;
-        while (ld_acquire_u32(&bar->gen) == g) {
+        while (ld_acquire_u64(&bar->count) < target) {
           if ((++spins & 255u) == 0) {
             if (*(volatile int*)status != kStatusOk) { ok = 0; break; }
             if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
@@ -169,7 +222,6 @@ struct GridGroup {
           }
         }
       }
-      __threadfence();
       s_ok = ok;
     }
     __syncthreads();
@@ -190,7 +242,7 @@ struct GridGroup {
     if (!sync()) return false;
     double acc[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) acc[k] = ((MaxMask >> k) & 1u) ? 0.0 : 0.0;
+    for (int k = 0; k < K; ++k) acc[k] = 0.0;
     bool first = true;
     for (unsigned b = threadIdx.x; b < nblk; b += kThreads) {
 #pragma unroll
@@ -199,6 +251,48 @@ struct GridGroup {
         acc[k] = first ? x : (((MaxMask >> k) & 1u) ? maxd(acc[k], x) : acc[k] + x);
       }
       first = false;
+    }
+    block_reduce<K, MaxMask>(acc, smem);
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = acc[k];
+    return true;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Group of CTAs working on one design: one thread-block cluster.  The cluster
+// barrier is a hardware barrier with release/acquire semantics at cluster
+// scope (no spin loop); partial sums travel through distributed shared memory.
+// ---------------------------------------------------------------------------
+struct ClusterGroup {
+  double* redbuf;     // this CTA's shared-memory ring, 2 x kRedWidth
+  int* status;        // the current design's status word
+  unsigned rank, nblk;
+  unsigned redCount;
+
+  __device__ bool sync() {
+    cg::this_cluster().sync();
+    return true;
+  }
+
+  template <int K, unsigned MaxMask>
+  __device__ bool sync_reduce(double (&v)[K], double* smem) {
+    block_reduce<K, MaxMask>(v, smem);
+    double* slot = redbuf + (redCount & 1u) * kRedWidth;
+    ++redCount;
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int k = 0; k < K; ++k) slot[k] = v[k];
+    }
+    cg::cluster_group cl = cg::this_cluster();
+    cl.sync();
+    double acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = 0.0;
+    if (threadIdx.x < nblk) {
+      const double* remote = cl.map_shared_rank(slot, threadIdx.x);
+#pragma unroll
+      for (int k = 0; k < K; ++k) acc[k] = remote[k];
     }
     block_reduce<K, MaxMask>(acc, smem);
 #pragma unroll
@@ -245,8 +339,12 @@ __device__ __forceinline__ double sou_correction(const DesignView& d, const doub
 // Momentum assembly at one unknown (momentum_solver.cpp:203-296) fused with
 // Jacobi sweep 1 (jacobi_solver.cpp:49-57, x0 = current velocity).  Returns the
 // squared residual of sweep 1 (0 when no sweep is run).
-template <bool IsU>
+//   FP64:  b = Sp, x1 = x0 + (b - A x0)/aP.
+//   mixed: b = r0 = Sp - A x0 (FP64 defect), delta1 = r0/aP (delta0 = 0).
+template <bool IsU, typename T>
 __device__ __forceinline__ double assemble_point(const DesignView& d, int i, int j, bool sweep) {
+  constexpr bool kMixed = sizeof(T) == 4;
+  const Inner<T>& w = inner<T>(d);
   const int M = d.M, N = d.N, P = d.P;
   const double* __restrict__ u = d.u;
   const double* __restrict__ v = d.v;
@@ -291,19 +389,14 @@ __device__ __forceinline__ double assemble_point(const DesignView& d, int i, int
   if (hasW) cW = -aW; else Sp += aW * xW;
   if (hasN) cN = -aN; else Sp += aN * xN;
   if (hasS) cS = -aS; else Sp += aS * xS;
-  double* c = IsU ? d.cU : d.cV;
+  T* c = IsU ? w.cU : w.cV;
   const long long ps = d.planeStride;
   const size_t o = (size_t)i * P + j;
-  c[o] = cE;
-  c[o + ps] = cW;
-  c[o + 2 * ps] = cN;
-  c[o + 3 * ps] = cS;
-  c[o + 4 * ps] = aP;
-  (IsU ? d.bU : d.bV)[o] = Sp;
-  if (!sweep) {
-    (IsU ? d.xU0 : d.xV0)[o] = velCur;
-    return 0.0;
-  }
+  c[o] = (T)cE;
+  c[o + ps] = (T)cW;
+  c[o + 2 * ps] = (T)cN;
+  c[o + 3 * ps] = (T)cS;
+  c[o + 4 * ps] = (T)aP;
   double Ax = 0.0;
   if (hasS) Ax += cS * xS;
   if (hasW) Ax += cW * xW;
@@ -311,62 +404,71 @@ __device__ __forceinline__ double assemble_point(const DesignView& d, int i, int
   if (hasE) Ax += cE * xE;
   if (hasN) Ax += cN * xN;
   const double r = Sp - Ax;
-  (IsU ? d.xU1 : d.xV1)[o] = velCur + r / aP;
+  if (kMixed) {
+    (IsU ? w.bU : w.bV)[o] = (T)r;
+    if (!sweep) {
+      (IsU ? w.xU0 : w.xV0)[o] = (T)0.0;
+      return 0.0;
+    }
+    (IsU ? w.xU1 : w.xV1)[o] = (T)(r / aP);
+    return r * r;
+  }
+  (IsU ? w.bU : w.bV)[o] = (T)Sp;
+  if (!sweep) {
+    (IsU ? w.xU0 : w.xV0)[o] = (T)velCur;
+    return 0.0;
+  }
+  (IsU ? w.xU1 : w.xV1)[o] = (T)(velCur + r / aP);
   return r * r;
 }
 
-// Jacobi sweep k >= 2 at one unknown (jacobi_solver.cpp:49-57).
-template <bool IsU>
-__device__ __forceinline__ double sweep_point(const DesignView& d, int i, int j, const double* __restrict__ xin,
-                                              double* __restrict__ xout) {
+// Jacobi sweep k >= 2 at one unknown (jacobi_solver.cpp:49-57).  Arithmetic in
+// FP64 on the stored values.
+template <bool IsU, typename T>
+__device__ __forceinline__ double sweep_point(const DesignView& d, int i, int j, const T* __restrict__ xin,
+                                              T* __restrict__ xout) {
+  const Inner<T>& w = inner<T>(d);
   const int M = d.M, N = d.N, P = d.P;
   const int iHi = IsU ? M - 1 : M - 2, jHi = IsU ? N - 2 : N - 1;
-  const double* __restrict__ c = IsU ? d.cU : d.cV;
+  const T* __restrict__ c = IsU ? w.cU : w.cV;
   const long long ps = d.planeStride;
   const size_t o = (size_t)i * P + j;
   double Ax = 0.0;
-  if (i - 1 >= 1) Ax += __ldg(c + o + 3 * ps) * xin[o - P];
-  if (j - 1 >= 1) Ax += __ldg(c + o + ps) * xin[o - 1];
-  const double aP = c[o + 4 * ps];
-  const double x0 = xin[o];
+  if (i - 1 >= 1) Ax += (double)c[o + 3 * ps] * (double)xin[o - P];
+  if (j - 1 >= 1) Ax += (double)c[o + ps] * (double)xin[o - 1];
+  const double aP = (double)c[o + 4 * ps];
+  const double x0 = (double)xin[o];
   Ax += aP * x0;
-  if (j + 1 <= jHi) Ax += c[o] * xin[o + 1];
-  if (i + 1 <= iHi) Ax += c[o + 2 * ps] * xin[o + P];
-  const double r = (IsU ? d.bU : d.bV)[o] - Ax;
-  xout[o] = x0 + r / aP;
+  if (j + 1 <= jHi) Ax += (double)c[o] * (double)xin[o + 1];
+  if (i + 1 <= iHi) Ax += (double)c[o + 2 * ps] * (double)xin[o + P];
+  const double r = (double)(IsU ? w.bU : w.bV)[o] - Ax;
+  xout[o] = (T)(x0 + r / aP);
   return r * r;
+}
+
+// Final Jacobi value at a U/V unknown: FP64 the iterate, mixed u + delta.
+template <typename T>
+__device__ __forceinline__ double final_velocity(const double* __restrict__ vel, const T* __restrict__ xf, size_t o) {
+  if (sizeof(T) == 4) return vel[o] + (double)xf[o];
+  return (double)xf[o];
 }
 
 // u* after scatter + clamp + velocity BCs, evaluated from the final Jacobi
 // iterate (momentum_solver.cpp:326, boundaries.cpp:57-103).
-__device__ __forceinline__ double ustar_at(const DesignView& d, const double* __restrict__ xU, int i, int j) {
+template <typename T>
+__device__ __forceinline__ double ustar_at(const DesignView& d, const T* __restrict__ xU, int i, int j) {
   const int M = d.M, N = d.N, P = d.P;
   if (i <= 0 || i >= M) return 0.0;
   if (j == 0) return (AT(d.gamma, i - 1, 0) > 0.5) ? d.Uin : 0.0;
   if (j >= N - 1) j = N - 2;
-  return clampd(AT(xU, i, j), -d.maxVel, d.maxVel);
+  return clampd(final_velocity<T>(d.u, xU, (size_t)i * P + j), -d.maxVel, d.maxVel);
 }
-__device__ __forceinline__ double vstar_at(const DesignView& d, const double* __restrict__ xV, int i, int j) {
+template <typename T>
+__device__ __forceinline__ double vstar_at(const DesignView& d, const T* __restrict__ xV, int i, int j) {
   const int M = d.M, N = d.N, P = d.P;
   if (i <= 0 || i >= M - 1 || j == 0) return 0.0;
   if (j >= N) j = N - 1;
-  return clampd(AT(xV, i, j), -d.maxVel, d.maxVel);
-}
-
-// Pressure-correction coefficients of P-unknown (i, j) (pressure_solver.cpp:698-703).
-struct PCoef {
-  double aE, aW, aN, aS, aP;
-};
-__device__ __forceinline__ PCoef pcoef(const DesignView& d, int i, int j) {
-  const int M = d.M, N = d.N, P = d.P;
-  PCoef c;
-  c.aE = (j < N - 1) ? d.rho * AT(d.dE, i, j) * d.hy : 0.0;
-  c.aW = (j > 1) ? d.rho * AT(d.dE, i, j - 1) * d.hy : 0.0;
-  c.aN = (i < M - 1) ? d.rho * AT(d.dN, i, j) * d.hx : 0.0;
-  c.aS = (i > 1) ? d.rho * AT(d.dN, i - 1, j) * d.hx : 0.0;
-  c.aP = c.aE + c.aW + c.aN + c.aS;
-  if (c.aP < 1e-20) c.aP = 1.0;
-  return c;
+  return clampd(final_velocity<T>(d.v, xV, (size_t)i * P + j), -d.maxVel, d.maxVel);
 }
 
 // ---------------------------------------------------------------------------
@@ -385,22 +487,22 @@ __device__ __forceinline__ void for_each_point(const DesignView& d, unsigned ran
 }
 
 // ---------------------------------------------------------------------------
-// One outer iteration for one design on group g.  Returns false if the group
-// must stop (device error).  out[8] receives the step diagnostics.
+// One outer iteration for one design on group g; out[8] receives the step
+// diagnostics.  Returns 0 to continue with another outer iteration, 1 when
+// this one is the last (iteration budget, convergence, or a non-finite
+// residual), -1 when the group must stop because a device-side wait failed.
 // ---------------------------------------------------------------------------
-// Returns 0 to continue with another outer iteration, 1 when this one is the
-// last (iteration budget, convergence, or a non-finite residual), -1 when the
-// group must stop because a device-side wait failed.
-template <class Group>
+template <typename T, class Group>
 __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, double (&out)[8], bool lastIter,
                                bool stopOnConv, double eps) {
+  const Inner<T>& w = inner<T>(d);
   const int M = d.M, N = d.N, P = d.P;
   // ---- A: assembly + sweep 1 ----
   const bool anySweep = d.maxMomIter > 0;
   double red2[2] = {0.0, 0.0};
   for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
-    if (j <= N - 2) red2[0] += assemble_point<true>(d, i, j, anySweep);
-    if (i <= M - 2) red2[1] += assemble_point<false>(d, i, j, anySweep);
+    if (j <= N - 2) red2[0] += assemble_point<true, T>(d, i, j, anySweep);
+    if (i <= M - 2) red2[1] += assemble_point<false, T>(d, i, j, anySweep);
   });
   if (!g.template sync_reduce<2, 0u>(red2, smem)) return -1;
   int kU = anySweep ? 1 : 0, kV = kU;
@@ -409,60 +511,71 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, doub
   // ---- B: sweeps 2.. ----
   while (actU || actV) {
     const int k = (actU ? kU : kV) + 1;  // both active components are at the same sweep
-    const double* xinU = (k & 1) ? d.xU0 : d.xU1;
-    double* xoutU = (k & 1) ? d.xU1 : d.xU0;
-    const double* xinV = (k & 1) ? d.xV0 : d.xV1;
-    double* xoutV = (k & 1) ? d.xV1 : d.xV0;
+    const T* xinU = (k & 1) ? w.xU0 : w.xU1;
+    T* xoutU = (k & 1) ? w.xU1 : w.xU0;
+    const T* xinV = (k & 1) ? w.xV0 : w.xV1;
+    T* xoutV = (k & 1) ? w.xV1 : w.xV0;
     double s[2] = {0.0, 0.0};
     const bool au = actU, av = actV;
     for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
-      if (au && j <= N - 2) s[0] += sweep_point<true>(d, i, j, xinU, xoutU);
-      if (av && i <= M - 2) s[1] += sweep_point<false>(d, i, j, xinV, xoutV);
+      if (au && j <= N - 2) s[0] += sweep_point<true, T>(d, i, j, xinU, xoutU);
+      if (av && i <= M - 2) s[1] += sweep_point<false, T>(d, i, j, xinV, xoutV);
     });
     if (!g.template sync_reduce<2, 0u>(s, smem)) return -1;
     if (au) { kU = k; actU = !(s[0] < d.thrU) && kU < d.maxMomIter; }
     if (av) { kV = k; actV = !(s[1] < d.thrV) && kV < d.maxMomIter; }
   }
-  const double* xfU = (kU & 1) ? d.xU1 : d.xU0;
-  const double* xfV = (kV & 1) ? d.xV1 : d.xV0;
+  const T* xfU = (kU & 1) ? w.xU1 : w.xU0;
+  const T* xfV = (kV & 1) ? w.xV1 : w.xV0;
   // ---- C: scatter, BCs, mass residual, PCG set-up ----
   // residU, residV, residMass, residMassDof, non-finite flag (max); r.z (sum)
   double rc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
     const size_t o = (size_t)i * P + j;
     if (j <= N - 2) {
-      const double val = clampd(xfU[o], -d.maxVel, d.maxVel);
+      const double val = clampd(final_velocity<T>(d.u, xfU, o), -d.maxVel, d.maxVel);
       d.us[o] = val;
       rc[0] = maxd(rc[0], fabs(val - d.u[o]));
       if (!isfinite(val)) rc[4] = 1.0;
       if (j == N - 2) d.us[o + 1] = val;
     }
-    if (j == 1) d.us[o - 1] = ustar_at(d, xfU, i, 0);
+    if (j == 1) d.us[o - 1] = ustar_at<T>(d, xfU, i, 0);
     if (i <= M - 2) {
-      const double val = clampd(xfV[o], -d.maxVel, d.maxVel);
+      const double val = clampd(final_velocity<T>(d.v, xfV, o), -d.maxVel, d.maxVel);
       d.vs[o] = val;
       rc[1] = maxd(rc[1], fabs(val - d.v[o]));
       if (!isfinite(val)) rc[4] = 1.0;
       if (j == N - 1) d.vs[o + 1] = val;
     }
-    const double massE = d.rho * ustar_at(d, xfU, i, j) * d.hy;
-    const double massW = d.rho * ustar_at(d, xfU, i, j - 1) * d.hy;
-    const double massN = d.rho * vstar_at(d, xfV, i, j) * d.hx;
-    const double massS = d.rho * vstar_at(d, xfV, i - 1, j) * d.hx;
+    const double massE = d.rho * ustar_at<T>(d, xfU, i, j) * d.hy;
+    const double massW = d.rho * ustar_at<T>(d, xfU, i, j - 1) * d.hy;
+    const double massN = d.rho * vstar_at<T>(d, xfV, i, j) * d.hx;
+    const double massS = d.rho * vstar_at<T>(d, xfV, i - 1, j) * d.hx;
     const double b = massW - massE + massS - massN;
     const double ab = fabs(b);
     if (!isfinite(ab)) rc[4] = 1.0;
     if (ab > rc[2]) rc[2] = ab;
     if (j <= N - 2) {
       if (ab > rc[3]) rc[3] = ab;
-      const PCoef c = pcoef(d, i, j);
-      d.pdiag[o] = c.aP;
-      d.pr[o] = b;
-      d.px[o] = 0.0;
-      const double z = (fabs(c.aP) > 1e-20) ? b / c.aP : b;
-      d.pz[o] = z;
-      d.pp0[o] = z;
-      rc[5] += b * z;
+      // pressure_solver.cpp:698-703
+      const double aE = (j < N - 1) ? d.rho * AT(d.dE, i, j) * d.hy : 0.0;
+      const double aW = (j > 1) ? d.rho * AT(d.dE, i, j - 1) * d.hy : 0.0;
+      const double aN = (i < M - 1) ? d.rho * AT(d.dN, i, j) * d.hx : 0.0;
+      const double aS = (i > 1) ? d.rho * AT(d.dN, i - 1, j) * d.hx : 0.0;
+      double aP = aE + aW + aN + aS;
+      if (aP < 1e-20) aP = 1.0;
+      const T dg = (T)aP;
+      w.pdiag[o] = dg;
+      w.cx[o] = (T)aE;
+      w.cy[o] = (T)aN;
+      const T rt = (T)b;
+      w.pr[o] = rt;
+      w.px[o] = (T)0.0;
+      const double rr = (double)rt, dd = (double)dg;
+      const T z = (T)((fabs(dd) > 1e-20) ? rr / dd : rr);
+      w.pz[o] = z;
+      w.pp0[o] = z;
+      rc[5] += rr * (double)z;
     }
   });
   if (!g.template sync_reduce<6, 0x1Fu>(rc, smem)) return -1;
@@ -482,14 +595,14 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, doub
   // The max reductions drop NaN the way std::max does, so non-finite values
   // are flagged explicitly.
   const bool finite = isfinite(e) && isfinite(out[3]) && rc[4] == 0.0;
-  if (!finite && g.rank == 0 && threadIdx.x == 0) atomicCAS(g.status, kStatusOk, kStatusDiverged);
+  if (!finite && g.rank == 0 && threadIdx.x == 0 && g.status) atomicCAS(g.status, kStatusOk, kStatusDiverged);
   const bool stop = lastIter || !finite || (stopOnConv && conv <= eps);
   // ---- P: Jacobi-preconditioned CG ----
   double rz = rc[5], beta = 0.0;
   int it = 0;
   for (; it < d.maxPIter; ++it) {
-    const double* pold = (it & 1) ? d.pp0 : d.pp1;  // p_{it-1}
-    double* pcur = (it & 1) ? d.pp1 : d.pp0;        // p_it
+    const T* pold = (it & 1) ? w.pp0 : w.pp1;  // p_{it-1}
+    T* pcur = (it & 1) ? w.pp1 : w.pp0;        // p_it
     const int k = it;
     const double bt = beta;
     double s1[1] = {0.0};
@@ -497,18 +610,20 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, doub
       if (j > N - 2) return;
       const size_t o = (size_t)i * P + j;
       // p_k at (i, j) and its unknown neighbours: p = z + beta p (pressure_solver.cpp:181)
-      auto pk = [&](size_t q) -> double { return k == 0 ? d.pp0[q] : d.pz[q] + bt * pold[q]; };
-      const PCoef c = pcoef(d, i, j);
+      auto pk = [&](size_t q) -> double {
+        return k == 0 ? (double)w.pp0[q] : (double)(T)((double)w.pz[q] + bt * (double)pold[q]);
+      };
       const double pc0 = pk(o);
       double Ap = 0.0;
-      if (i > 1) Ap += -c.aS * pk(o - P);
-      if (j > 1) Ap += -c.aW * pk(o - 1);
-      Ap += c.aP * pc0;
-      if (j + 1 <= N - 2) Ap += -c.aE * pk(o + 1);
-      if (i < M - 1) Ap += -c.aN * pk(o + P);
-      if (k > 0) pcur[o] = pc0;
-      d.pAp[o] = Ap;
-      s1[0] += pc0 * Ap;
+      if (i > 1) Ap += -(double)w.cy[o - P] * pk(o - P);
+      if (j > 1) Ap += -(double)w.cx[o - 1] * pk(o - 1);
+      Ap += (double)w.pdiag[o] * pc0;
+      if (j + 1 <= N - 2) Ap += -(double)w.cx[o] * pk(o + 1);
+      if (i < M - 1) Ap += -(double)w.cy[o] * pk(o + P);
+      if (k > 0) pcur[o] = (T)pc0;
+      const T apt = (T)Ap;
+      w.pAp[o] = apt;
+      s1[0] += pc0 * (double)apt;
     });
     if (!g.template sync_reduce<1, 0u>(s1, smem)) return -1;
     const double pAp = s1[0];
@@ -518,14 +633,15 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, doub
     for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
       if (j > N - 2) return;
       const size_t o = (size_t)i * P + j;
-      d.px[o] = d.px[o] + alpha * pcur[o];
-      const double r = d.pr[o] - alpha * d.pAp[o];
-      d.pr[o] = r;
+      w.px[o] = (T)((double)w.px[o] + alpha * (double)pcur[o]);
+      const T rt = (T)((double)w.pr[o] - alpha * (double)w.pAp[o]);
+      w.pr[o] = rt;
+      const double r = (double)rt;
       s2[0] += r * r;
-      const double dg = d.pdiag[o];
-      const double z = (fabs(dg) > 1e-20) ? r / dg : r;
-      d.pz[o] = z;
-      s2[1] += r * z;
+      const double dg = (double)w.pdiag[o];
+      const T z = (T)((fabs(dg) > 1e-20) ? r / dg : r);
+      w.pz[o] = z;
+      s2[1] += r * (double)z;
     });
     if (!g.template sync_reduce<2, 0u>(s2, smem)) return -1;
     if (sqrt(s2[0]) < d.pTol) break;
@@ -537,7 +653,7 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, doub
   // ---- D: pressure and velocity correction ----
   for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
     const size_t o = (size_t)i * P + j;
-    const double pcv = (j == N - 1) ? 0.0 : d.px[o];
+    const double pcv = (j == N - 1) ? 0.0 : (double)w.px[o];
     d.pc[o] = pcv;
     const double pn = d.p[o] + d.pAlpha * pcv;
     d.p[o] = pn;
@@ -547,7 +663,7 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, doub
     if (j == N - 1) d.p[o + 1] = 0.0;
     const double mv = d.maxVel;
     if (j <= N - 2) {
-      const double pcE = (j + 1 == N - 1) ? 0.0 : d.px[o + 1];
+      const double pcE = (j + 1 == N - 1) ? 0.0 : (double)w.px[o + 1];
       double du = d.dE[o] * (pcv - pcE);
       du = maxd(-mv, mind(mv, du));
       double un = d.us[o] + du;
@@ -556,7 +672,7 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, doub
       if (j == N - 2) d.u[o + 1] = un;
     }
     if (i <= M - 2) {
-      const double pcN = (j == N - 1) ? 0.0 : d.px[o + P];
+      const double pcN = (j == N - 1) ? 0.0 : (double)w.px[o + P];
       double dv = d.dN[o] * (pcv - pcN);
       dv = maxd(-mv, mind(mv, dv));
       double vn = d.vs[o] + dv;

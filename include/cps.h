@@ -126,6 +126,57 @@ cps_status cps_sample_plane(cps_ctx* ctx, double x, cps_plane* out);
 cps_status cps_download_fields(cps_ctx* ctx, double* u, double* v, double* p, double* pStar, double* uStar,
                                double* vStar, double* dE, double* dN, int layout);
 
+/* Replace alpha and gamma (M x N) of an existing context: the outputs of the
+ * reference's loadTopology/loadDensityField/buildAlphaFromDensity
+ * (SIMPLE.cpp:517-630) for a new design of the same grid. */
+cps_status cps_upload_geometry(cps_ctx* ctx, const double* alpha, const double* gamma, int layout);
+
+/* Zero u, v, p and every derived field on the device: the state cps_create
+ * leaves (SIMPLE.cpp:184-197), without a host copy. */
+cps_status cps_reset_fields(cps_ctx* ctx);
+
+/* The cudaStream_t (as void*) every call of this context issues its work on,
+ * for callers that time or order work against it. */
+cps_status cps_get_stream(cps_ctx* ctx, void** stream);
+
+/* Device time of the outer-iteration kernel launches issued since the last
+ * reset, measured with CUDA events on the launching stream; reset != 0
+ * clears the counters after reading. */
+cps_status cps_kernel_timing(cps_ctx* ctx, double* kernel_ms, long long* launches, long long* outer_iterations,
+                             int reset);
+
+/* Options of a batched solve. */
+typedef struct {
+  int cluster_ctas;   /* CTAs of the thread-block cluster that runs one design (1..16; 0 = 8) */
+  int max_clusters;   /* upper bound on concurrent clusters (0 = as many as fit) */
+  int max_outer;      /* outer-iteration budget of every design in this call */
+  double eps;         /* stop a design once max(residU, residV, residMassDof) <= eps (0 = never) */
+  int order_by_size;  /* start the largest designs first */
+} cps_batch_opts;
+
+/* Per-design outcome of a batched solve. */
+typedef struct {
+  int n_done;         /* outer iterations run in this call */
+  int converged;      /* the eps test passed on the last iteration */
+  int status;         /* CPS_OK or CPS_ERR_DIVERGED */
+  cps_step_out last;  /* diagnostics of the last iteration */
+} cps_batch_result;
+
+/* Many designs in one persistent launch: each design runs on one thread-block
+ * cluster (hardware cluster barrier, no host round trips) until it meets eps
+ * or spends max_outer outer iterations; clusters take designs from a device
+ * work queue, so designs of uneven size share the GPU.  Every context must be
+ * on the same device with the same precision.  Has no reference counterpart:
+ * the reference solves one design per process (SIMPLE.cpp:638-642).
+ * inletVelocity: n values or NULL to keep each context's last value.
+ * *kernel_ms (may be NULL) receives the launch's device time. */
+cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVelocity, const cps_batch_opts* opts,
+                           cps_batch_result* results, double* kernel_ms);
+
+/* The first n (<= 4096) diagnostics of the last cps_solve launch chunk or
+ * cps_batch_solve visit of this context. */
+cps_status cps_get_history(cps_ctx* ctx, int n, cps_step_out* history);
+
 /* Device bytes held by a context created from desc (admission control). */
 cps_status cps_footprint(const cps_desc* desc, unsigned long long* bytes);
 

@@ -39,6 +39,9 @@
 
 #include "SIMPLE.h"
 #include "Utilities/solvers/cpu/jacobi_solver.h"
+#ifdef CPS_DROPIN
+#include "b200_dropin.h"
+#endif
 
 typedef decltype(SIMPLE::hx) real;                 // float as shipped, double when promoted
 typedef decltype(SIMPLE::u) Matrix;                // Eigen::MatrixXf / MatrixXd
@@ -208,7 +211,7 @@ int main(int argc, char** argv) {
     s.maxPressureIter = geti(recs, "maxPIter");
     s.momentumTol = static_cast<real>(getd(recs, "momTol"));
     s.maxMomentumIter = geti(recs, "maxMomIter");
-    s.pressureSolverType = 1;           // Parallel CG (pressure_solver.cpp:759)
+    s.pressureSolverType = recs.count("solverType") ? geti(recs, "solverType") : 1;  // 1 = Parallel CG
     s.momentumSolverType = 1;           // implicit Jacobi (iterations.cpp:109)
     s.enablePseudoTimeStepping = false; // SIMPLE.h:262 default
     s.usePressureDropConvergence = false;
@@ -235,6 +238,9 @@ int main(int argc, char** argv) {
       auto t0 = std::chrono::steady_clock::now();
       real err = s.calculateStep(pIt);
       elapsed += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+#ifdef CPS_DROPIN
+      if (s.pressureSolverType == 5) b200SyncFieldsToHost(s);  // uStar/vStar for the residual below
+#endif
       real massDof = mass_residual_dof(s);
       hU.push_back(s.residU);
       hV.push_back(s.residV);
@@ -247,6 +253,9 @@ int main(int argc, char** argv) {
       double conv = std::max({(double)s.residU, (double)s.residV, (double)massDof});
       if (stopOnConv && conv <= eps) break;
     }
+#ifdef CPS_DROPIN
+    if (s.pressureSolverType == 5) b200SyncFieldsToHost(s);  // fields live on the GPU between steps
+#endif
     w.d("residU", hU);
     w.d("residV", hV);
     w.d("residMass", hMass);

@@ -23,7 +23,10 @@ REF_DIR = os.path.join(_HERE, "_ref")
 
 
 def binary(precision: str) -> str:
-    return os.path.join(REF_DIR, "ref_f64" if precision == "f64" else "ref_f32")
+    """"f64": the reference promoted to FP64; "f32": as shipped; "dropin": the
+    FP64 reference with the B200 drop-in patched into calculateStep (selected
+    by pressureSolverType = 5), linked to libcps.so."""
+    return os.path.join(REF_DIR, {"f64": "ref_f64", "f32": "ref_f32", "dropin": "ref_dropin"}[precision])
 
 
 def available(precision: str = "f64") -> bool:
@@ -56,7 +59,10 @@ def run(design, max_outer: int, precision: str = "f64", eps: float = 1e-6, stop_
         raise FileNotFoundError(f"{binary(precision)} not built (make -C oracle ref)")
     with tempfile.TemporaryDirectory(prefix="cps_ref_") as tmp:
         cpath, opath = os.path.join(tmp, "case.bin"), os.path.join(tmp, "out.bin")
-        casefile.write_records(cpath, case_records(design, max_outer, eps, stop_on_conv, threads, init))
+        rec = case_records(design, max_outer, eps, stop_on_conv, threads, init)
+        if precision == "dropin":
+            rec["solverType"] = [5]
+        casefile.write_records(cpath, rec)
         env = dict(os.environ, OMP_NUM_THREADS=str(threads))
         proc = subprocess.run([binary(precision), cpath, opath], cwd=tmp, env=env, stdout=subprocess.DEVNULL,
                               stderr=subprocess.PIPE, timeout=timeout)
