@@ -230,7 +230,7 @@ def run_b200(args) -> None:
 
     def one_solve():
         solver.reset_fields()
-        return solver.solve(MAX_OUTER, eps=EPS)
+        return solver.solve(args.max_outer, eps=EPS)
 
     hist = None
     for _ in range(args.warmup):
@@ -277,7 +277,7 @@ def run_b200(args) -> None:
     for _ in range(e2e_steps):
         solver.upload_geometry(alpha, gamma)
         solver.upload_fields(host_in["u"], host_in["v"], host_in["p"])
-        solver.solve(MAX_OUTER, eps=EPS)
+        solver.solve(args.max_outer, eps=EPS)
         solver.download()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world, local)
     barrier(world)
@@ -380,6 +380,8 @@ def main() -> None:
     ap.add_argument("--cpu-sample-iters", type=int, default=200)
     ap.add_argument("--ref-sample-iters", type=int, default=300)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--max-outer", type=int, default=MAX_OUTER,
+                    help="cap on outer iterations per solve (small profiling captures; the line then says converged=false)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
