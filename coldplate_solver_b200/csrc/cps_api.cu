@@ -484,7 +484,7 @@ cps_status cps_create(const cps_desc* d, cps_ctx** out) {
     return bail(CPS_ERR_CUDA);
   if (per_sm < 1) return bail(fail(c, CPS_ERR_CUDA, "persistent kernel does not fit on an SM"));
   const int tiles = ((d->M - 1 + cps::kTileI - 1) / cps::kTileI) * ((d->N - 1 + cps::kTileJ - 1) / cps::kTileJ);
-  int grid = d->grid_ctas > 0 ? d->grid_ctas : std::min(sms, std::max(1, (tiles + 1) / 2));
+  int grid = d->grid_ctas > 0 ? d->grid_ctas : std::min(sms * per_sm, std::max(1, (tiles + 1) / 2));
   grid = std::min(std::min(grid, sms * per_sm), kMaxGridCtas);
   grid = std::max(1, std::min(grid, tiles));
   c->grid = grid;

@@ -30,8 +30,9 @@ def test_reference_driver_with_b200_branch(case):
         n = int(z["n_outer"])
     a = reference.run(d, n, precision="dropin", init=init)
     b = reference.run(d, n, precision="f64", init=init)
-    for k in ("pIters", "uSweeps", "vSweeps"):
-        assert np.array_equal(a[k], b[k]), k
+    # calculateStep's signature carries the PCG count only (iterations.cpp:82); the
+    # Jacobi sweep counts are not observable through it on the B200 branch.
+    assert np.array_equal(a["pIters"], b["pIters"])
     for k in ("residU", "residV", "residMass", "residMassDof", "err"):
         np.testing.assert_allclose(a[k], b[k], rtol=1e-8, atol=1e-300)
     for k in FIELDS:

@@ -3,9 +3,12 @@
 FP64 path.
 
 Tolerances: a mixed-precision outer iteration applies FP32 corrections to FP64
-fields, so from an identical state its fields agree with the FP64 step to
-REL_MIXED_STEP = 1e-5 relative L2; at convergence both sit on the same FP64
-fixed point (REL_FIELD = 1e-6, REL_DP = 1e-5, as for the FP64 path).  A
+fields.  Its later Jacobi sweeps test the RMS stop rule on FP32-stored values,
+so a sweep can stop one sweep before or after the FP64 one; from an identical
+state its fields therefore agree with the FP64 step to REL_MIXED_STEP = 1e-4
+relative L2 (one Jacobi update of a stiff Brinkman field is ~4e-5).  At
+convergence both sit on the same FP64 fixed point (REL_FIELD = 1e-6,
+REL_DP = 1e-5, as for the FP64 path).  A
 batched design differs from the same design solved alone on the whole grid
 only in the grouping of the grid-wide sums: REL_STEP = 1e-10 and identical
 inner iteration counts.
@@ -17,7 +20,7 @@ from coldplate_solver_b200 import cps, geometry
 
 pytestmark = pytest.mark.gpu
 
-REL_MIXED_STEP = 1e-5
+REL_MIXED_STEP = 1e-4
 REL_STEP = 1e-10
 REL_FIELD = 1e-6
 REL_DP = 1e-5
