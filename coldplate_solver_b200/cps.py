@@ -95,6 +95,9 @@ SIGNATURES = {
     "cps_batch_solve": (ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_int, _D, ctypes.POINTER(CpsBatchOpts),
                                        ctypes.POINTER(CpsBatchResult), _D]),
     "cps_get_history": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(CpsStepOut)]),
+    "cps_solve_noalloc": (ctypes.c_int, [ctypes.POINTER(CpsDesc), ctypes.c_int, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
+                                         ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.POINTER(CpsStepOut),
+                                         ctypes.POINTER(ctypes.c_int), _P]),
     "cps_last_error": (ctypes.c_char_p, [_P]),
     "cps_version": (ctypes.c_char_p, []),
 }

@@ -177,6 +177,31 @@ cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVeloc
  * cps_batch_solve visit of this context. */
 cps_status cps_get_history(cps_ctx* ctx, int n, cps_step_out* history);
 
+/* Allocation-free FP64 solve of one design, for callers that cannot call
+ * cudaMalloc (an application that owns all device memory through its own
+ * pool, a real-time loop that must not enter the driver's allocator, a plugin
+ * handed only buffers and a stream).  No counterpart in the reference.
+ *
+ * The caller passes device buffers, all with row pitch `pitch` (>= N+1
+ * doubles): alpha, gamma (M rows, inputs), u, v, p ((M+1) rows, inputs and
+ * outputs), and pStar, uStar, vStar, dE, dN ((M+1) rows, outputs, zeroed by
+ * the call first).  Runs up to max_outer (<= 4096) outer iterations on
+ * `stream` (a cudaStream_t; NULL = default stream), stopping when
+ * max(residU, residV, residMassDof) <= eps (eps > 0); history (host, may be
+ * NULL) and *n_done as for cps_solve; desc's alpha/gamma/layout/device/
+ * grid_ctas are ignored and precision must be CPS_FP64.
+ *
+ * All scratch lives in one static device array of about 27 MB per GPU, held
+ * until the process exits; designs need (M+1)*pitch <= 131072 elements or are
+ * rejected with CPS_ERR_ARG (reason printed to stderr).  Every call on a device
+ * shares that array: calls overlapping on the GPU race, so serialise them.
+ * The first call on a device looks up the array's device address; make it
+ * before any stream capture. */
+cps_status cps_solve_noalloc(const cps_desc* desc, int pitch, const double* alpha, const double* gamma, double* u,
+                             double* v, double* p, double* pStar, double* uStar, double* vStar, double* dE,
+                             double* dN, double inletVelocity, int max_outer, double eps, cps_step_out* history,
+                             int* n_done, void* stream);
+
 /* Device bytes held by a context created from desc (admission control). */
 cps_status cps_footprint(const cps_desc* desc, unsigned long long* bytes);
 
