@@ -1,13 +1,16 @@
 """Batched solves of many designs of uneven size, and the project's autotuner.
 
-A batch runs every design on one thread-block cluster (``cps_batch_solve``);
-the two knobs are the cluster size (CTAs per design: more CTAs shorten one
-design's phases, fewer CTAs let more designs run at once) and the number of
-outer iterations a design runs per launch (its "visit": long visits amortise
-the launch, short ones let the host retire converged designs and admit new
-ones sooner).  :func:`autotune` times short visits of a sample of the actual
-designs for each candidate cluster size and keeps the fastest in cell-updates
-per second; results are cached per size bucket.
+A batch places every design on a group of CTAs of one persistent launch
+(``cps_batch_solve``): either a group of K CTAs of a cooperative launch with a
+software group barrier, or one thread-block cluster with the hardware cluster
+barrier.  The knobs are the placement (CTAs per design: more CTAs shorten one
+design's phases, fewer CTAs let more designs run at once, and the designs in
+flight share the 126 MB L2) and the number of outer iterations a design runs
+per launch (its "visit": long visits amortise the launch, short ones let the
+host retire converged designs and admit new ones sooner).  :func:`autotune`
+times short visits of a sample of the actual designs for each candidate
+placement and keeps the fastest in cell-updates per second; results are
+cached per size bucket.
 """
 from __future__ import annotations
 
@@ -21,7 +24,21 @@ import numpy as np
 from . import cps
 from .geometry import Design
 
-CLUSTER_CANDIDATES = (2, 4, 8, 16)
+def mode_candidates(device: int = 0) -> List[dict]:
+    """Placements the autotuner tries: groups of 2x, 1x, 1/2x and 1/4x the SM
+    count of CTAs (2, 1, 2 ... designs in flight at 2 CTAs per SM) and
+    thread-block clusters of 8 and 16 CTAs."""
+    try:
+        import torch
+        sms = torch.cuda.get_device_properties(device).multi_processor_count
+    except Exception:  # noqa: BLE001 - no torch/GPU: B200 count
+        sms = 148
+    groups = [2 * sms, sms, sms // 2, sms // 4]
+    return [{"group_ctas": k} for k in groups if k >= 1] + [{"cluster_ctas": 8}, {"cluster_ctas": 16}]
+
+
+def mode_label(mode: dict) -> str:
+    return ",".join(f"{k}={v}" for k, v in sorted(mode.items()))
 
 
 def size_bucket(cells: float) -> int:
@@ -31,73 +48,110 @@ def size_bucket(cells: float) -> int:
 
 @dataclass
 class TuneResult:
-    cluster_ctas: int
-    cell_updates_per_s: Dict[int, float] = field(default_factory=dict)
+    mode: dict
+    cell_updates_per_s: Dict[str, float] = field(default_factory=dict)
 
 
-_CACHE: Dict[Tuple[int, int], TuneResult] = {}
+_CACHE: Dict[Tuple[int, int, int], TuneResult] = {}
 
 
-def autotune(designs: Sequence[Design], precision: int = cps.CPS_FP64, device: int = 0, sample: int = 12,
-             visit: int = 30, candidates: Sequence[int] = CLUSTER_CANDIDATES, use_cache: bool = True) -> TuneResult:
-    """Pick the cluster size with the highest cell-updates/s on a sample of
-    ``designs`` (``visit`` outer iterations each, from the zero state)."""
+def autotune(designs: Sequence[Design], precision: int = cps.CPS_FP64, device: int = 0, sample: int = 8,
+             visit: int = 60, candidates: Optional[Sequence[dict]] = None, use_cache: bool = True) -> TuneResult:
+    """Pick the placement with the highest cell-updates/s on a sample of
+    ``designs`` (``visit`` outer iterations each, from the zero state, after a
+    short warm-up)."""
     cells = float(np.median([d.M * d.N for d in designs]))
-    key = (size_bucket(cells), precision)
+    key = (size_bucket(cells), precision, min(sample, len(designs)))
     if use_cache and key in _CACHE:
         return _CACHE[key]
+    cands = list(candidates) if candidates is not None else mode_candidates(device)
     rng = np.random.default_rng(0)
     idx = rng.choice(len(designs), size=min(sample, len(designs)), replace=False)
     chosen = [designs[int(k)] for k in idx]
     solvers = [cps.Solver(d, precision=precision, device=device) for d in chosen]
-    rates: Dict[int, float] = {}
+    rates: Dict[str, float] = {}
+    best, best_rate = cands[0], -1.0
     try:
-        cps.batch_solve(solvers, 2, eps=0.0, cluster_ctas=candidates[0])  # warm-up (module load, first touch)
-        for c in candidates:
+        cps.batch_solve(solvers, 2, eps=0.0, **cands[0])  # warm-up (module load, first touch)
+        for mode in cands:
             for s in solvers:
                 s.reset_fields()
-            res, ms = cps.batch_solve(solvers, visit, eps=0.0, cluster_ctas=c)
+            try:
+                res, ms = cps.batch_solve(solvers, visit, eps=0.0, **mode)
+            except cps.CpsError:
+                continue  # placement does not fit this device
             work = sum(r["n_done"] * s.design.M * s.design.N for r, s in zip(res, solvers))
-            rates[c] = work / (ms / 1e3) if ms > 0 else 0.0
+            rate = work / (ms / 1e3) if ms > 0 else 0.0
+            rates[mode_label(mode)] = rate
+            if rate > best_rate:
+                best, best_rate = mode, rate
     finally:
         for s in solvers:
             s.close()
-    best = max(rates, key=rates.get)
-    out = TuneResult(cluster_ctas=best, cell_updates_per_s=rates)
+    out = TuneResult(mode=dict(best), cell_updates_per_s=rates)
     _CACHE[key] = out
     return out
 
 
-def solve_batch(designs: Sequence[Design], eps: float = 1e-6, max_outer: int = 200000,
-                precision: int = cps.CPS_FP64, cluster_ctas: Optional[int] = None, visit: int = 0,
-                device: int = 0) -> Tuple[List[dict], float]:
-    """Solve all designs to ``eps``; returns (per-design results, device ms).
+class BatchRunner:
+    """A set of designs kept resident on one GPU and solved together.
 
-    ``visit`` > 0 splits the work into launches of at most ``visit`` outer
-    iterations per design (converged designs leave the batch between
-    launches); 0 runs everything in one launch."""
-    if cluster_ctas is None:
-        cluster_ctas = autotune(designs, precision, device).cluster_ctas
-    solvers = [cps.Solver(d, precision=precision, device=device) for d in designs]
-    total_ms = 0.0
-    results: List[Optional[dict]] = [None] * len(designs)
-    done_iters = [0] * len(designs)
-    try:
-        active = list(range(len(designs)))
+    ``run()`` resets every design to the zero state on the device and solves
+    all of them to ``eps`` in launches of at most ``visit`` outer iterations
+    per design; designs that converge leave the batch between launches.
+    ``mode`` is the keyword of :func:`cps.batch_solve` that places designs:
+    ``{"group_ctas": K}`` (groups of K CTAs of one cooperative launch) or
+    ``{"cluster_ctas": C}`` (one thread-block cluster per design)."""
+
+    def __init__(self, designs: Sequence[Design], precision: int = cps.CPS_MIXED, device: int = 0,
+                 mode: Optional[dict] = None):
+        self.designs = list(designs)
+        self.solvers = [cps.Solver(d, precision=precision, device=device) for d in self.designs]
+        self.mode = dict(mode or {"group_ctas": 74})
+
+    def close(self) -> None:
+        for s in self.solvers:
+            s.close()
+        self.solvers = []
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def run(self, eps: float = 1e-6, max_outer: int = 200000, visit: int = 4096, reset: bool = True):
+        """Returns (per-design results with total outer_iterations, device ms, launches)."""
+        if reset:
+            for s in self.solvers:
+                s.reset_fields()
+        n = len(self.solvers)
+        done = [0] * n
+        results: List[Optional[dict]] = [None] * n
+        active = list(range(n))
+        total_ms, launches = 0.0, 0
         while active:
-            budget = max_outer if visit <= 0 else visit
-            budget = min(budget, max(max_outer - min(done_iters[k] for k in active), 1))
-            res, ms = cps.batch_solve([solvers[k] for k in active], budget, eps=eps, cluster_ctas=cluster_ctas)
+            budget = min(visit, max(1, max_outer - min(done[k] for k in active)))
+            res, ms = cps.batch_solve([self.solvers[k] for k in active], budget, eps=eps, **self.mode)
             total_ms += ms
+            launches += 1
             still = []
             for k, r in zip(active, res):
-                done_iters[k] += r["n_done"]
-                r = dict(r, outer_iterations=done_iters[k])
-                results[k] = r
-                if not r["converged"] and r["status"] == 0 and done_iters[k] < max_outer:
+                done[k] += r["n_done"]
+                results[k] = dict(r, outer_iterations=done[k])
+                if not r["converged"] and r["status"] == 0 and done[k] < max_outer:
                     still.append(k)
             active = still
-    finally:
-        for s in solvers:
-            s.close()
-    return results, total_ms
+        return results, total_ms, launches
+
+
+def solve_batch(designs: Sequence[Design], eps: float = 1e-6, max_outer: int = 200000,
+                precision: int = cps.CPS_FP64, mode: Optional[dict] = None, visit: int = 4096,
+                device: int = 0) -> Tuple[List[dict], float]:
+    """Solve all designs to ``eps`` (placement ``mode`` or the autotuner's);
+    returns (per-design results, device ms)."""
+    if mode is None:
+        mode = autotune(designs, precision, device).mode
+    with BatchRunner(designs, precision, device, mode) as runner:
+        res, ms, _ = runner.run(eps=eps, max_outer=max_outer, visit=visit, reset=False)
+    return res, ms

@@ -21,6 +21,7 @@ CPS_OK = 0
 CPS_ERR_ARG, CPS_ERR_OOM, CPS_ERR_CUDA, CPS_ERR_TIMEOUT, CPS_ERR_DIVERGED, CPS_ERR_STATE = -1, -2, -3, -4, -5, -6
 CPS_ROW_MAJOR, CPS_COL_MAJOR = 0, 1
 CPS_FP64, CPS_MIXED = 0, 1
+CPS_PCG_REFERENCE, CPS_PCG_SINGLE_REDUCTION = 0, 1
 
 _STATUS_NAMES = {0: "OK", -1: "CPS_ERR_ARG", -2: "CPS_ERR_OOM", -3: "CPS_ERR_CUDA", -4: "CPS_ERR_TIMEOUT",
                  -5: "CPS_ERR_DIVERGED", -6: "CPS_ERR_STATE"}
@@ -46,6 +47,7 @@ class CpsDesc(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("alpha", ctypes.POINTER(ctypes.c_double)), ("gamma", ctypes.POINTER(ctypes.c_double)),
         ("layout", ctypes.c_int), ("device", ctypes.c_int), ("grid_ctas", ctypes.c_int),
+        ("pcg_variant", ctypes.c_int),
     ]
 
 
@@ -66,7 +68,7 @@ class CpsPlane(ctypes.Structure):
 
 class CpsBatchOpts(ctypes.Structure):
     _fields_ = [("cluster_ctas", ctypes.c_int), ("max_clusters", ctypes.c_int), ("max_outer", ctypes.c_int),
-                ("eps", ctypes.c_double), ("order_by_size", ctypes.c_int)]
+                ("eps", ctypes.c_double), ("order_by_size", ctypes.c_int), ("group_ctas", ctypes.c_int)]
 
 
 class CpsBatchResult(ctypes.Structure):
@@ -133,7 +135,8 @@ def field_shapes(M: int, N: int) -> Dict[str, tuple]:
             "uStar": (M + 1, N), "vStar": (M, N + 1), "dE": (M + 1, N), "dN": (M, N + 1)}
 
 
-def make_desc(design: Design, precision: int = CPS_FP64, device: int = 0, grid_ctas: int = 0):
+def make_desc(design: Design, precision: int = CPS_FP64, device: int = 0, grid_ctas: int = 0,
+              pcg_variant: int = CPS_PCG_REFERENCE):
     """Build a CpsDesc; returns (desc, keepalive) -- keep the arrays alive."""
     alpha = np.ascontiguousarray(design.alpha, dtype=np.float64)
     gamma = np.ascontiguousarray(design.gamma, dtype=np.float64)
@@ -144,7 +147,8 @@ def make_desc(design: Design, precision: int = CPS_FP64, device: int = 0, grid_c
                 enableTwoPointFiveD=int(design.enableTwoPointFiveD),
                 enableConvectionScaling=int(design.enableConvectionScaling), Ht_channel=design.Ht_channel,
                 twoPointFiveDSinkMultiplier=design.twoPointFiveDSinkMultiplier, precision=precision,
-                alpha=_dptr(alpha), gamma=_dptr(gamma), layout=CPS_ROW_MAJOR, device=device, grid_ctas=grid_ctas)
+                alpha=_dptr(alpha), gamma=_dptr(gamma), layout=CPS_ROW_MAJOR, device=device, grid_ctas=grid_ctas,
+                pcg_variant=pcg_variant)
     return d, (alpha, gamma)
 
 
@@ -167,10 +171,11 @@ class Solver:
     ``sample_plane()`` ``samplePlaneAtX`` (postprocessing.cpp:97-230).
     """
 
-    def __init__(self, design: Design, precision: int = CPS_FP64, device: int = 0, grid_ctas: int = 0):
+    def __init__(self, design: Design, precision: int = CPS_FP64, device: int = 0, grid_ctas: int = 0,
+                 pcg_variant: int = CPS_PCG_REFERENCE):
         self.lib = load_library()
         self.design = design
-        desc, keep = make_desc(design, precision, device, grid_ctas)
+        desc, keep = make_desc(design, precision, device, grid_ctas, pcg_variant)
         ctx = _P()
         st = self.lib.cps_create(ctypes.byref(desc), ctypes.byref(ctx))
         if st != CPS_OK:
@@ -284,7 +289,7 @@ def history_to_array(hist, n: int) -> np.ndarray:
 
 
 def batch_solve(solvers, max_outer: int, eps: float = 1e-6, cluster_ctas: int = 8, max_clusters: int = 0,
-                order_by_size: bool = True, inlet_velocities=None):
+                order_by_size: bool = True, inlet_velocities=None, group_ctas: int = 0):
     """Run many resident designs in one persistent cluster launch
     (cps_batch_solve).  Returns (results, kernel_ms); results[k] is a dict with
     n_done, converged, status and the last step's diagnostics."""
@@ -296,11 +301,11 @@ def batch_solve(solvers, max_outer: int, eps: float = 1e-6, cluster_ctas: int = 
     uin = np.ascontiguousarray([s.inletVelocity if inlet_velocities is None else inlet_velocities[k]
                                 for k, s in enumerate(solvers)], dtype=np.float64)
     opts = CpsBatchOpts(cluster_ctas=cluster_ctas, max_clusters=max_clusters, max_outer=max_outer, eps=eps,
-                        order_by_size=int(order_by_size))
+                        order_by_size=int(order_by_size), group_ctas=group_ctas)
     res = (CpsBatchResult * n)()
     ms = ctypes.c_double(0.0)
     st = lib.cps_batch_solve(ctxs, n, _dptr(uin), ctypes.byref(opts), res, ctypes.byref(ms))
-    if st not in (CPS_OK, CPS_ERR_DIVERGED):
+    if st not in (CPS_OK, CPS_ERR_DIVERGED, CPS_ERR_TIMEOUT):
         raise CpsError(st, lib.cps_last_error(None).decode())
     out = []
     for k in range(n):

@@ -137,6 +137,61 @@ __global__ void __launch_bounds__(cps::kThreads) cps_cluster_kernel(const cps::B
   cl.sync();    // no CTA leaves while another may still read its shared memory
 }
 
+// Batched solves on groups of CTAs inside one cooperative launch: CTAs
+// [g*K, (g+1)*K) form group g, which takes designs from the queue one at a
+// time and runs each with the bounded software barrier of its own counter.
+// The group count sets how many designs are in flight (and so the in-flight
+// working set against the 126 MB L2); K sets how many CTAs share one design.
+template <typename T>
+__global__ void __launch_bounds__(cps::kThreads, 2) cps_group_kernel(const cps::BatchItem* __restrict__ items,
+                                                                    const int* __restrict__ order, int n_items,
+                                                                    int* queue, cps::BatchResult* results,
+                                                                    cps::GridBarrier* bars, double* rings,
+                                                                    int* slots, int group_ctas) {
+  __shared__ double smem[cps::kRedWidth * 8];
+  __shared__ __align__(16) cps::BatchItem s_item;
+  const unsigned grp = blockIdx.x / group_ctas;
+  int* slot = slots + 2 * grp;  // [0] next queue index, [1] group status before a design is assigned
+  cps::GridGroup g{bars + grp, rings + (size_t)grp * cps::kRedSlots * group_ctas * cps::kRedWidth, slot + 1,
+                   blockIdx.x % group_ctas, (unsigned)group_ctas, 0u, 0ull};
+  for (;;) {
+    g.status = slot + 1;
+    if (g.rank == 0 && threadIdx.x == 0) slot[0] = atomicAdd(queue, 1);
+    if (!g.sync()) return;
+    const int idx = __ldcg(slot);
+    if (!g.sync()) return;  // every CTA has read the index before the leader takes the next one
+    if (idx >= n_items) return;
+    const int id = order[idx];
+    {
+      const int* src = reinterpret_cast<const int*>(items + id);
+      int* dst = reinterpret_cast<int*>(&s_item);
+      for (int k = threadIdx.x; k < (int)(sizeof(cps::BatchItem) / sizeof(int)); k += blockDim.x) dst[k] = src[k];
+    }
+    __syncthreads();
+    const cps::BatchItem& item = s_item;
+    cps::BatchResult* res = results + id;
+    g.status = &res->status;
+    double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int done = 0;
+    for (int it = 0; it < item.n_outer; ++it) {
+      const int r = cps::outer_iteration<T>(item.view, g, smem, out, it + 1 == item.n_outer, item.stop_on_conv != 0,
+                                            item.eps);
+      if (r < 0) return;  // a bounded wait expired; the design's status says so
+      done = it + 1;
+      if (g.rank == 0 && threadIdx.x == 0 && item.hist && it < item.hist_cap)
+        for (int k = 0; k < 8; ++k) item.hist[(size_t)it * 8 + k] = out[k];
+      if (r != 0) break;
+    }
+    if (g.rank == 0 && threadIdx.x == 0) {
+      res->n_done = done;
+      const double conv = cps::maxd(cps::maxd(out[0], out[1]), out[3]);
+      res->converged = (done > 0 && conv <= item.eps) ? 1 : 0;
+      for (int k = 0; k < 8; ++k) res->last[k] = out[k];
+    }
+    __syncthreads();  // s_item is reloaded next round
+  }
+}
+
 // samplePlaneAtX (postprocessing.cpp:62-230) for one plane, one CTA: every row's
 // contribution is evaluated with the reference's expressions; the five sums are
 // combined in a fixed tree order.
@@ -234,6 +289,8 @@ cps_status validate(const cps_desc* d) {
   if (d->layout != CPS_ROW_MAJOR && d->layout != CPS_COL_MAJOR) return fail(nullptr, CPS_ERR_ARG, "bad layout");
   if (!d->alpha || !d->gamma) return fail(nullptr, CPS_ERR_ARG, "alpha and gamma are required");
   if (d->grid_ctas < 0) return fail(nullptr, CPS_ERR_ARG, "grid_ctas < 0");
+  if (d->pcg_variant != CPS_PCG_REFERENCE && d->pcg_variant != CPS_PCG_SINGLE_REDUCTION)
+    return fail(nullptr, CPS_ERR_ARG, "bad pcg_variant");
   return CPS_OK;
 }
 
@@ -346,6 +403,9 @@ struct BatchWorkspace {
   cps::BatchItem* h_items = nullptr;
   int* h_order = nullptr;
   cps::BatchResult* h_results = nullptr;
+  cps::GridBarrier* bars = nullptr;  // group kernel: one barrier, ring and slot pair per group
+  double* rings = nullptr;
+  int* slots = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 std::mutex g_batch_mutex;
@@ -359,8 +419,11 @@ BatchWorkspace* batch_workspace(int device, size_t n, std::string& err) {
     g_batch_ws.emplace_back();
     ws = &g_batch_ws.back();
     ws->device = device;
-    if (cudaEventCreate(&ws->ev0) != cudaSuccess || cudaEventCreate(&ws->ev1) != cudaSuccess) {
-      err = "event create failed";
+    if (cudaEventCreate(&ws->ev0) != cudaSuccess || cudaEventCreate(&ws->ev1) != cudaSuccess ||
+        cudaMalloc(&ws->bars, sizeof(cps::GridBarrier) * kMaxGridCtas) != cudaSuccess ||
+        cudaMalloc(&ws->rings, sizeof(double) * cps::kRedSlots * kMaxGridCtas * cps::kRedWidth) != cudaSuccess ||
+        cudaMalloc(&ws->slots, sizeof(int) * 2 * kMaxGridCtas) != cudaSuccess) {
+      err = "batch workspace allocation failed";
       return nullptr;
     }
   }
@@ -446,6 +509,7 @@ cps_status cps_create(const cps_desc* d, cps_ctx** out) {
   cps::DesignView& v = c->view;
   v.M = d->M; v.N = d->N; v.P = c->P;
   v.conv = d->convectionScheme; v.maxPIter = d->maxPressureIter; v.maxMomIter = d->maxMomentumIter;
+  v.pcgSingleReduction = d->pcg_variant == CPS_PCG_SINGLE_REDUCTION ? 1 : 0;
   v.hx = d->hx; v.hy = d->hy; v.rho = d->rho; v.uvAlpha = d->uvAlpha; v.pAlpha = d->pAlpha; v.pTol = d->pTol;
   // Derived constants, evaluated in the reference's operation order
   // (momentum_solver.cpp:166-191, 220-222, 261; jacobi_solver.cpp:41, 63).
@@ -613,6 +677,34 @@ cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVeloc
       !cuda_ok(c0, cudaMemsetAsync(ws->queue, 0, sizeof(int), st), "memset") ||
       !cuda_ok(c0, cudaMemsetAsync(ws->results, 0, sizeof(cps::BatchResult) * n, st), "memset"))
     return CPS_ERR_CUDA;
+  if (opts->group_ctas > 0) {
+    // Groups of CTAs in one cooperative launch (all CTAs co-resident).
+    const void* gk = c0->precision == CPS_MIXED ? (const void*)cps_group_kernel<float>
+                                                : (const void*)cps_group_kernel<double>;
+    int per_sm = 0, sms = 0;
+    if (!cuda_ok(c0, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gk, cps::kThreads, 0), "occupancy") ||
+        !cuda_ok(c0, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c0->device), "attribute"))
+      return CPS_ERR_CUDA;
+    const int K = opts->group_ctas;
+    const int max_ctas = std::min(sms * per_sm, kMaxGridCtas);
+    if (K > max_ctas) return fail(c0, CPS_ERR_ARG, "group_ctas exceeds the co-resident CTAs of the device");
+    int groups = std::min(max_ctas / K, n);
+    if (opts->max_clusters > 0) groups = std::min(groups, opts->max_clusters);
+    groups = std::max(groups, 1);
+    if (!cuda_ok(c0, cudaMemsetAsync(ws->bars, 0, sizeof(cps::GridBarrier) * groups, st), "memset") ||
+        !cuda_ok(c0, cudaMemsetAsync(ws->slots, 0, sizeof(int) * 2 * groups, st), "memset"))
+      return CPS_ERR_CUDA;
+    const cps::BatchItem* items = ws->items;
+    const int* order = ws->order;
+    int* queue = ws->queue;
+    cps::BatchResult* res = ws->results;
+    int nn = n, kk = K;
+    void* args[] = {&items, &order, &nn, &queue, &res, &ws->bars, &ws->rings, &ws->slots, &kk};
+    if (!cuda_ok(c0, cudaEventRecord(ws->ev0, st), "event")) return CPS_ERR_CUDA;
+    if (!cuda_ok(c0, cudaLaunchCooperativeKernel(gk, dim3(groups * K), dim3(cps::kThreads), args, 0, st),
+                 "cooperative group launch"))
+      return CPS_ERR_CUDA;
+  } else {
   using KernFn = void (*)(const cps::BatchItem*, const int*, int, int*, cps::BatchResult*);
   KernFn kern = c0->precision == CPS_MIXED ? (KernFn)cps_cluster_kernel<float> : (KernFn)cps_cluster_kernel<double>;
   if (cl > 8 &&
@@ -643,6 +735,7 @@ cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVeloc
   cps::BatchResult* res = ws->results;
   if (!cuda_ok(c0, cudaEventRecord(ws->ev0, st), "event")) return CPS_ERR_CUDA;
   if (!cuda_ok(c0, cudaLaunchKernelEx(&cfg, kern, items, order, n, queue, res), "cluster launch")) return CPS_ERR_CUDA;
+  }
   if (!cuda_ok(c0, cudaEventRecord(ws->ev1, st), "event") ||
       !cuda_ok(c0, cudaMemcpyAsync(ws->h_results, ws->results, sizeof(cps::BatchResult) * n, cudaMemcpyDeviceToHost,
                                    st), "d2h") ||
@@ -656,12 +749,15 @@ cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVeloc
     const cps::BatchResult& r = ws->h_results[k];
     results[k].n_done = r.n_done;
     results[k].converged = r.converged;
-    results[k].status = r.status == cps::kStatusOk ? CPS_OK : CPS_ERR_DIVERGED;
+    results[k].status = r.status == cps::kStatusOk        ? CPS_OK
+                        : r.status == cps::kStatusTimeout ? CPS_ERR_TIMEOUT
+                                                          : CPS_ERR_DIVERGED;
     to_step_out(r.last, &results[k].last);
     ctxs[k]->outer_done += r.n_done;
     if (r.status != cps::kStatusOk) {
-      status = CPS_ERR_DIVERGED;
-      ctxs[k]->err = "residual is not finite (solution diverged)";
+      status = (cps_status)results[k].status;
+      ctxs[k]->err = r.status == cps::kStatusTimeout ? "device group barrier timed out"
+                                                     : "residual is not finite (solution diverged)";
     }
   }
   c0->kernel_ms += ms;

@@ -83,6 +83,7 @@ struct Inner {
 struct DesignView {
   int M, N, P;
   int conv, maxPIter, maxMomIter;
+  int pcgSingleReduction;  // 1: single-reduction PCG recurrences; 0: the reference's two-reduction PCG
   double hx, hy, rho, uvAlpha, pAlpha, pTol;
   double vol, De, Dn, sinkDiag, Fcx, Fcy, relax;  // Fcx = cs*rho*hy, Fcy = cs*rho*hx, relax = (1-uvA)/uvA
   double thrU, thrV;                              // momTol^2 * nU, momTol^2 * nV
@@ -487,125 +488,25 @@ __device__ __forceinline__ void for_each_point(const DesignView& d, unsigned ran
 }
 
 // ---------------------------------------------------------------------------
-// One outer iteration for one design on group g; out[8] receives the step
-// diagnostics.  Returns 0 to continue with another outer iteration, 1 when
-// this one is the last (iteration budget, convergence, or a non-finite
-// residual), -1 when the group must stop because a device-side wait failed.
+// PCG as the reference runs it (pressure_solver.cpp:121-184): two grid-wide
+// reductions per iteration (p.Ap, then |r|^2 and r.z).  Phase P1 forms
+// p = z + beta p on the fly for the 5-point stencil and Ap; phase P2 updates
+// x, r, z.  Returns the reference's iteration count, or -1 if a wait failed.
 // ---------------------------------------------------------------------------
 template <typename T, class Group>
-__device__ int outer_iteration(const DesignView& d, Group& g, double* smem, double (&out)[8], bool lastIter,
-                               bool stopOnConv, double eps) {
+__device__ int pcg_two_reductions(const DesignView& d, Group& g, double* smem, double rz0, double pAp0) {
   const Inner<T>& w = inner<T>(d);
   const int M = d.M, N = d.N, P = d.P;
-  // ---- A: assembly + sweep 1 ----
-  const bool anySweep = d.maxMomIter > 0;
-  double red2[2] = {0.0, 0.0};
-  for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
-    if (j <= N - 2) red2[0] += assemble_point<true, T>(d, i, j, anySweep);
-    if (i <= M - 2) red2[1] += assemble_point<false, T>(d, i, j, anySweep);
-  });
-  if (!g.template sync_reduce<2, 0u>(red2, smem)) return -1;
-  int kU = anySweep ? 1 : 0, kV = kU;
-  bool actU = anySweep && !(red2[0] < d.thrU) && kU < d.maxMomIter;
-  bool actV = anySweep && !(red2[1] < d.thrV) && kV < d.maxMomIter;
-  // ---- B: sweeps 2.. ----
-  while (actU || actV) {
-    const int k = (actU ? kU : kV) + 1;  // both active components are at the same sweep
-    const T* xinU = (k & 1) ? w.xU0 : w.xU1;
-    T* xoutU = (k & 1) ? w.xU1 : w.xU0;
-    const T* xinV = (k & 1) ? w.xV0 : w.xV1;
-    T* xoutV = (k & 1) ? w.xV1 : w.xV0;
-    double s[2] = {0.0, 0.0};
-    const bool au = actU, av = actV;
-    for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
-      if (au && j <= N - 2) s[0] += sweep_point<true, T>(d, i, j, xinU, xoutU);
-      if (av && i <= M - 2) s[1] += sweep_point<false, T>(d, i, j, xinV, xoutV);
-    });
-    if (!g.template sync_reduce<2, 0u>(s, smem)) return -1;
-    if (au) { kU = k; actU = !(s[0] < d.thrU) && kU < d.maxMomIter; }
-    if (av) { kV = k; actV = !(s[1] < d.thrV) && kV < d.maxMomIter; }
-  }
-  const T* xfU = (kU & 1) ? w.xU1 : w.xU0;
-  const T* xfV = (kV & 1) ? w.xV1 : w.xV0;
-  // ---- C: scatter, BCs, mass residual, PCG set-up ----
-  // residU, residV, residMass, residMassDof, non-finite flag (max); r.z (sum)
-  double rc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
-    const size_t o = (size_t)i * P + j;
-    if (j <= N - 2) {
-      const double val = clampd(final_velocity<T>(d.u, xfU, o), -d.maxVel, d.maxVel);
-      d.us[o] = val;
-      rc[0] = maxd(rc[0], fabs(val - d.u[o]));
-      if (!isfinite(val)) rc[4] = 1.0;
-      if (j == N - 2) d.us[o + 1] = val;
-    }
-    if (j == 1) d.us[o - 1] = ustar_at<T>(d, xfU, i, 0);
-    if (i <= M - 2) {
-      const double val = clampd(final_velocity<T>(d.v, xfV, o), -d.maxVel, d.maxVel);
-      d.vs[o] = val;
-      rc[1] = maxd(rc[1], fabs(val - d.v[o]));
-      if (!isfinite(val)) rc[4] = 1.0;
-      if (j == N - 1) d.vs[o + 1] = val;
-    }
-    const double massE = d.rho * ustar_at<T>(d, xfU, i, j) * d.hy;
-    const double massW = d.rho * ustar_at<T>(d, xfU, i, j - 1) * d.hy;
-    const double massN = d.rho * vstar_at<T>(d, xfV, i, j) * d.hx;
-    const double massS = d.rho * vstar_at<T>(d, xfV, i - 1, j) * d.hx;
-    const double b = massW - massE + massS - massN;
-    const double ab = fabs(b);
-    if (!isfinite(ab)) rc[4] = 1.0;
-    if (ab > rc[2]) rc[2] = ab;
-    if (j <= N - 2) {
-      if (ab > rc[3]) rc[3] = ab;
-      // pressure_solver.cpp:698-703
-      const double aE = (j < N - 1) ? d.rho * AT(d.dE, i, j) * d.hy : 0.0;
-      const double aW = (j > 1) ? d.rho * AT(d.dE, i, j - 1) * d.hy : 0.0;
-      const double aN = (i < M - 1) ? d.rho * AT(d.dN, i, j) * d.hx : 0.0;
-      const double aS = (i > 1) ? d.rho * AT(d.dN, i - 1, j) * d.hx : 0.0;
-      double aP = aE + aW + aN + aS;
-      if (aP < 1e-20) aP = 1.0;
-      const T dg = (T)aP;
-      w.pdiag[o] = dg;
-      w.cx[o] = (T)aE;
-      w.cy[o] = (T)aN;
-      const T rt = (T)b;
-      w.pr[o] = rt;
-      w.px[o] = (T)0.0;
-      const double rr = (double)rt, dd = (double)dg;
-      const T z = (T)((fabs(dd) > 1e-20) ? rr / dd : rr);
-      w.pz[o] = z;
-      w.pp0[o] = z;
-      rc[5] += rr * (double)z;
-    }
-  });
-  if (!g.template sync_reduce<6, 0x1Fu>(rc, smem)) return -1;
-  out[0] = rc[0];
-  out[1] = rc[1];
-  out[2] = rc[2];
-  out[3] = rc[3];
-  out[6] = kU;
-  out[7] = kV;
-  // std::max({residU, residV, residMass}) (iterations.cpp:525); the stop test
-  // uses the mass imbalance over the pressure unknowns.
-  double e = out[0];
-  if (e < out[1]) e = out[1];
-  if (e < out[2]) e = out[2];
-  out[4] = e;
-  const double conv = maxd(maxd(out[0], out[1]), out[3]);
-  // The max reductions drop NaN the way std::max does, so non-finite values
-  // are flagged explicitly.
-  const bool finite = isfinite(e) && isfinite(out[3]) && rc[4] == 0.0;
-  if (!finite && g.rank == 0 && threadIdx.x == 0 && g.status) atomicCAS(g.status, kStatusOk, kStatusDiverged);
-  const bool stop = lastIter || !finite || (stopOnConv && conv <= eps);
-  // ---- P: Jacobi-preconditioned CG ----
-  double rz = rc[5], beta = 0.0;
+  double rz = rz0, beta = 0.0;
   int it = 0;
   for (; it < d.maxPIter; ++it) {
     const T* pold = (it & 1) ? w.pp0 : w.pp1;  // p_{it-1}
     T* pcur = (it & 1) ? w.pp1 : w.pp0;        // p_it
     const int k = it;
     const double bt = beta;
-    double s1[1] = {0.0};
+    double s1[1] = {pAp0};  // iteration 0's A p and p.Ap come from phase C
+    if (k > 0) {
+    s1[0] = 0.0;
     for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
       if (j > N - 2) return;
       const size_t o = (size_t)i * P + j;
@@ -626,6 +527,7 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, doub
       s1[0] += pc0 * (double)apt;
     });
     if (!g.template sync_reduce<1, 0u>(s1, smem)) return -1;
+    }
     const double pAp = s1[0];
     if (fabs(pAp) < 1e-20) break;
     const double alpha = rz / pAp;
@@ -649,8 +551,118 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, doub
     rz = s2[1];
     beta = rz / rzPrev;
   }
-  out[5] = it;
-  // ---- D: pressure and velocity correction ----
+  return it;
+}
+
+// ---------------------------------------------------------------------------
+// Single-reduction Jacobi-PCG (Chronopoulos-Gear recurrences), selected per
+// design by pcgSingleReduction: the same Krylov iterates as the reference's PCG in exact
+// arithmetic, with one grid-wide reduction per iteration instead of two.
+//   u0 = M^-1 r0, w0 = A u0, gamma0 = (r0,u0), delta0 = (w0,u0), alpha0 = gamma0/delta0
+//   iteration k: p_k = u_k + beta_k p_{k-1};  s_k = w_k + beta_k s_{k-1}  (= A p_k)
+//                x += alpha_k p_k;  r_{k+1} = r_k - alpha_k s_k;  u_{k+1} = M^-1 r_{k+1}
+//                w_{k+1} = A u_{k+1};  |r_{k+1}|^2, gamma_{k+1}, delta_{k+1}  (one reduction)
+//                beta_{k+1} = gamma_{k+1}/gamma_k
+//                alpha_{k+1} = gamma_{k+1} / (delta_{k+1} - beta_{k+1} gamma_{k+1} / alpha_k)
+// The neighbours' s_k, r_{k+1}, u_{k+1} needed by w_{k+1} = A u_{k+1} are
+// recomputed from the previous iteration's planes, so each iteration is one
+// phase.  Stop rules and counter as the reference (pressure_solver.cpp:152-182):
+// ||r_{k+1}|| < pTol stops with count k; the (p, Ap) < 1e-20 test of iteration
+// k+1 is the denominator of alpha_{k+1} and stops with count k+1.
+// Plane use: x = px, r = pr/pz, s = pp0/pp1, w = pAp/cU[0], u = cU[1],
+// p = cU[2]; the momentum coefficient planes are free after phase C.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T* cg1_u(const Inner<T>& w, long long ps) { return w.cU + ps; }
+
+template <typename T, class Group>
+__device__ int pcg_single_reduction(const DesignView& d, Group& g, double* smem, double gamma0, double delta0) {
+  const Inner<T>& w = inner<T>(d);
+  const int M = d.M, N = d.N, P = d.P;
+  const long long ps = d.planeStride;
+  T* const rb[2] = {w.pr, w.pz};
+  T* const sb[2] = {w.pp0, w.pp1};
+  T* const wb[2] = {w.pAp, w.cU};
+  T* const ub = w.cU + ps;
+  T* const pb = w.cU + 2 * ps;
+  if (d.maxPIter <= 0) return 0;
+  auto inv_diag = [&](size_t q, double r) -> double {
+    const double dg = (double)w.pdiag[q];
+    return (fabs(dg) > 1e-20) ? r / dg : r;
+  };
+  // w0 = A u0 and delta0 = (w0, u0) come from phase C
+  double gam = gamma0;
+  double denom = delta0;
+  if (fabs(denom) < 1e-20) return 0;
+  double alpha = gam / denom, beta = 0.0;
+  int k = 0;
+  for (; k < d.maxPIter; ++k) {
+    const T* rin = rb[k & 1];
+    T* rout = rb[(k + 1) & 1];
+    const T* sin = sb[(k + 1) & 1];  // s_{k-1}
+    T* sout = sb[k & 1];             // s_k
+    const T* win = wb[k & 1];        // w_k
+    T* wout = wb[(k + 1) & 1];       // w_{k+1}
+    const double a = alpha, bt = beta;
+    const bool first = (k == 0);
+    double red[3] = {0.0, 0.0, 0.0};  // |r|^2, gamma, delta
+    for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
+      if (j > N - 2) return;
+      const size_t o = (size_t)i * P + j;
+      // s_k, r_{k+1}, u_{k+1} at q (identical arithmetic at the owner and its neighbours)
+      auto s_at = [&](size_t q) -> T {
+        return first ? win[q] : (T)((double)win[q] + bt * (double)sin[q]);
+      };
+      auto r_at = [&](size_t q, T sq) -> T { return (T)((double)rin[q] - a * (double)sq); };
+      auto u_at = [&](size_t q) -> double {
+        const T rq = r_at(q, s_at(q));
+        return (double)(T)inv_diag(q, (double)rq);
+      };
+      const T sc = s_at(o);
+      const T rc = r_at(o, sc);
+      const double uc = (double)(T)inv_diag(o, (double)rc);
+      const T pk = first ? ub[o] : (T)((double)ub[o] + bt * (double)pb[o]);
+      w.px[o] = (T)((double)w.px[o] + a * (double)pk);
+      double Au = 0.0;
+      if (i > 1) Au += -(double)w.cy[o - P] * u_at(o - P);
+      if (j > 1) Au += -(double)w.cx[o - 1] * u_at(o - 1);
+      Au += (double)w.pdiag[o] * uc;
+      if (j + 1 <= N - 2) Au += -(double)w.cx[o] * u_at(o + 1);
+      if (i < M - 1) Au += -(double)w.cy[o] * u_at(o + P);
+      const T wt = (T)Au;
+      pb[o] = pk;
+      sout[o] = sc;
+      rout[o] = rc;
+      ub[o] = (T)uc;
+      wout[o] = wt;
+      const double rr = (double)rc;
+      red[0] += rr * rr;
+      red[1] += rr * uc;
+      red[2] += (double)wt * uc;
+    });
+    if (!g.template sync_reduce<3, 0u>(red, smem)) return -1;
+    if (sqrt(red[0]) < d.pTol) break;
+    if (k + 1 >= d.maxPIter) { k = d.maxPIter; break; }
+    const double gNew = red[1];
+    const double bNew = gNew / gam;
+    denom = red[2] - bNew * gNew / alpha;
+    if (fabs(denom) < 1e-20) { ++k; break; }
+    alpha = gNew / denom;
+    beta = bNew;
+    gam = gNew;
+  }
+  return k;
+}
+
+// ---------------------------------------------------------------------------
+// Phase D: p' scatter with the outlet column p' = 0 (pressure_solver.cpp:
+// 796-805), p += pAlpha p' and pressure BCs (iterations.cpp:456-467,
+// boundaries.cpp:111-134), velocity correction and BCs (iterations.cpp:473-499).
+// ---------------------------------------------------------------------------
+template <typename T, class Group>
+__device__ void correct_fields(const DesignView& d, Group& g) {
+  const Inner<T>& w = inner<T>(d);
+  const int M = d.M, N = d.N, P = d.P;
   for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
     const size_t o = (size_t)i * P + j;
     const double pcv = (j == N - 1) ? 0.0 : (double)w.px[o];
@@ -698,6 +710,170 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, doub
       d.v[o - 1] = 0.0;
     }
   });
+}
+
+// ---------------------------------------------------------------------------
+// One outer iteration for one design on group g; out[8] receives the step
+// diagnostics.  Returns 0 to continue with another outer iteration, 1 when
+// this one is the last (iteration budget, convergence, or a non-finite
+// residual), -1 when the group must stop because a device-side wait failed.
+// ---------------------------------------------------------------------------
+template <typename T, class Group>
+__device__ int outer_iteration(const DesignView& d, Group& g, double* smem, double (&out)[8], bool lastIter,
+                               bool stopOnConv, double eps) {
+  const Inner<T>& w = inner<T>(d);
+  const int M = d.M, N = d.N, P = d.P;
+  // ---- A: assembly + sweep 1 ----
+  const bool anySweep = d.maxMomIter > 0;
+  double red2[2] = {0.0, 0.0};
+  for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
+    if (j <= N - 2) red2[0] += assemble_point<true, T>(d, i, j, anySweep);
+    if (i <= M - 2) red2[1] += assemble_point<false, T>(d, i, j, anySweep);
+  });
+  if (!g.template sync_reduce<2, 0u>(red2, smem)) return -1;
+  int kU = anySweep ? 1 : 0, kV = kU;
+  bool actU = anySweep && !(red2[0] < d.thrU) && kU < d.maxMomIter;
+  bool actV = anySweep && !(red2[1] < d.thrV) && kV < d.maxMomIter;
+  // ---- B: sweeps 2.. ----
+  while (actU || actV) {
+    const int k = (actU ? kU : kV) + 1;  // both active components are at the same sweep
+    const T* xinU = (k & 1) ? w.xU0 : w.xU1;
+    T* xoutU = (k & 1) ? w.xU1 : w.xU0;
+    const T* xinV = (k & 1) ? w.xV0 : w.xV1;
+    T* xoutV = (k & 1) ? w.xV1 : w.xV0;
+    double s[2] = {0.0, 0.0};
+    const bool au = actU, av = actV;
+    for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
+      if (au && j <= N - 2) s[0] += sweep_point<true, T>(d, i, j, xinU, xoutU);
+      if (av && i <= M - 2) s[1] += sweep_point<false, T>(d, i, j, xinV, xoutV);
+    });
+    if (!g.template sync_reduce<2, 0u>(s, smem)) return -1;
+    if (au) { kU = k; actU = !(s[0] < d.thrU) && kU < d.maxMomIter; }
+    if (av) { kV = k; actV = !(s[1] < d.thrV) && kV < d.maxMomIter; }
+  }
+  const T* xfU = (kU & 1) ? w.xU1 : w.xU0;
+  const T* xfV = (kV & 1) ? w.xV1 : w.xV0;
+  // ---- C: scatter, BCs, mass residual, PCG set-up ----
+  // residU, residV, residMass, residMassDof, non-finite flag (max); r.z, p.Ap (sum)
+  double rc[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  // Mass imbalance b and pressure diagonal of any P-cell, evaluated exactly as
+  // below for the cell's own thread, so that z0 = b/diag of the four
+  // neighbours -- and with it the first PCG product A z0 -- is formed here
+  // instead of in a phase of its own.
+  auto mass_b = [&](int ii, int jj) -> double {
+    const double mE = d.rho * ustar_at<T>(d, xfU, ii, jj) * d.hy;
+    const double mW = d.rho * ustar_at<T>(d, xfU, ii, jj - 1) * d.hy;
+    const double mN = d.rho * vstar_at<T>(d, xfV, ii, jj) * d.hx;
+    const double mS = d.rho * vstar_at<T>(d, xfV, ii - 1, jj) * d.hx;
+    return mW - mE + mS - mN;
+  };
+  auto p_diag = [&](int ii, int jj) -> double {
+    const double aE = (jj < N - 1) ? d.rho * AT(d.dE, ii, jj) * d.hy : 0.0;
+    const double aW = (jj > 1) ? d.rho * AT(d.dE, ii, jj - 1) * d.hy : 0.0;
+    const double aN = (ii < M - 1) ? d.rho * AT(d.dN, ii, jj) * d.hx : 0.0;
+    const double aS = (ii > 1) ? d.rho * AT(d.dN, ii - 1, jj) * d.hx : 0.0;
+    double aP = aE + aW + aN + aS;
+    if (aP < 1e-20) aP = 1.0;
+    return aP;
+  };
+  auto z0_at = [&](int ii, int jj) -> double {
+    const double rr = (double)(T)mass_b(ii, jj), dd = (double)(T)p_diag(ii, jj);
+    return (double)(T)((fabs(dd) > 1e-20) ? rr / dd : rr);
+  };
+  for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
+    const size_t o = (size_t)i * P + j;
+    if (j <= N - 2) {
+      const double val = clampd(final_velocity<T>(d.u, xfU, o), -d.maxVel, d.maxVel);
+      d.us[o] = val;
+      rc[0] = maxd(rc[0], fabs(val - d.u[o]));
+      if (!isfinite(val)) rc[4] = 1.0;
+      if (j == N - 2) d.us[o + 1] = val;
+    }
+    if (j == 1) d.us[o - 1] = ustar_at<T>(d, xfU, i, 0);
+    if (i <= M - 2) {
+      const double val = clampd(final_velocity<T>(d.v, xfV, o), -d.maxVel, d.maxVel);
+      d.vs[o] = val;
+      rc[1] = maxd(rc[1], fabs(val - d.v[o]));
+      if (!isfinite(val)) rc[4] = 1.0;
+      if (j == N - 1) d.vs[o + 1] = val;
+    }
+    const double massE = d.rho * ustar_at<T>(d, xfU, i, j) * d.hy;
+    const double massW = d.rho * ustar_at<T>(d, xfU, i, j - 1) * d.hy;
+    const double massN = d.rho * vstar_at<T>(d, xfV, i, j) * d.hx;
+    const double massS = d.rho * vstar_at<T>(d, xfV, i - 1, j) * d.hx;
+    const double b = massW - massE + massS - massN;
+    const double ab = fabs(b);
+    if (!isfinite(ab)) rc[4] = 1.0;
+    if (ab > rc[2]) rc[2] = ab;
+    if (j <= N - 2) {
+      if (ab > rc[3]) rc[3] = ab;
+      // pressure_solver.cpp:698-703
+      const double aE = (j < N - 1) ? d.rho * AT(d.dE, i, j) * d.hy : 0.0;
+      const double aW = (j > 1) ? d.rho * AT(d.dE, i, j - 1) * d.hy : 0.0;
+      const double aN = (i < M - 1) ? d.rho * AT(d.dN, i, j) * d.hx : 0.0;
+      const double aS = (i > 1) ? d.rho * AT(d.dN, i - 1, j) * d.hx : 0.0;
+      double aP = aE + aW + aN + aS;
+      if (aP < 1e-20) aP = 1.0;
+      const T dg = (T)aP;
+      w.pdiag[o] = dg;
+      w.cx[o] = (T)aE;
+      w.cy[o] = (T)aN;
+      const T rt = (T)b;
+      w.pr[o] = rt;
+      w.px[o] = (T)0.0;
+      const double rr = (double)rt, dd = (double)dg;
+      const T z = (T)((fabs(dd) > 1e-20) ? rr / dd : rr);
+      if (d.pcgSingleReduction) {
+        cg1_u(w, d.planeStride)[o] = z;  // u0 = M^-1 r0 of the single-reduction recurrences
+      } else {
+        w.pz[o] = z;
+        w.pp0[o] = z;
+      }
+      rc[5] += rr * (double)z;
+      // first PCG product: A p0 with p0 = z0 (pressure_solver.cpp:153-156), in CSR order S, W, P, E, N
+      const double zc = (double)z;
+      double Ap = 0.0;
+      if (i > 1) Ap += -(double)(T)aS * z0_at(i - 1, j);
+      if (j > 1) Ap += -(double)(T)aW * z0_at(i, j - 1);
+      Ap += (double)dg * zc;
+      if (j + 1 <= N - 2) Ap += -(double)(T)aE * z0_at(i, j + 1);
+      if (i < M - 1) Ap += -(double)(T)aN * z0_at(i + 1, j);
+      const T apt = (T)Ap;
+      w.pAp[o] = apt;  // FP64: A p0; mixed: w0 = A u0 (the same plane)
+      rc[6] += zc * (double)apt;
+    }
+  });
+  if (!g.template sync_reduce<7, 0x1Fu>(rc, smem)) return -1;
+  out[0] = rc[0];
+  out[1] = rc[1];
+  out[2] = rc[2];
+  out[3] = rc[3];
+  out[6] = kU;
+  out[7] = kV;
+  // std::max({residU, residV, residMass}) (iterations.cpp:525); the stop test
+  // uses the mass imbalance over the pressure unknowns.
+  double e = out[0];
+  if (e < out[1]) e = out[1];
+  if (e < out[2]) e = out[2];
+  out[4] = e;
+  const double conv = maxd(maxd(out[0], out[1]), out[3]);
+  // The max reductions drop NaN the way std::max does, so non-finite values
+  // are flagged explicitly.
+  const bool finite = isfinite(e) && isfinite(out[3]) && rc[4] == 0.0;
+  if (!finite && g.rank == 0 && threadIdx.x == 0 && g.status) atomicCAS(g.status, kStatusOk, kStatusDiverged);
+  const bool stop = lastIter || !finite || (stopOnConv && conv <= eps);
+  // ---- P: Jacobi-preconditioned CG ----
+  if (d.pcgSingleReduction) {
+    const int its = pcg_single_reduction<T>(d, g, smem, rc[5], rc[6]);
+    if (its < 0) return -1;
+    out[5] = its;
+  } else {
+    const int its = pcg_two_reductions<T>(d, g, smem, rc[5], rc[6]);
+    if (its < 0) return -1;
+    out[5] = its;
+  }
+  // ---- D: pressure and velocity correction ----
+  correct_fields<T>(d, g);
   if (!stop) return g.sync() ? 0 : -1;
   return 1;
 }

@@ -70,7 +70,13 @@ typedef struct {
   int layout;                     /* CPS_ROW_MAJOR or CPS_COL_MAJOR for alpha/gamma */
   int device;                     /* CUDA device ordinal */
   int grid_ctas;                  /* CTAs of the persistent kernel; 0 = automatic */
+  int pcg_variant;                /* CPS_PCG_REFERENCE (two reductions per iteration, as
+                                     pressure_solver.cpp:121-184) or CPS_PCG_SINGLE_REDUCTION
+                                     (Chronopoulos-Gear recurrences: one reduction per iteration) */
 } cps_desc;
+
+/* PCG recurrences (same Krylov iterates in exact arithmetic). */
+enum { CPS_PCG_REFERENCE = 0, CPS_PCG_SINGLE_REDUCTION = 1 };
 
 /* Per-step inputs (SIMPLE.h:344 inletVelocity; SIMPLE.cpp:303-307). */
 typedef struct {
@@ -152,6 +158,8 @@ typedef struct {
   int max_outer;      /* outer-iteration budget of every design in this call */
   double eps;         /* stop a design once max(residU, residV, residMassDof) <= eps (0 = never) */
   int order_by_size;  /* start the largest designs first */
+  int group_ctas;     /* > 0: run designs on groups of this many CTAs of one cooperative launch (software
+                         group barrier, bounded waits) instead of on thread-block clusters */
 } cps_batch_opts;
 
 /* Per-design outcome of a batched solve. */
@@ -163,9 +171,10 @@ typedef struct {
 } cps_batch_result;
 
 /* Many designs in one persistent launch: each design runs on one thread-block
- * cluster (hardware cluster barrier, no host round trips) until it meets eps
- * or spends max_outer outer iterations; clusters take designs from a device
- * work queue, so designs of uneven size share the GPU.  Every context must be
+ * cluster (hardware cluster barrier) or, with group_ctas > 0, on one group of
+ * CTAs of a cooperative launch (software group barrier), until it meets eps
+ * or spends max_outer outer iterations; clusters/groups take designs from a
+ * device work queue, so designs of uneven size share the GPU.  Every context must be
  * on the same device with the same precision.  Has no reference counterpart:
  * the reference solves one design per process (SIMPLE.cpp:638-642).
  * inletVelocity: n values or NULL to keep each context's last value.
@@ -189,7 +198,8 @@ cps_status cps_get_history(cps_ctx* ctx, int n, cps_step_out* history);
  * `stream` (a cudaStream_t; NULL = default stream), stopping when
  * max(residU, residV, residMassDof) <= eps (eps > 0); history (host, may be
  * NULL) and *n_done as for cps_solve; desc's alpha/gamma/layout/device/
- * grid_ctas are ignored and precision must be CPS_FP64.
+ * grid_ctas/pcg_variant are ignored (the reference's PCG is used) and
+ * precision must be CPS_FP64.
  *
  * All scratch lives in one static device array of about 27 MB per GPU, held
  * until the process exits; designs need (M+1)*pitch <= 131072 elements or are

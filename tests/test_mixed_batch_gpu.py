@@ -3,10 +3,13 @@
 FP64 path.
 
 Tolerances: a mixed-precision outer iteration applies FP32 corrections to FP64
-fields.  Its later Jacobi sweeps test the RMS stop rule on FP32-stored values,
-so a sweep can stop one sweep before or after the FP64 one; from an identical
-state its fields therefore agree with the FP64 step to REL_MIXED_STEP = 1e-4
-relative L2 (one Jacobi update of a stiff Brinkman field is ~4e-5).  At
+fields.  Its inner solves are inexact by design (Jacobi RMS 1e-5, PCG
+||r|| < 1e-4) and test their stop rules on FP32-stored values, so they stop
+at slightly different iterates than the FP64 ones (a Jacobi sweep earlier or
+later, a PCG residual at the tolerance instead of below it); from an
+identical state the fields therefore agree with the FP64 step only to the
+inner tolerances: REL_MIXED_STEP = 1e-3 relative L2 (observed 4e-5 to 1.5e-4
+on stiff Brinkman fields).  At
 convergence both sit on the same FP64 fixed point (REL_FIELD = 1e-6,
 REL_DP = 1e-5, as for the FP64 path).  A
 batched design differs from the same design solved alone on the whole grid
@@ -20,7 +23,7 @@ from coldplate_solver_b200 import cps, geometry
 
 pytestmark = pytest.mark.gpu
 
-REL_MIXED_STEP = 1e-4
+REL_MIXED_STEP = 1e-3
 REL_STEP = 1e-10
 REL_FIELD = 1e-6
 REL_DP = 1e-5
@@ -91,8 +94,9 @@ def uneven_designs():
             geometry.channel_network(M=40, N=90, h=20e-6, wmin=3, wmax=6, seed=9)]
 
 
-@pytest.mark.parametrize("cluster", [1, 4, 8, 16])
-def test_batch_matches_solo_solves(cluster):
+@pytest.mark.parametrize("mode,size", [("cluster", 1), ("cluster", 4), ("cluster", 8), ("cluster", 16),
+                                       ("group", 3), ("group", 37), ("group", 74)])
+def test_batch_matches_solo_solves(mode, size):
     designs = uneven_designs()
     n = 7
     solo = []
@@ -102,7 +106,10 @@ def test_batch_matches_solo_solves(cluster):
             solo.append((h, s.download()))
     solvers = [cps.Solver(d) for d in designs]
     try:
-        res, ms = cps.batch_solve(solvers, n, eps=0.0, cluster_ctas=cluster)
+        if mode == "cluster":
+            res, ms = cps.batch_solve(solvers, n, eps=0.0, cluster_ctas=size)
+        else:
+            res, ms = cps.batch_solve(solvers, n, eps=0.0, group_ctas=size)
         assert ms > 0
         for k, s in enumerate(solvers):
             assert res[k]["n_done"] == n and res[k]["status"] == 0
@@ -118,15 +125,16 @@ def test_batch_matches_solo_solves(cluster):
             s.close()
 
 
-def test_batch_result_is_the_same_alone_and_in_the_mix():
+@pytest.mark.parametrize("kw", [{"cluster_ctas": 8}, {"group_ctas": 37}])
+def test_batch_result_is_the_same_alone_and_in_the_mix(kw):
     designs = uneven_designs()
     target = 2
     with cps.Solver(designs[target]) as alone:
-        cps.batch_solve([alone], 9, eps=0.0, cluster_ctas=8)
+        cps.batch_solve([alone], 9, eps=0.0, **kw)
         fa = alone.download()
     solvers = [cps.Solver(d) for d in designs]
     try:
-        cps.batch_solve(solvers, 9, eps=0.0, cluster_ctas=8)
+        cps.batch_solve(solvers, 9, eps=0.0, **kw)
         fm = solvers[target].download()
     finally:
         for s in solvers:
@@ -154,11 +162,12 @@ def test_batch_stops_each_design_at_convergence():
         assert abs(r["n_done"] - solo_iters[k]) <= max(3, solo_iters[k] // 5), (r["n_done"], solo_iters[k])
 
 
-def test_batch_mixed_precision_runs():
+@pytest.mark.parametrize("kw", [{"cluster_ctas": 8}, {"group_ctas": 16}])
+def test_batch_mixed_precision_runs(kw):
     designs = uneven_designs()[:4]
     solvers = [cps.Solver(d, precision=cps.CPS_MIXED) for d in designs]
     try:
-        res, _ = cps.batch_solve(solvers, 5, eps=0.0, cluster_ctas=8)
+        res, _ = cps.batch_solve(solvers, 5, eps=0.0, **kw)
         for s, r in zip(solvers, res):
             assert r["n_done"] == 5 and r["status"] == 0
             assert np.isfinite(s.download()["u"]).all()
@@ -177,3 +186,37 @@ def test_batch_rejects_mixed_precisions():
     finally:
         a.close()
         b.close()
+
+
+@pytest.mark.parametrize("which", ["straight", "network"])
+def test_single_reduction_pcg_fp64_tracks_the_reference_pcg(which):
+    """The single-reduction recurrences produce the reference PCG's iterates in
+    exact arithmetic; in FP64 one outer iteration from an identical state stays
+    within 1e-8 of the oracle (only rounding of the carried vectors differs)."""
+    from oracle import restatement as rs
+    d = {"straight": geometry.straight_channel(M=40, N=70, band=(10, 30)),
+         "network": geometry.channel_network(M=60, N=120, h=20e-6, wmin=4, wmax=8, seed=2)}[which]
+    init = random_state(d, 5)
+    with cps.Solver(d, pcg_variant=cps.CPS_PCG_SINGLE_REDUCTION) as s:
+        s.upload_fields(init["u"], init["v"], init["p"])
+        h = s.solve(1, eps=0.0)
+        f = s.download()
+    fr = rs.new_fields(d)
+    for k in ("u", "v", "p"):
+        fr[k][...] = init[k]
+    hr = rs.solve(d, fr, 1, stop_on_conv=False)
+    assert h[0, 5] == hr[0, 5]
+    for k in FIELDS:
+        assert rel(f[k], fr[k]) <= 1e-8, (k, rel(f[k], fr[k]))
+
+
+def test_single_reduction_pcg_converges_to_the_same_fixed_point():
+    d = geometry.straight_channel()
+    with cps.Solver(d) as a, cps.Solver(d, pcg_variant=cps.CPS_PCG_SINGLE_REDUCTION) as b:
+        a.solve(100000, eps=1e-10)
+        b.solve(100000, eps=1e-10)
+        fa, fb = a.download(), b.download()
+        dpa, dpb = a.full_dp(), b.full_dp()
+    for k in ("u", "v"):
+        assert rel(fb[k], fa[k]) <= REL_FIELD, (k, rel(fb[k], fa[k]))
+    assert abs(dpb - dpa) <= REL_DP * abs(dpa)

@@ -68,6 +68,6 @@ def test_latency_statistics():
 def test_autotuner_picks_a_candidate_and_batch_solves():
     designs = [geometry.density_field(Nx=nx, seed=nx, sigma=3.0) for nx in (48, 64, 80, 96)]
     t = batch.autotune(designs, sample=4, visit=10, use_cache=False)
-    assert t.cluster_ctas in batch.CLUSTER_CANDIDATES and all(v > 0 for v in t.cell_updates_per_s.values())
-    res, ms = batch.solve_batch(designs, eps=1e-6, max_outer=40000, cluster_ctas=t.cluster_ctas, visit=500)
+    assert t.mode in batch.mode_candidates() and all(v > 0 for v in t.cell_updates_per_s.values())
+    res, ms = batch.solve_batch(designs, eps=1e-6, max_outer=40000, mode=t.mode, visit=500)
     assert all(r["converged"] for r in res) and ms > 0
