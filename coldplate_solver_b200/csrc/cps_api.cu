@@ -73,7 +73,7 @@ struct cps_ctx {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(cps::kThreads, 2) cps_grid_kernel(cps::DesignView d, cps::RunControl rc,
+__global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_grid_kernel(cps::DesignView d, cps::RunControl rc,
                                                                 cps::GridBarrier* bar, double* red) {
   __shared__ double smem[cps::kRedWidth * 8];
   cps::GridGroup g{bar, red, rc.status, blockIdx.x, gridDim.x, 0u, 0ull};
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(cps::kThreads) cps_cluster_kernel(const cps::B
 // The group count sets how many designs are in flight (and so the in-flight
 // working set against the 126 MB L2); K sets how many CTAs share one design.
 template <typename T>
-__global__ void __launch_bounds__(cps::kThreads, 2) cps_group_kernel(const cps::BatchItem* __restrict__ items,
+__global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_group_kernel(const cps::BatchItem* __restrict__ items,
                                                                     const int* __restrict__ order, int n_items,
                                                                     int* queue, cps::BatchResult* results,
                                                                     cps::GridBarrier* bars, double* rings,

@@ -60,6 +60,22 @@ constexpr int kTileI = 8;       // tile rows (one warp per row)
 constexpr int kTileJ = 32;      // tile columns (one lane per column)
 constexpr int kRedWidth = 8;    // doubles per CTA per reduction
 constexpr int kRedSlots = 4;    // ring of reduction slots (grid group)
+// CTAs per SM the persistent kernels are compiled for (128 registers per
+// thread at 2), and tiles per round of the staged phases P1, P2 and D.  More
+// than one tile per round overlaps the tiles' load latencies but spills at
+// 128 registers; one per round measured fastest on B200.
+#ifndef CPS_MIN_BLOCKS
+#define CPS_MIN_BLOCKS 2
+#endif
+#ifndef CPS_U_P1
+#define CPS_U_P1 1
+#endif
+#ifndef CPS_U_P2
+#define CPS_U_P2 1
+#endif
+#ifndef CPS_U_D
+#define CPS_U_D 1
+#endif
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
 
 enum DeviceStatus : int { kStatusOk = 0, kStatusTimeout = 1, kStatusDiverged = 2 };
@@ -205,58 +221,104 @@ struct GridGroup {
     __shared__ int s_ok;
     __syncthreads();
     ++epoch;
-    if (threadIdx.x == 0) {
-      int ok = 1;
-      const unsigned long long target = epoch * nblk;
-      const unsigned long long old = atom_add_acq_rel_u64(&bar->count, 1ull);
-      if (old + 1 < target) {
-        const unsigned long long t0 = globaltimer_ns();
-        unsigned spins = 0;
-        while (ld_acquire_u64(&bar->count) < target) {
-          if ((++spins & 255u) == 0) {
-            if (*(volatile int*)status != kStatusOk) { ok = 0; break; }
-            if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
-              atomicCAS(status, kStatusOk, kStatusTimeout);
-              ok = 0;
-              break;
-            }
-          }
-        }
-      }
-      s_ok = ok;
-    }
+    if (threadIdx.x == 0) s_ok = arrive_and_wait();
     __syncthreads();
     return s_ok != 0;
   }
 
+  // Thread 0 only: arrive at barrier number `epoch` and wait for the others.
+  __device__ int arrive_and_wait() {
+    const unsigned long long target = epoch * nblk;
+    const unsigned long long old = atom_add_acq_rel_u64(&bar->count, 1ull);
+    if (old + 1 >= target) return 1;
+    const unsigned long long t0 = globaltimer_ns();
+    unsigned spins = 0;
+    while (ld_acquire_u64(&bar->count) < target) {
+      if ((++spins & 255u) == 0) {
+        if (*(volatile int*)status != kStatusOk) return 0;
+        if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
+          atomicCAS(status, kStatusOk, kStatusTimeout);
+          return 0;
+        }
+      }
+    }
+    return 1;
+  }
+
   // Publish this CTA's K values, synchronise, and combine all CTAs' values in
-  // CTA order.  Result valid in every thread of every CTA.
+  // a fixed order.  Result valid in every thread of every CTA.
+  //   CTA value: warp trees (shfl_xor), then the 8 warps in order.
+  //   Grid value: lane l of warp 0 folds CTAs l, l+32, ... in order, then a
+  //   warp tree.  The ring holds value k of CTA b at [k * nblk + b].
+  // Two __syncthreads per reduction: the first orders every thread's tile
+  // writes before thread 0's release (cumulativity) and hands the warp values
+  // to thread 0; the second hands the result (and thread 0's acquire, through
+  // __syncwarp in warp 0) to the whole CTA.
   template <int K, unsigned MaxMask>
   __device__ bool sync_reduce(double (&v)[K], double* smem) {
-    block_reduce<K, MaxMask>(v, smem);
+    __shared__ double s_res[kRedWidth];
+    __shared__ int s_ok;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double o = __shfl_xor_sync(0xffffffffu, v[k], off);
+        v[k] = ((MaxMask >> k) & 1u) ? maxd(v[k], o) : v[k] + o;
+      }
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int k = 0; k < K; ++k) smem[k * 8 + warp] = v[k];
+    }
     double* slot = red + (size_t)(redCount % kRedSlots) * nblk * kRedWidth;
     ++redCount;
-    if (threadIdx.x == 0) {
+    ++epoch;
+    __syncthreads();
+    if (warp == 0) {
+      int ok = 1;
+      if (lane == 0) {
 #pragma unroll
-      for (int k = 0; k < K; ++k) slot[rank * kRedWidth + k] = v[k];
-    }
-    if (!sync()) return false;
-    double acc[K];
+        for (int k = 0; k < K; ++k) {
+          double a = smem[k * 8 + 0];
 #pragma unroll
-    for (int k = 0; k < K; ++k) acc[k] = 0.0;
-    bool first = true;
-    for (unsigned b = threadIdx.x; b < nblk; b += kThreads) {
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const double x = __ldcg(slot + b * kRedWidth + k);
-        acc[k] = first ? x : (((MaxMask >> k) & 1u) ? maxd(acc[k], x) : acc[k] + x);
+          for (int w = 1; w < 8; ++w) a = ((MaxMask >> k) & 1u) ? maxd(a, smem[k * 8 + w]) : a + smem[k * 8 + w];
+          slot[(size_t)k * nblk + rank] = a;
+        }
+        ok = arrive_and_wait();
       }
-      first = false;
-    }
-    block_reduce<K, MaxMask>(acc, smem);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      __syncwarp();
+      double acc[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) v[k] = acc[k];
-    return true;
+      for (int k = 0; k < K; ++k) acc[k] = 0.0;
+      if (ok) {
+        for (unsigned b = lane; b < nblk; b += 32) {
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            const double x = __ldcg(slot + (size_t)k * nblk + b);
+            acc[k] = ((MaxMask >> k) & 1u) ? maxd(acc[k], x) : acc[k] + x;
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) {
+            const double o = __shfl_xor_sync(0xffffffffu, acc[k], off);
+            acc[k] = ((MaxMask >> k) & 1u) ? maxd(acc[k], o) : acc[k] + o;
+          }
+        }
+      }
+      if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) s_res[k] = acc[k];
+        s_ok = ok;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = s_res[k];
+    return s_ok != 0;
   }
 };
 
@@ -487,12 +549,56 @@ __device__ __forceinline__ void for_each_point(const DesignView& d, unsigned ran
   }
 }
 
+// The same points in the same order, in rounds of U tiles: load(i, j) returns
+// everything a point reads and runs for all U tiles of a round before
+// body(i, j, loaded) runs for any of them, so the round's memory latencies
+// overlap instead of forming a chain through the stores.  Only for phases in
+// which no point reads what another point of the same phase writes.
+template <int U, class Load, class Body>
+__device__ __forceinline__ void for_each_point_staged(const DesignView& d, unsigned rank, unsigned nblk, Load&& load,
+                                                      Body&& body) {
+  const int tilesJ = (d.N - 1 + kTileJ - 1) / kTileJ;
+  const int tilesI = (d.M - 1 + kTileI - 1) / kTileI;
+  const int nt = tilesI * tilesJ;
+  const int ty = threadIdx.x >> 5, tx = threadIdx.x & 31;
+  using L = decltype(load(1, 1));
+  for (int t0 = rank; t0 < nt; t0 += U * (int)nblk) {
+    L buf[U];
+    int ii[U], jj[U];
+    bool on[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int t = t0 + u * (int)nblk;
+      ii[u] = 1 + (t / tilesJ) * kTileI + ty;
+      jj[u] = 1 + (t % tilesJ) * kTileJ + tx;
+      on[u] = t < nt && ii[u] <= d.M - 1 && jj[u] <= d.N - 1;
+      if (on[u]) buf[u] = load(ii[u], jj[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (on[u]) body(ii[u], jj[u], buf[u]);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // PCG as the reference runs it (pressure_solver.cpp:121-184): two grid-wide
 // reductions per iteration (p.Ap, then |r|^2 and r.z).  Phase P1 forms
 // p = z + beta p on the fly for the 5-point stencil and Ap; phase P2 updates
 // x, r, z.  Returns the reference's iteration count, or -1 if a wait failed.
 // ---------------------------------------------------------------------------
+// Values phase P1 reads at one unknown: z and p_{k-1} at the point and its
+// S, W, E, N neighbours (index 0..4), and the stencil row.
+template <typename T>
+struct P1In {
+  T z[5], po[5];
+  T cS, cW, dg, cE, cN;
+};
+// Values phase P2 reads at one unknown.
+template <typename T>
+struct P2In {
+  T x, p, r, ap, dg;
+};
+
 template <typename T, class Group>
 __device__ int pcg_two_reductions(const DesignView& d, Group& g, double* smem, double rz0, double pAp0) {
   const Inner<T>& w = inner<T>(d);
@@ -502,49 +608,74 @@ __device__ int pcg_two_reductions(const DesignView& d, Group& g, double* smem, d
   for (; it < d.maxPIter; ++it) {
     const T* pold = (it & 1) ? w.pp0 : w.pp1;  // p_{it-1}
     T* pcur = (it & 1) ? w.pp1 : w.pp0;        // p_it
-    const int k = it;
     const double bt = beta;
-    double s1[1] = {pAp0};  // iteration 0's A p and p.Ap come from phase C
-    if (k > 0) {
-    s1[0] = 0.0;
-    for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
-      if (j > N - 2) return;
-      const size_t o = (size_t)i * P + j;
-      // p_k at (i, j) and its unknown neighbours: p = z + beta p (pressure_solver.cpp:181)
-      auto pk = [&](size_t q) -> double {
-        return k == 0 ? (double)w.pp0[q] : (double)(T)((double)w.pz[q] + bt * (double)pold[q]);
-      };
-      const double pc0 = pk(o);
-      double Ap = 0.0;
-      if (i > 1) Ap += -(double)w.cy[o - P] * pk(o - P);
-      if (j > 1) Ap += -(double)w.cx[o - 1] * pk(o - 1);
-      Ap += (double)w.pdiag[o] * pc0;
-      if (j + 1 <= N - 2) Ap += -(double)w.cx[o] * pk(o + 1);
-      if (i < M - 1) Ap += -(double)w.cy[o] * pk(o + P);
-      if (k > 0) pcur[o] = (T)pc0;
-      const T apt = (T)Ap;
-      w.pAp[o] = apt;
-      s1[0] += pc0 * (double)apt;
-    });
-    if (!g.template sync_reduce<1, 0u>(s1, smem)) return -1;
+    double s1[1] = {pAp0};  // iteration 0's p = z, A p and p.Ap come from phase C
+    if (it > 0) {
+      s1[0] = 0.0;
+      for_each_point_staged<CPS_U_P1>(
+          d, g.rank, g.nblk,
+          [&](int i, int j) {
+            P1In<T> a{};
+            if (j > N - 2) return a;
+            const size_t o = (size_t)i * P + j;
+            a.z[0] = w.pz[o];
+            a.po[0] = pold[o];
+            a.dg = w.pdiag[o];
+            if (i > 1) { a.z[1] = w.pz[o - P]; a.po[1] = pold[o - P]; a.cS = w.cy[o - P]; }
+            if (j > 1) { a.z[2] = w.pz[o - 1]; a.po[2] = pold[o - 1]; a.cW = w.cx[o - 1]; }
+            if (j + 1 <= N - 2) { a.z[3] = w.pz[o + 1]; a.po[3] = pold[o + 1]; a.cE = w.cx[o]; }
+            if (i < M - 1) { a.z[4] = w.pz[o + P]; a.po[4] = pold[o + P]; a.cN = w.cy[o]; }
+            return a;
+          },
+          [&](int i, int j, const P1In<T>& a) {
+            if (j > N - 2) return;
+            const size_t o = (size_t)i * P + j;
+            // p_k at (i, j) and its unknown neighbours: p = z + beta p (pressure_solver.cpp:181)
+            auto pk = [&](int q) -> double { return (double)(T)((double)a.z[q] + bt * (double)a.po[q]); };
+            const double pc0 = pk(0);
+            double Ap = 0.0;
+            if (i > 1) Ap += -(double)a.cS * pk(1);
+            if (j > 1) Ap += -(double)a.cW * pk(2);
+            Ap += (double)a.dg * pc0;
+            if (j + 1 <= N - 2) Ap += -(double)a.cE * pk(3);
+            if (i < M - 1) Ap += -(double)a.cN * pk(4);
+            pcur[o] = (T)pc0;
+            const T apt = (T)Ap;
+            w.pAp[o] = apt;
+            s1[0] += pc0 * (double)apt;
+          });
+      if (!g.template sync_reduce<1, 0u>(s1, smem)) return -1;
     }
     const double pAp = s1[0];
     if (fabs(pAp) < 1e-20) break;
     const double alpha = rz / pAp;
     double s2[2] = {0.0, 0.0};  // |r|^2, r.z
-    for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
-      if (j > N - 2) return;
-      const size_t o = (size_t)i * P + j;
-      w.px[o] = (T)((double)w.px[o] + alpha * (double)pcur[o]);
-      const T rt = (T)((double)w.pr[o] - alpha * (double)w.pAp[o]);
-      w.pr[o] = rt;
-      const double r = (double)rt;
-      s2[0] += r * r;
-      const double dg = (double)w.pdiag[o];
-      const T z = (T)((fabs(dg) > 1e-20) ? r / dg : r);
-      w.pz[o] = z;
-      s2[1] += r * (double)z;
-    });
+    for_each_point_staged<CPS_U_P2>(
+        d, g.rank, g.nblk,
+        [&](int i, int j) {
+          P2In<T> a{};
+          if (j > N - 2) return a;
+          const size_t o = (size_t)i * P + j;
+          a.x = w.px[o];
+          a.p = pcur[o];
+          a.r = w.pr[o];
+          a.ap = w.pAp[o];
+          a.dg = w.pdiag[o];
+          return a;
+        },
+        [&](int i, int j, const P2In<T>& a) {
+          if (j > N - 2) return;
+          const size_t o = (size_t)i * P + j;
+          w.px[o] = (T)((double)a.x + alpha * (double)a.p);
+          const T rt = (T)((double)a.r - alpha * (double)a.ap);
+          w.pr[o] = rt;
+          const double r = (double)rt;
+          s2[0] += r * r;
+          const double dg = (double)a.dg;
+          const T z = (T)((fabs(dg) > 1e-20) ? r / dg : r);
+          w.pz[o] = z;
+          s2[1] += r * (double)z;
+        });
     if (!g.template sync_reduce<2, 0u>(s2, smem)) return -1;
     if (sqrt(s2[0]) < d.pTol) break;
     const double rzPrev = rz;
@@ -659,15 +790,40 @@ __device__ int pcg_single_reduction(const DesignView& d, Group& g, double* smem,
 // 796-805), p += pAlpha p' and pressure BCs (iterations.cpp:456-467,
 // boundaries.cpp:111-134), velocity correction and BCs (iterations.cpp:473-499).
 // ---------------------------------------------------------------------------
+struct DIn {
+  double pc, pcE, pcN, p, dE, us, dN, vs, g0;
+};
+
 template <typename T, class Group>
 __device__ void correct_fields(const DesignView& d, Group& g) {
   const Inner<T>& w = inner<T>(d);
   const int M = d.M, N = d.N, P = d.P;
-  for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
+  // Reads: p' (own point, E and N), p, dE, u*, dN, v*, gamma of the inlet
+  // column; writes p', p, u, v and the boundary copies, none of which another
+  // point of this phase reads.
+  auto load = [&](int i, int j) {
+    DIn a{};
     const size_t o = (size_t)i * P + j;
-    const double pcv = (j == N - 1) ? 0.0 : (double)w.px[o];
+    a.pc = (j == N - 1) ? 0.0 : (double)w.px[o];
+    a.p = d.p[o];
+    if (j <= N - 2) {
+      a.pcE = (j + 1 == N - 1) ? 0.0 : (double)w.px[o + 1];
+      a.dE = d.dE[o];
+      a.us = d.us[o];
+    }
+    if (i <= M - 2) {
+      a.pcN = (j == N - 1) ? 0.0 : (double)w.px[o + P];
+      a.dN = d.dN[o];
+      a.vs = d.vs[o];
+    }
+    if (j == 1) a.g0 = AT(d.gamma, i - 1, 0);
+    return a;
+  };
+  for_each_point_staged<CPS_U_D>(d, g.rank, g.nblk, load, [&](int i, int j, const DIn& a) {
+    const size_t o = (size_t)i * P + j;
+    const double pcv = a.pc;
     d.pc[o] = pcv;
-    const double pn = d.p[o] + d.pAlpha * pcv;
+    const double pn = a.p + d.pAlpha * pcv;
     d.p[o] = pn;
     if (i == 1) d.p[o - P] = pn;
     if (i == M - 1) d.p[o + P] = pn;
@@ -675,19 +831,17 @@ __device__ void correct_fields(const DesignView& d, Group& g) {
     if (j == N - 1) d.p[o + 1] = 0.0;
     const double mv = d.maxVel;
     if (j <= N - 2) {
-      const double pcE = (j + 1 == N - 1) ? 0.0 : (double)w.px[o + 1];
-      double du = d.dE[o] * (pcv - pcE);
+      double du = a.dE * (pcv - a.pcE);
       du = maxd(-mv, mind(mv, du));
-      double un = d.us[o] + du;
+      double un = a.us + du;
       un = maxd(-mv, mind(mv, un));
       d.u[o] = un;
       if (j == N - 2) d.u[o + 1] = un;
     }
     if (i <= M - 2) {
-      const double pcN = (j == N - 1) ? 0.0 : (double)w.px[o + P];
-      double dv = d.dN[o] * (pcv - pcN);
+      double dv = a.dN * (pcv - a.pcN);
       dv = maxd(-mv, mind(mv, dv));
-      double vn = d.vs[o] + dv;
+      double vn = a.vs + dv;
       vn = maxd(-mv, mind(mv, vn));
       d.v[o] = vn;
       if (j == N - 1) d.v[o + 1] = vn;
@@ -706,7 +860,7 @@ __device__ void correct_fields(const DesignView& d, Group& g) {
       if (j == N - 1) d.v[o + 1] = 0.0;
     }
     if (j == 1) {
-      d.u[o - 1] = (AT(d.gamma, i - 1, 0) > 0.5) ? d.Uin : 0.0;
+      d.u[o - 1] = (a.g0 > 0.5) ? d.Uin : 0.0;
       d.v[o - 1] = 0.0;
     }
   });

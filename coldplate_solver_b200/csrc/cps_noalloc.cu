@@ -62,7 +62,7 @@ cps_status fail(cps_status s, const std::string& m) {
 
 }  // namespace
 
-__global__ void __launch_bounds__(cps::kThreads, 2) cps_noalloc_kernel(cps::DesignView d, cps::RunControl rc,
+__global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_noalloc_kernel(cps::DesignView d, cps::RunControl rc,
                                                                       cps::GridBarrier* bar, double* red) {
   __shared__ double smem[cps::kRedWidth * 8];
   cps::GridGroup g{bar, red, rc.status, blockIdx.x, gridDim.x, 0u, 0ull};
