@@ -76,10 +76,12 @@ template <typename T>
 __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_grid_kernel(cps::DesignView d, cps::RunControl rc,
                                                                 cps::GridBarrier* bar, double* red) {
   __shared__ double smem[cps::kRedWidth * 8];
+  extern __shared__ __align__(16) char tile_smem[];
   cps::GridGroup g{bar, red, rc.status, blockIdx.x, gridDim.x, 0u, 0ull};
   for (int it = 0; it < rc.n_outer; ++it) {
     double out[8];
-    const int r = cps::outer_iteration<T>(d, g, smem, out, it + 1 == rc.n_outer, rc.stop_on_conv != 0, rc.eps);
+    const int r = cps::outer_iteration<T>(d, g, smem, tile_smem, out, it + 1 == rc.n_outer, rc.stop_on_conv != 0,
+                                          rc.eps);
     if (r < 0) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       for (int k = 0; k < 8; ++k) rc.hist[(size_t)it * 8 + k] = out[k];
@@ -99,6 +101,7 @@ __global__ void __launch_bounds__(cps::kThreads) cps_cluster_kernel(const cps::B
   __shared__ double redbuf[2 * cps::kRedWidth];
   __shared__ __align__(16) cps::BatchItem s_item;
   __shared__ int s_next;
+  extern __shared__ __align__(16) char tile_smem[];
   cps::cg::cluster_group cl = cps::cg::this_cluster();
   cps::ClusterGroup g{redbuf, nullptr, cl.block_rank(), cl.num_blocks(), 0u};
   for (;;) {
@@ -119,7 +122,7 @@ __global__ void __launch_bounds__(cps::kThreads) cps_cluster_kernel(const cps::B
     double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int done = 0;
     for (int it = 0; it < item.n_outer; ++it) {
-      const int r = cps::outer_iteration<T>(item.view, g, smem, out, it + 1 == item.n_outer, item.stop_on_conv != 0,
+      const int r = cps::outer_iteration<T>(item.view, g, smem, tile_smem, out, it + 1 == item.n_outer, item.stop_on_conv != 0,
                                             item.eps);
       done = it + 1;
       if (g.rank == 0 && threadIdx.x == 0 && item.hist && it < item.hist_cap)
@@ -150,6 +153,7 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_group_kerne
                                                                     int* slots, int group_ctas) {
   __shared__ double smem[cps::kRedWidth * 8];
   __shared__ __align__(16) cps::BatchItem s_item;
+  extern __shared__ __align__(16) char tile_smem[];
   const unsigned grp = blockIdx.x / group_ctas;
   int* slot = slots + 2 * grp;  // [0] next queue index, [1] group status before a design is assigned
   cps::GridGroup g{bars + grp, rings + (size_t)grp * cps::kRedSlots * group_ctas * cps::kRedWidth, slot + 1,
@@ -174,7 +178,7 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_group_kerne
     double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int done = 0;
     for (int it = 0; it < item.n_outer; ++it) {
-      const int r = cps::outer_iteration<T>(item.view, g, smem, out, it + 1 == item.n_outer, item.stop_on_conv != 0,
+      const int r = cps::outer_iteration<T>(item.view, g, smem, tile_smem, out, it + 1 == item.n_outer, item.stop_on_conv != 0,
                                             item.eps);
       if (r < 0) return;  // a bounded wait expired; the design's status says so
       done = it + 1;
@@ -345,6 +349,16 @@ const void* grid_kernel_for(int precision) {
   return precision == CPS_MIXED ? (const void*)cps_grid_kernel<float> : (const void*)cps_grid_kernel<double>;
 }
 
+// Dynamic shared memory of the persistent kernels (tile staging buffers).
+size_t tile_smem_for(int precision) {
+  return precision == CPS_MIXED ? cps::tile_smem_bytes<float>() : cps::tile_smem_bytes<double>();
+}
+
+// Let kernel fn use `bytes` of dynamic shared memory on the current device.
+bool allow_smem(cps_ctx* c, const void* fn, size_t bytes) {
+  return cuda_ok(c, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes), "smem attribute");
+}
+
 void to_step_out(const double* h, cps_step_out* o) {
   o->residU = h[0]; o->residV = h[1]; o->residMass = h[2]; o->residMassDof = h[3]; o->err = h[4];
   o->pIters = (int)h[5]; o->uSweeps = (int)h[6]; o->vSweeps = (int)h[7];
@@ -361,7 +375,7 @@ cps_status run(cps_ctx* c, int n_outer, int stop_on_conv, double eps, cps_step_o
     void* args[] = {&c->view, &rc, &c->bar, &c->red};
     if (!cuda_ok(c, cudaEventRecord(c->ev0, c->stream), "event")) return CPS_ERR_CUDA;
     if (!cuda_ok(c, cudaLaunchCooperativeKernel(grid_kernel_for(c->precision), dim3(c->grid), dim3(cps::kThreads),
-                                                args, 0, c->stream), "cooperative launch"))
+                                                args, tile_smem_for(c->precision), c->stream), "cooperative launch"))
       return CPS_ERR_CUDA;
     if (!cuda_ok(c, cudaEventRecord(c->ev1, c->stream), "event")) return CPS_ERR_CUDA;
     if (!cuda_ok(c, cudaMemcpyAsync(c->hflags, c->dstatus, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream), "d2h"))
@@ -542,14 +556,20 @@ cps_status cps_create(const cps_desc* d, cps_ctx** out) {
 
   // Persistent grid: co-resident CTAs, at most one per tile of the design.
   int per_sm = 0, sms = 0;
-  if (!cuda_ok(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_kernel_for(d->precision),
-                                                                cps::kThreads, 0), "occupancy") ||
+  if (!allow_smem(c, grid_kernel_for(d->precision), tile_smem_for(d->precision)) ||
+      !cuda_ok(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_kernel_for(d->precision),
+                                                                cps::kThreads, tile_smem_for(d->precision)),
+               "occupancy") ||
       !cuda_ok(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->device), "attribute"))
     return bail(CPS_ERR_CUDA);
   if (per_sm < 1) return bail(fail(c, CPS_ERR_CUDA, "persistent kernel does not fit on an SM"));
   const int tiles = ((d->M - 1 + cps::kTileI - 1) / cps::kTileI) * ((d->N - 1 + cps::kTileJ - 1) / cps::kTileJ);
-  int grid = d->grid_ctas > 0 ? d->grid_ctas : std::min(sms * per_sm, std::max(1, (tiles + 1) / 2));
-  grid = std::min(std::min(grid, sms * per_sm), kMaxGridCtas);
+  // Default: the fewest rounds of tiles per CTA the co-resident CTAs allow,
+  // with the tiles spread evenly (every CTA takes part in every barrier).
+  const int cap = std::min(sms * per_sm, kMaxGridCtas);
+  const int rounds = (tiles + cap - 1) / cap;
+  int grid = d->grid_ctas > 0 ? d->grid_ctas : (tiles + rounds - 1) / rounds;
+  grid = std::min(grid, cap);
   grid = std::max(1, std::min(grid, tiles));
   c->grid = grid;
   *out = c;
@@ -682,7 +702,9 @@ cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVeloc
     const void* gk = c0->precision == CPS_MIXED ? (const void*)cps_group_kernel<float>
                                                 : (const void*)cps_group_kernel<double>;
     int per_sm = 0, sms = 0;
-    if (!cuda_ok(c0, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gk, cps::kThreads, 0), "occupancy") ||
+    const size_t tsm = tile_smem_for(c0->precision);
+    if (!allow_smem(c0, gk, tsm) ||
+        !cuda_ok(c0, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gk, cps::kThreads, tsm), "occupancy") ||
         !cuda_ok(c0, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c0->device), "attribute"))
       return CPS_ERR_CUDA;
     const int K = opts->group_ctas;
@@ -701,7 +723,7 @@ cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVeloc
     int nn = n, kk = K;
     void* args[] = {&items, &order, &nn, &queue, &res, &ws->bars, &ws->rings, &ws->slots, &kk};
     if (!cuda_ok(c0, cudaEventRecord(ws->ev0, st), "event")) return CPS_ERR_CUDA;
-    if (!cuda_ok(c0, cudaLaunchCooperativeKernel(gk, dim3(groups * K), dim3(cps::kThreads), args, 0, st),
+    if (!cuda_ok(c0, cudaLaunchCooperativeKernel(gk, dim3(groups * K), dim3(cps::kThreads), args, tsm, st),
                  "cooperative group launch"))
       return CPS_ERR_CUDA;
   } else {
@@ -710,6 +732,7 @@ cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVeloc
   if (cl > 8 &&
       !cuda_ok(c0, cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1), "attr"))
     return CPS_ERR_CUDA;
+  if (!allow_smem(c0, (const void*)kern, tile_smem_for(c0->precision))) return CPS_ERR_CUDA;
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -717,7 +740,7 @@ cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVeloc
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cfg.blockDim = dim3(cps::kThreads);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = tile_smem_for(c0->precision);
   cfg.stream = st;
   cfg.attrs = attr;
   cfg.numAttrs = 1;

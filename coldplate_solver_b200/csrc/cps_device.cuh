@@ -46,6 +46,12 @@
 // index space; element (i, j) at base[i * P + j] with P >= N + 1 a multiple of
 // 32 elements, so a warp's 32 consecutive j are one 256-byte (FP64) or
 // 128-byte (FP32) segment.
+//
+// Phases A, C and D stage each tile's inputs, halo included, in shared memory
+// with cp.async, kStageDepth tiles ahead; C then evaluates u*, v* and z0 once
+// per tile over the halo instead of once per neighbour.  B, P1 and P2 read
+// global memory directly.  Per-point expressions and per-thread summation
+// order are the same either way, so the results do not depend on staging.
 #pragma once
 #include <cuda_runtime.h>
 #include <cooperative_groups.h>
@@ -61,21 +67,11 @@ constexpr int kTileJ = 32;      // tile columns (one lane per column)
 constexpr int kRedWidth = 8;    // doubles per CTA per reduction
 constexpr int kRedSlots = 4;    // ring of reduction slots (grid group)
 // CTAs per SM the persistent kernels are compiled for (128 registers per
-// thread at 2), and tiles per round of the staged phases P1, P2 and D.  More
-// than one tile per round overlaps the tiles' load latencies but spills at
-// 128 registers; one per round measured fastest on B200.
+// thread at 2).
 #ifndef CPS_MIN_BLOCKS
 #define CPS_MIN_BLOCKS 2
 #endif
-#ifndef CPS_U_P1
-#define CPS_U_P1 1
-#endif
-#ifndef CPS_U_P2
-#define CPS_U_P2 1
-#endif
-#ifndef CPS_U_D
-#define CPS_U_D 1
-#endif
+constexpr int kStageDepth = 3;  // tiles whose shared-memory copies are in flight at once
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
 
 enum DeviceStatus : int { kStatusOk = 0, kStatusTimeout = 1, kStatusDiverged = 2 };
@@ -169,6 +165,22 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+
+// Asynchronous global -> shared copies of one 4- or 8-byte element (cp.async,
+// cached at all levels; ordered after the grid barrier's acquire like any
+// other load of this thread).
+template <typename E>
+__device__ __forceinline__ void cp_async_elem(E* smem_dst, const E* gsrc) {
+  static_assert(sizeof(E) == 4 || sizeof(E) == 8, "4- or 8-byte elements");
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  if (sizeof(E) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gsrc) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // ---------------------------------------------------------------------------
 // Block reduction of K values, fixed order (deterministic).  Bit k of MaxMask
@@ -365,36 +377,178 @@ struct ClusterGroup {
 };
 
 // ---------------------------------------------------------------------------
-// Per-point kernels
+// Tile staging.  Every phase walks the CTA's tiles (kTileI x kTileJ points,
+// one point per thread) in a fixed order.  The values a tile reads, halo
+// included, are first copied into shared memory with cp.async, which holds no
+// registers while in flight; the copies of the next tile are issued before the
+// current tile is evaluated, and every point is then evaluated from shared
+// memory with the same expressions as the reference.  Within one phase no
+// point reads a value that another point of that phase writes, so staging a
+// tile ahead of the writes of the tile before it is exact.
 // ---------------------------------------------------------------------------
 #define AT(a, i, j) (a)[(size_t)(i) * P + (j)]
 
+// Rows [r0, r0 + NR) x columns [c0, c0 + NC) of a pitched plane whose rows
+// 0..rmax and columns 0..P-1 exist, copied into dst[NR][NC].  Elements outside
+// the plane are not copied (and never read by the phases).
+template <int NR, int NC, typename E>
+__device__ __forceinline__ void stage_region(E* dst, const E* src, int P, int rmax, int r0, int c0) {
+  for (int k = threadIdx.x; k < NR * NC; k += kThreads) {
+    const int r = k / NC, c = k - r * NC;
+    const int gi = r0 + r, gj = c0 + c;
+    if (gi >= 0 && gi <= rmax && gj >= 0 && gj < P) cp_async_elem(dst + k, src + (size_t)gi * P + gj);
+  }
+}
+
+// A tile's window onto one plane: rows i0+R0 .. i0+R0+NR-1 and columns
+// j0+C0 .. j0+C0+NC-1, indexed by global (i, j).
+template <typename E, int R0, int NR, int C0, int NC>
+struct Staged {
+  using Elem = E;
+  static constexpr int kElems = NR * NC;
+  static constexpr int kPadded = (NR * NC + 3) & ~3;  // next window stays 16-byte aligned
+  static constexpr size_t kBytes = sizeof(E) * kPadded;
+  E* s;
+  int i0, j0;
+  __device__ __forceinline__ E operator()(int i, int j) const { return s[(i - i0 - R0) * NC + (j - j0 - C0)]; }
+  __device__ __forceinline__ void stage(const E* src, int P, int rmax) const {
+    stage_region<NR, NC>(s, src, P, rmax, i0 + R0, j0 + C0);
+  }
+  // (i, j) of the k-th element, for loops that fill a window from registers
+  __device__ __forceinline__ void coords(int k, int& i, int& j) const {
+    const int r = k / NC;
+    i = i0 + R0 + r;
+    j = j0 + C0 + (k - r * NC);
+  }
+};
+
+// Column 0 of a plane (gamma's inlet column) for rows i0+R0 .. i0+R0+NR-1.
+template <int R0, int NR>
+struct StagedCol0 {
+  static constexpr int kPadded = (NR + 3) & ~3;
+  static constexpr size_t kBytes = sizeof(double) * kPadded;
+  double* s;
+  int i0;
+  __device__ __forceinline__ double operator()(int row) const { return s[row - i0 - R0]; }
+  __device__ __forceinline__ void stage(const double* src, int P, int rmax) const {
+    stage_region<NR, 1>(s, src, P, rmax, i0 + R0, 0);
+  }
+};
+
+// Carves consecutive windows out of one tile buffer.
+struct Carver {
+  char* p;
+  template <class W>
+  __device__ __forceinline__ W take(int i0, int j0) {
+    W w{reinterpret_cast<typename W::Elem*>(p), i0, j0};
+    p += W::kBytes;
+    return w;
+  }
+  template <class W>
+  __device__ __forceinline__ W take_col(int i0) {
+    W w{reinterpret_cast<double*>(p), i0};
+    p += W::kBytes;
+    return w;
+  }
+};
+
+// Walk the CTA's tiles t = rank, rank + nblk, ... (the order every phase uses
+// for its per-thread sums).  Layout(buffer, i0, j0) names the tile's windows;
+// stage(L) issues the copies; compute(L, i, j, inside) evaluates the thread's
+// point (i, j) (inside: the point lies in 1..M-1 x 1..N-1; every thread of the
+// CTA calls compute, so compute may use __syncthreads).  kStageDepth tiles are
+// in flight.
+template <class Layout, class Stage, class Compute>
+__device__ __forceinline__ void for_each_tile(const DesignView& d, unsigned rank, unsigned nblk, char* tbuf,
+                                              Stage&& stage, Compute&& compute) {
+  const int tilesJ = (d.N - 1 + kTileJ - 1) / kTileJ;
+  const int tilesI = (d.M - 1 + kTileI - 1) / kTileI;
+  const int nt = tilesI * tilesJ;
+  auto buf = [&](int k) { return tbuf + (size_t)(k % kStageDepth) * Layout::kBytes; };
+  auto at = [&](int t, int k) {
+    return Layout(buf(k), 1 + (t / tilesJ) * kTileI, 1 + (t % tilesJ) * kTileJ);
+  };
+#pragma unroll
+  for (int k = 0; k < kStageDepth - 1; ++k) {
+    const int t = (int)rank + k * (int)nblk;
+    if (t < nt) stage(at(t, k));
+    cp_async_commit();
+  }
+  int k = 0;
+  for (int t = (int)rank; t < nt; t += (int)nblk, ++k) {
+    const int tn = t + (kStageDepth - 1) * (int)nblk;
+    if (tn < nt) stage(at(tn, k + kStageDepth - 1));
+    cp_async_commit();
+    cp_async_wait<kStageDepth - 1>();
+    __syncthreads();
+    const Layout L = at(t, k);
+    const int i = L.i0 + (threadIdx.x >> 5), j = L.j0 + (threadIdx.x & 31);
+    compute(L, i, j, i <= d.M - 1 && j <= d.N - 1);
+    __syncthreads();  // the buffer is restaged next round
+  }
+}
+
+// Tile iteration without staging: the same points in the same order, loads
+// straight from global memory.
+template <class F>
+__device__ __forceinline__ void for_each_point(const DesignView& d, unsigned rank, unsigned nblk, F&& f) {
+  const int tilesJ = (d.N - 1 + kTileJ - 1) / kTileJ;
+  const int tilesI = (d.M - 1 + kTileI - 1) / kTileI;
+  const int ty = threadIdx.x >> 5, tx = threadIdx.x & 31;
+  for (int t = rank; t < tilesI * tilesJ; t += nblk) {
+    const int i = 1 + (t / tilesJ) * kTileI + ty;
+    const int j = 1 + (t % tilesJ) * kTileJ + tx;
+    if (i <= d.M - 1 && j <= d.N - 1) f(i, j);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Phase A: momentum assembly + Jacobi sweep 1
+// ---------------------------------------------------------------------------
+struct LayoutA {
+  using WU = Staged<double, -2, kTileI + 4, -2, kTileJ + 4>;  // u, v: SOU reaches two cells
+  using WP = Staged<double, 0, kTileI + 1, 0, kTileJ + 1>;
+  using WA = Staged<double, -1, kTileI + 1, -1, kTileJ + 1>;
+  static constexpr size_t kBytes = 2 * WU::kBytes + WP::kBytes + WA::kBytes;
+  int i0, j0;
+  WU u, v;
+  WP p;
+  WA a;
+  __device__ __forceinline__ LayoutA(char* b, int i0_, int j0_) : i0(i0_), j0(j0_) {
+    Carver c{b};
+    u = c.take<WU>(i0, j0);
+    v = c.take<WU>(i0, j0);
+    p = c.take<WP>(i0, j0);
+    a = c.take<WA>(i0, j0);
+  }
+};
+
 // SOU deferred correction, convection.cpp:53-118 (U) and :121-186 (V); the two
 // components' range guards differ and are kept as in the reference.
-template <bool IsU>
-__device__ __forceinline__ double sou_correction(const DesignView& d, const double* __restrict__ x, int i, int j,
-                                                 double Fe, double Fw, double Fn, double Fs) {
-  const int M = d.M, N = d.N, P = d.P;
+template <bool IsU, class X>
+__device__ __forceinline__ double sou_correction(const DesignView& d, const X& x, int i, int j, double Fe, double Fw,
+                                                 double Fn, double Fs) {
+  const int M = d.M, N = d.N;
   double Sdc = 0.0;
   if (Fe >= 0.0) {
-    if (j >= 2) Sdc -= Fe * ((1.5 * AT(x, i, j) - 0.5 * AT(x, i, j - 1)) - AT(x, i, j));
+    if (j >= 2) Sdc -= Fe * ((1.5 * x(i, j) - 0.5 * x(i, j - 1)) - x(i, j));
   } else {
-    if (IsU ? (j + 2 < N) : (j + 2 <= N)) Sdc -= Fe * ((1.5 * AT(x, i, j + 1) - 0.5 * AT(x, i, j + 2)) - AT(x, i, j + 1));
+    if (IsU ? (j + 2 < N) : (j + 2 <= N)) Sdc -= Fe * ((1.5 * x(i, j + 1) - 0.5 * x(i, j + 2)) - x(i, j + 1));
   }
   if (Fw >= 0.0) {
-    if (j >= 2) Sdc += Fw * ((1.5 * AT(x, i, j - 1) - 0.5 * AT(x, i, j - 2)) - AT(x, i, j - 1));
+    if (j >= 2) Sdc += Fw * ((1.5 * x(i, j - 1) - 0.5 * x(i, j - 2)) - x(i, j - 1));
   } else {
-    if (IsU ? (j + 1 < N) : (j + 1 <= N)) Sdc += Fw * ((1.5 * AT(x, i, j) - 0.5 * AT(x, i, j + 1)) - AT(x, i, j));
+    if (IsU ? (j + 1 < N) : (j + 1 <= N)) Sdc += Fw * ((1.5 * x(i, j) - 0.5 * x(i, j + 1)) - x(i, j));
   }
   if (Fn >= 0.0) {
-    if (i >= 1) Sdc -= Fn * ((1.5 * AT(x, i, j) - 0.5 * AT(x, i - 1, j)) - AT(x, i, j));
+    if (i >= 1) Sdc -= Fn * ((1.5 * x(i, j) - 0.5 * x(i - 1, j)) - x(i, j));
   } else {
-    if (IsU ? (i + 2 <= M) : (i + 2 < M)) Sdc -= Fn * ((1.5 * AT(x, i + 1, j) - 0.5 * AT(x, i + 2, j)) - AT(x, i + 1, j));
+    if (IsU ? (i + 2 <= M) : (i + 2 < M)) Sdc -= Fn * ((1.5 * x(i + 1, j) - 0.5 * x(i + 2, j)) - x(i + 1, j));
   }
   if (Fs >= 0.0) {
-    if (i >= 2) Sdc += Fs * ((1.5 * AT(x, i - 1, j) - 0.5 * AT(x, i - 2, j)) - AT(x, i - 1, j));
+    if (i >= 2) Sdc += Fs * ((1.5 * x(i - 1, j) - 0.5 * x(i - 2, j)) - x(i - 1, j));
   } else {
-    if (IsU ? (i + 1 <= M) : (i + 1 < M)) Sdc += Fs * ((1.5 * AT(x, i, j) - 0.5 * AT(x, i + 1, j)) - AT(x, i, j));
+    if (IsU ? (i + 1 <= M) : (i + 1 < M)) Sdc += Fs * ((1.5 * x(i, j) - 0.5 * x(i + 1, j)) - x(i, j));
   }
   return Sdc;
 }
@@ -405,28 +559,26 @@ __device__ __forceinline__ double sou_correction(const DesignView& d, const doub
 //   FP64:  b = Sp, x1 = x0 + (b - A x0)/aP.
 //   mixed: b = r0 = Sp - A x0 (FP64 defect), delta1 = r0/aP (delta0 = 0).
 template <bool IsU, typename T>
-__device__ __forceinline__ double assemble_point(const DesignView& d, int i, int j, bool sweep) {
+__device__ __forceinline__ double assemble_point(const DesignView& d, const LayoutA& L, int i, int j, bool sweep) {
   constexpr bool kMixed = sizeof(T) == 4;
   const Inner<T>& w = inner<T>(d);
   const int M = d.M, N = d.N, P = d.P;
-  const double* __restrict__ u = d.u;
-  const double* __restrict__ v = d.v;
-  const double* __restrict__ p = d.p;
-  const double* __restrict__ A = d.alpha;
+  const auto& u = L.u;
+  const auto& v = L.v;
   const double mv = d.maxVel;
   double alphaLocal, ue, uw, vn, vs;
   if (IsU) {
-    alphaLocal = 0.5 * (AT(A, i - 1, j - 1) + AT(A, i - 1, j));
-    ue = clampd(0.5 * (AT(u, i, j) + AT(u, i, j + 1)), -mv, mv);
-    uw = clampd(0.5 * (AT(u, i, j - 1) + AT(u, i, j)), -mv, mv);
-    vn = clampd(0.5 * (AT(v, i, j) + AT(v, i, j + 1)), -mv, mv);
-    vs = clampd(0.5 * (AT(v, i - 1, j) + AT(v, i - 1, j + 1)), -mv, mv);
+    alphaLocal = 0.5 * (L.a(i - 1, j - 1) + L.a(i - 1, j));
+    ue = clampd(0.5 * (u(i, j) + u(i, j + 1)), -mv, mv);
+    uw = clampd(0.5 * (u(i, j - 1) + u(i, j)), -mv, mv);
+    vn = clampd(0.5 * (v(i, j) + v(i, j + 1)), -mv, mv);
+    vs = clampd(0.5 * (v(i - 1, j) + v(i - 1, j + 1)), -mv, mv);
   } else {
-    alphaLocal = 0.5 * (AT(A, i - 1, j - 1) + AT(A, i, j - 1));
-    ue = clampd(0.5 * (AT(u, i, j) + AT(u, i + 1, j)), -mv, mv);
-    uw = clampd(0.5 * (AT(u, i, j - 1) + AT(u, i + 1, j - 1)), -mv, mv);
-    vn = clampd(0.5 * (AT(v, i, j) + AT(v, i + 1, j)), -mv, mv);
-    vs = clampd(0.5 * (AT(v, i - 1, j) + AT(v, i, j)), -mv, mv);
+    alphaLocal = 0.5 * (L.a(i - 1, j - 1) + L.a(i, j - 1));
+    ue = clampd(0.5 * (u(i, j) + u(i + 1, j)), -mv, mv);
+    uw = clampd(0.5 * (u(i, j - 1) + u(i + 1, j - 1)), -mv, mv);
+    vn = clampd(0.5 * (v(i, j) + v(i + 1, j)), -mv, mv);
+    vs = clampd(0.5 * (v(i - 1, j) + v(i, j)), -mv, mv);
   }
   const double Fe = d.Fcx * ue, Fw = d.Fcx * uw, Fn = d.Fcy * vn, Fs = d.Fcy * vs;
   const double aE = d.De + maxd(0.0, -Fe), aW = d.De + maxd(0.0, Fw);
@@ -437,16 +589,16 @@ __device__ __forceinline__ double assemble_point(const DesignView& d, int i, int
   double aP0 = sumA + (Fe - Fw + Fn - Fs) + transCoeff + d.sinkDiag + brinkmanDrag;
   aP0 = maxd(aP0, 1e-10);
   const double aP = aP0 / d.uvAlpha;
-  const double* __restrict__ X = IsU ? u : v;
-  const double velCur = AT(X, i, j);
-  double Sp = IsU ? (AT(p, i, j) - AT(p, i, j + 1)) * d.hy : (AT(p, i, j) - AT(p, i + 1, j)) * d.hx;
+  const auto& X = IsU ? u : v;
+  const double velCur = X(i, j);
+  double Sp = IsU ? (L.p(i, j) - L.p(i, j + 1)) * d.hy : (L.p(i, j) - L.p(i + 1, j)) * d.hx;
   Sp += transCoeff * velCur;
   Sp += d.relax * aP0 * velCur;
   if (d.conv == 1) Sp += sou_correction<IsU>(d, X, i, j, Fe, Fw, Fn, Fs);
   if (IsU) AT(d.dE, i, j) = d.hy / aP0; else AT(d.dN, i, j) = d.hx / aP0;
   const int iHi = IsU ? M - 1 : M - 2, jHi = IsU ? N - 2 : N - 1;
   const bool hasE = j + 1 <= jHi, hasW = j - 1 >= 1, hasN = i + 1 <= iHi, hasS = i - 1 >= 1;
-  const double xE = AT(X, i, j + 1), xW = AT(X, i, j - 1), xN = AT(X, i + 1, j), xS = AT(X, i - 1, j);
+  const double xE = X(i, j + 1), xW = X(i, j - 1), xN = X(i + 1, j), xS = X(i - 1, j);
   double cE = 0.0, cW = 0.0, cN = 0.0, cS = 0.0;
   if (hasE) cE = -aE; else Sp += aE * xE;
   if (hasW) cW = -aW; else Sp += aW * xW;
@@ -485,8 +637,11 @@ __device__ __forceinline__ double assemble_point(const DesignView& d, int i, int
   return r * r;
 }
 
-// Jacobi sweep k >= 2 at one unknown (jacobi_solver.cpp:49-57).  Arithmetic in
-// FP64 on the stored values.
+// ---------------------------------------------------------------------------
+// Phase B: Jacobi sweep k >= 2 at one unknown (jacobi_solver.cpp:49-57),
+// arithmetic in FP64 on the stored values; loads straight from global memory
+// (staging the twelve planes of a tile costs more than it saves).
+// ---------------------------------------------------------------------------
 template <bool IsU, typename T>
 __device__ __forceinline__ double sweep_point(const DesignView& d, int i, int j, const T* __restrict__ xin,
                                               T* __restrict__ xout) {
@@ -509,96 +664,15 @@ __device__ __forceinline__ double sweep_point(const DesignView& d, int i, int j,
   return r * r;
 }
 
-// Final Jacobi value at a U/V unknown: FP64 the iterate, mixed u + delta.
-template <typename T>
-__device__ __forceinline__ double final_velocity(const double* __restrict__ vel, const T* __restrict__ xf, size_t o) {
-  if (sizeof(T) == 4) return vel[o] + (double)xf[o];
-  return (double)xf[o];
-}
-
-// u* after scatter + clamp + velocity BCs, evaluated from the final Jacobi
-// iterate (momentum_solver.cpp:326, boundaries.cpp:57-103).
-template <typename T>
-__device__ __forceinline__ double ustar_at(const DesignView& d, const T* __restrict__ xU, int i, int j) {
-  const int M = d.M, N = d.N, P = d.P;
-  if (i <= 0 || i >= M) return 0.0;
-  if (j == 0) return (AT(d.gamma, i - 1, 0) > 0.5) ? d.Uin : 0.0;
-  if (j >= N - 1) j = N - 2;
-  return clampd(final_velocity<T>(d.u, xU, (size_t)i * P + j), -d.maxVel, d.maxVel);
-}
-template <typename T>
-__device__ __forceinline__ double vstar_at(const DesignView& d, const T* __restrict__ xV, int i, int j) {
-  const int M = d.M, N = d.N, P = d.P;
-  if (i <= 0 || i >= M - 1 || j == 0) return 0.0;
-  if (j >= N) j = N - 1;
-  return clampd(final_velocity<T>(d.v, xV, (size_t)i * P + j), -d.maxVel, d.maxVel);
-}
-
-// ---------------------------------------------------------------------------
-// Tile iteration over the region i = 1..M-1, j = 1..N-1 shared by all phases.
-// ---------------------------------------------------------------------------
-template <class F>
-__device__ __forceinline__ void for_each_point(const DesignView& d, unsigned rank, unsigned nblk, F&& f) {
-  const int tilesJ = (d.N - 1 + kTileJ - 1) / kTileJ;
-  const int tilesI = (d.M - 1 + kTileI - 1) / kTileI;
-  const int ty = threadIdx.x >> 5, tx = threadIdx.x & 31;
-  for (int t = rank; t < tilesI * tilesJ; t += nblk) {
-    const int i = 1 + (t / tilesJ) * kTileI + ty;
-    const int j = 1 + (t % tilesJ) * kTileJ + tx;
-    if (i <= d.M - 1 && j <= d.N - 1) f(i, j);
-  }
-}
-
-// The same points in the same order, in rounds of U tiles: load(i, j) returns
-// everything a point reads and runs for all U tiles of a round before
-// body(i, j, loaded) runs for any of them, so the round's memory latencies
-// overlap instead of forming a chain through the stores.  Only for phases in
-// which no point reads what another point of the same phase writes.
-template <int U, class Load, class Body>
-__device__ __forceinline__ void for_each_point_staged(const DesignView& d, unsigned rank, unsigned nblk, Load&& load,
-                                                      Body&& body) {
-  const int tilesJ = (d.N - 1 + kTileJ - 1) / kTileJ;
-  const int tilesI = (d.M - 1 + kTileI - 1) / kTileI;
-  const int nt = tilesI * tilesJ;
-  const int ty = threadIdx.x >> 5, tx = threadIdx.x & 31;
-  using L = decltype(load(1, 1));
-  for (int t0 = rank; t0 < nt; t0 += U * (int)nblk) {
-    L buf[U];
-    int ii[U], jj[U];
-    bool on[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int t = t0 + u * (int)nblk;
-      ii[u] = 1 + (t / tilesJ) * kTileI + ty;
-      jj[u] = 1 + (t % tilesJ) * kTileJ + tx;
-      on[u] = t < nt && ii[u] <= d.M - 1 && jj[u] <= d.N - 1;
-      if (on[u]) buf[u] = load(ii[u], jj[u]);
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-      if (on[u]) body(ii[u], jj[u], buf[u]);
-  }
-}
-
 // ---------------------------------------------------------------------------
 // PCG as the reference runs it (pressure_solver.cpp:121-184): two grid-wide
 // reductions per iteration (p.Ap, then |r|^2 and r.z).  Phase P1 forms
 // p = z + beta p on the fly for the 5-point stencil and Ap; phase P2 updates
-// x, r, z.  Returns the reference's iteration count, or -1 if a wait failed.
+// x, r, z.  Both load straight from global memory, every load of a point
+// issued before its first store so that the loads overlap (staging these two
+// light phases through shared memory measured slower on B200).  Returns the
+// reference's iteration count, or -1 if a wait failed.
 // ---------------------------------------------------------------------------
-// Values phase P1 reads at one unknown: z and p_{k-1} at the point and its
-// S, W, E, N neighbours (index 0..4), and the stencil row.
-template <typename T>
-struct P1In {
-  T z[5], po[5];
-  T cS, cW, dg, cE, cN;
-};
-// Values phase P2 reads at one unknown.
-template <typename T>
-struct P2In {
-  T x, p, r, ap, dg;
-};
-
 template <typename T, class Group>
 __device__ int pcg_two_reductions(const DesignView& d, Group& g, double* smem, double rz0, double pAp0) {
   const Inner<T>& w = inner<T>(d);
@@ -612,70 +686,43 @@ __device__ int pcg_two_reductions(const DesignView& d, Group& g, double* smem, d
     double s1[1] = {pAp0};  // iteration 0's p = z, A p and p.Ap come from phase C
     if (it > 0) {
       s1[0] = 0.0;
-      for_each_point_staged<CPS_U_P1>(
-          d, g.rank, g.nblk,
-          [&](int i, int j) {
-            P1In<T> a{};
-            if (j > N - 2) return a;
-            const size_t o = (size_t)i * P + j;
-            a.z[0] = w.pz[o];
-            a.po[0] = pold[o];
-            a.dg = w.pdiag[o];
-            if (i > 1) { a.z[1] = w.pz[o - P]; a.po[1] = pold[o - P]; a.cS = w.cy[o - P]; }
-            if (j > 1) { a.z[2] = w.pz[o - 1]; a.po[2] = pold[o - 1]; a.cW = w.cx[o - 1]; }
-            if (j + 1 <= N - 2) { a.z[3] = w.pz[o + 1]; a.po[3] = pold[o + 1]; a.cE = w.cx[o]; }
-            if (i < M - 1) { a.z[4] = w.pz[o + P]; a.po[4] = pold[o + P]; a.cN = w.cy[o]; }
-            return a;
-          },
-          [&](int i, int j, const P1In<T>& a) {
-            if (j > N - 2) return;
-            const size_t o = (size_t)i * P + j;
-            // p_k at (i, j) and its unknown neighbours: p = z + beta p (pressure_solver.cpp:181)
-            auto pk = [&](int q) -> double { return (double)(T)((double)a.z[q] + bt * (double)a.po[q]); };
-            const double pc0 = pk(0);
-            double Ap = 0.0;
-            if (i > 1) Ap += -(double)a.cS * pk(1);
-            if (j > 1) Ap += -(double)a.cW * pk(2);
-            Ap += (double)a.dg * pc0;
-            if (j + 1 <= N - 2) Ap += -(double)a.cE * pk(3);
-            if (i < M - 1) Ap += -(double)a.cN * pk(4);
-            pcur[o] = (T)pc0;
-            const T apt = (T)Ap;
-            w.pAp[o] = apt;
-            s1[0] += pc0 * (double)apt;
-          });
+      for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
+        if (j > N - 2) return;
+        const size_t o = (size_t)i * P + j;
+        // p_k at (i, j) and its unknown neighbours: p = z + beta p (pressure_solver.cpp:181)
+        auto pk = [&](size_t q) -> double { return (double)(T)((double)w.pz[q] + bt * (double)pold[q]); };
+        const double pc0 = pk(o);
+        double Ap = 0.0;
+        if (i > 1) Ap += -(double)w.cy[o - P] * pk(o - P);
+        if (j > 1) Ap += -(double)w.cx[o - 1] * pk(o - 1);
+        Ap += (double)w.pdiag[o] * pc0;
+        if (j + 1 <= N - 2) Ap += -(double)w.cx[o] * pk(o + 1);
+        if (i < M - 1) Ap += -(double)w.cy[o] * pk(o + P);
+        pcur[o] = (T)pc0;
+        const T apt = (T)Ap;
+        w.pAp[o] = apt;
+        s1[0] += pc0 * (double)apt;
+      });
       if (!g.template sync_reduce<1, 0u>(s1, smem)) return -1;
     }
     const double pAp = s1[0];
     if (fabs(pAp) < 1e-20) break;
     const double alpha = rz / pAp;
     double s2[2] = {0.0, 0.0};  // |r|^2, r.z
-    for_each_point_staged<CPS_U_P2>(
-        d, g.rank, g.nblk,
-        [&](int i, int j) {
-          P2In<T> a{};
-          if (j > N - 2) return a;
-          const size_t o = (size_t)i * P + j;
-          a.x = w.px[o];
-          a.p = pcur[o];
-          a.r = w.pr[o];
-          a.ap = w.pAp[o];
-          a.dg = w.pdiag[o];
-          return a;
-        },
-        [&](int i, int j, const P2In<T>& a) {
-          if (j > N - 2) return;
-          const size_t o = (size_t)i * P + j;
-          w.px[o] = (T)((double)a.x + alpha * (double)a.p);
-          const T rt = (T)((double)a.r - alpha * (double)a.ap);
-          w.pr[o] = rt;
-          const double r = (double)rt;
-          s2[0] += r * r;
-          const double dg = (double)a.dg;
-          const T z = (T)((fabs(dg) > 1e-20) ? r / dg : r);
-          w.pz[o] = z;
-          s2[1] += r * (double)z;
-        });
+    for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
+      if (j > N - 2) return;
+      const size_t o = (size_t)i * P + j;
+      const T xo = w.px[o], pc = pcur[o], ro = w.pr[o], ap = w.pAp[o], dgo = w.pdiag[o];
+      w.px[o] = (T)((double)xo + alpha * (double)pc);
+      const T rt = (T)((double)ro - alpha * (double)ap);
+      w.pr[o] = rt;
+      const double r = (double)rt;
+      s2[0] += r * r;
+      const double dg = (double)dgo;
+      const T z = (T)((fabs(dg) > 1e-20) ? r / dg : r);
+      w.pz[o] = z;
+      s2[1] += r * (double)z;
+    });
     if (!g.template sync_reduce<2, 0u>(s2, smem)) return -1;
     if (sqrt(s2[0]) < d.pTol) break;
     const double rzPrev = rz;
@@ -785,105 +832,327 @@ __device__ int pcg_single_reduction(const DesignView& d, Group& g, double* smem,
   return k;
 }
 
+
 // ---------------------------------------------------------------------------
 // Phase D: p' scatter with the outlet column p' = 0 (pressure_solver.cpp:
 // 796-805), p += pAlpha p' and pressure BCs (iterations.cpp:456-467,
 // boundaries.cpp:111-134), velocity correction and BCs (iterations.cpp:473-499).
+// Reads p' (own point, E and N), p, dE, u*, dN, v* and gamma's inlet column;
+// writes p', p, u, v and boundary copies, none of which a point of this phase
+// reads.
 // ---------------------------------------------------------------------------
-struct DIn {
-  double pc, pcE, pcN, p, dE, us, dN, vs, g0;
+template <typename T>
+struct LayoutD {
+  using WX = Staged<T, 0, kTileI + 1, 0, kTileJ + 1>;
+  using WO = Staged<double, 0, kTileI, 0, kTileJ>;
+  using WG = StagedCol0<-1, kTileI>;
+  static constexpr size_t kBytes = WX::kBytes + 5 * WO::kBytes + WG::kBytes;
+  int i0, j0;
+  WX px;
+  WO p, dE, us, dN, vs;
+  WG g0;
+  __device__ __forceinline__ LayoutD(char* b, int i0_, int j0_) : i0(i0_), j0(j0_) {
+    Carver c{b};
+    px = c.take<WX>(i0, j0);
+    p = c.take<WO>(i0, j0);
+    dE = c.take<WO>(i0, j0);
+    us = c.take<WO>(i0, j0);
+    dN = c.take<WO>(i0, j0);
+    vs = c.take<WO>(i0, j0);
+    g0 = c.take_col<WG>(i0);
+  }
 };
 
 template <typename T, class Group>
-__device__ void correct_fields(const DesignView& d, Group& g) {
+__device__ void correct_fields(const DesignView& d, Group& g, char* tbuf) {
   const Inner<T>& w = inner<T>(d);
   const int M = d.M, N = d.N, P = d.P;
-  // Reads: p' (own point, E and N), p, dE, u*, dN, v*, gamma of the inlet
-  // column; writes p', p, u, v and the boundary copies, none of which another
-  // point of this phase reads.
-  auto load = [&](int i, int j) {
-    DIn a{};
-    const size_t o = (size_t)i * P + j;
-    a.pc = (j == N - 1) ? 0.0 : (double)w.px[o];
-    a.p = d.p[o];
-    if (j <= N - 2) {
-      a.pcE = (j + 1 == N - 1) ? 0.0 : (double)w.px[o + 1];
-      a.dE = d.dE[o];
-      a.us = d.us[o];
-    }
-    if (i <= M - 2) {
-      a.pcN = (j == N - 1) ? 0.0 : (double)w.px[o + P];
-      a.dN = d.dN[o];
-      a.vs = d.vs[o];
-    }
-    if (j == 1) a.g0 = AT(d.gamma, i - 1, 0);
-    return a;
-  };
-  for_each_point_staged<CPS_U_D>(d, g.rank, g.nblk, load, [&](int i, int j, const DIn& a) {
-    const size_t o = (size_t)i * P + j;
-    const double pcv = a.pc;
-    d.pc[o] = pcv;
-    const double pn = a.p + d.pAlpha * pcv;
-    d.p[o] = pn;
-    if (i == 1) d.p[o - P] = pn;
-    if (i == M - 1) d.p[o + P] = pn;
-    if (j == 1) d.p[o - 1] = pn;
-    if (j == N - 1) d.p[o + 1] = 0.0;
-    const double mv = d.maxVel;
-    if (j <= N - 2) {
-      double du = a.dE * (pcv - a.pcE);
-      du = maxd(-mv, mind(mv, du));
-      double un = a.us + du;
-      un = maxd(-mv, mind(mv, un));
-      d.u[o] = un;
-      if (j == N - 2) d.u[o + 1] = un;
-    }
-    if (i <= M - 2) {
-      double dv = a.dN * (pcv - a.pcN);
-      dv = maxd(-mv, mind(mv, dv));
-      double vn = a.vs + dv;
-      vn = maxd(-mv, mind(mv, vn));
-      d.v[o] = vn;
-      if (j == N - 1) d.v[o + 1] = vn;
-    }
-    // walls, inlet (boundaries.cpp:57-94)
-    if (i == 1) {
-      d.u[o - P] = 0.0;
-      d.v[o - P] = 0.0;
-      if (j == 1) { d.u[o - P - 1] = 0.0; d.v[o - P - 1] = 0.0; }
-      if (j == N - 1) d.v[o - P + 1] = 0.0;
-    }
-    if (i == M - 1) {
-      d.u[o + P] = 0.0;
-      d.v[o] = 0.0;
-      if (j == 1) { d.u[o + P - 1] = 0.0; d.v[o - 1] = 0.0; }
-      if (j == N - 1) d.v[o + 1] = 0.0;
-    }
-    if (j == 1) {
-      d.u[o - 1] = (a.g0 > 0.5) ? d.Uin : 0.0;
-      d.v[o - 1] = 0.0;
-    }
-  });
+  for_each_tile<LayoutD<T>>(
+      d, g.rank, g.nblk, tbuf,
+      [&](const LayoutD<T>& L) {
+        L.px.stage(w.px, P, M);
+        L.p.stage(d.p, P, M);
+        L.dE.stage(d.dE, P, M);
+        L.us.stage(d.us, P, M);
+        L.dN.stage(d.dN, P, M);
+        L.vs.stage(d.vs, P, M);
+        if (L.j0 == 1) L.g0.stage(d.gamma, P, M - 1);
+      },
+      [&](const LayoutD<T>& L, int i, int j, bool inside) {
+        if (!inside) return;
+        const size_t o = (size_t)i * P + j;
+        const double pcv = (j == N - 1) ? 0.0 : (double)L.px(i, j);
+        d.pc[o] = pcv;
+        const double pn = L.p(i, j) + d.pAlpha * pcv;
+        d.p[o] = pn;
+        if (i == 1) d.p[o - P] = pn;
+        if (i == M - 1) d.p[o + P] = pn;
+        if (j == 1) d.p[o - 1] = pn;
+        if (j == N - 1) d.p[o + 1] = 0.0;
+        const double mv = d.maxVel;
+        if (j <= N - 2) {
+          const double pcE = (j + 1 == N - 1) ? 0.0 : (double)L.px(i, j + 1);
+          double du = L.dE(i, j) * (pcv - pcE);
+          du = maxd(-mv, mind(mv, du));
+          double un = L.us(i, j) + du;
+          un = maxd(-mv, mind(mv, un));
+          d.u[o] = un;
+          if (j == N - 2) d.u[o + 1] = un;
+        }
+        if (i <= M - 2) {
+          const double pcN = (j == N - 1) ? 0.0 : (double)L.px(i + 1, j);
+          double dv = L.dN(i, j) * (pcv - pcN);
+          dv = maxd(-mv, mind(mv, dv));
+          double vn = L.vs(i, j) + dv;
+          vn = maxd(-mv, mind(mv, vn));
+          d.v[o] = vn;
+          if (j == N - 1) d.v[o + 1] = vn;
+        }
+        // walls, inlet (boundaries.cpp:57-94)
+        if (i == 1) {
+          d.u[o - P] = 0.0;
+          d.v[o - P] = 0.0;
+          if (j == 1) { d.u[o - P - 1] = 0.0; d.v[o - P - 1] = 0.0; }
+          if (j == N - 1) d.v[o - P + 1] = 0.0;
+        }
+        if (i == M - 1) {
+          d.u[o + P] = 0.0;
+          d.v[o] = 0.0;
+          if (j == 1) { d.u[o + P - 1] = 0.0; d.v[o - 1] = 0.0; }
+          if (j == N - 1) d.v[o + 1] = 0.0;
+        }
+        if (j == 1) {
+          d.u[o - 1] = (L.g0(i - 1) > 0.5) ? d.Uin : 0.0;
+          d.v[o - 1] = 0.0;
+        }
+      });
+}
+
+// ---------------------------------------------------------------------------
+// Phase C: scatter + clamp + max|dx| (momentum_solver.cpp:319-337), velocity
+// BCs on u*, v* (boundaries.cpp:48-106), mass imbalance (pressure_solver.cpp:
+// 468-486), pressure matrix (pressure_solver.cpp:693-732) and PCG set-up
+// (x0 = 0, r = b, z = r/diag, p = z; pressure_solver.cpp:121-150) with the
+// first PCG product A p0 (pressure_solver.cpp:153-156).
+// u* and v* are evaluated once per tile over the halo the tile needs, then z0
+// over the tile and a one-cell ring, so the neighbours' z0 entering A p0 cost
+// no extra memory traffic.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct LayoutC {
+  using WUx = Staged<T, -1, kTileI + 2, -2, kTileJ + 3>;       // final U iterate
+  using WUd = Staged<double, -1, kTileI + 2, -2, kTileJ + 3>;  // u (mixed: u + delta; both: residual), dE
+  using WVx = Staged<T, -2, kTileI + 3, -1, kTileJ + 2>;       // final V iterate
+  using WVd = Staged<double, -2, kTileI + 3, -1, kTileJ + 2>;  // v, dN
+  using WG = StagedCol0<-2, kTileI + 2>;                      // gamma(i-1, 0) for u*(i, 0)
+  using WZ = Staged<double, -1, kTileI + 2, -1, kTileJ + 2>;
+  static constexpr size_t kBytes = WUx::kBytes + 2 * WUd::kBytes + WVx::kBytes + 2 * WVd::kBytes + WG::kBytes;
+  // evaluated windows after the staging buffers (not double buffered)
+  static constexpr size_t kExtraBytes = WUd::kBytes + WVd::kBytes + WZ::kBytes;
+  int i0, j0;
+  WUx xu;
+  WUd u, dE;
+  WVx xv;
+  WVd v, dN;
+  WG g0;
+  __device__ __forceinline__ LayoutC(char* b, int i0_, int j0_) : i0(i0_), j0(j0_) {
+    Carver c{b};
+    xu = c.take<WUx>(i0, j0);
+    u = c.take<WUd>(i0, j0);
+    dE = c.take<WUd>(i0, j0);
+    xv = c.take<WVx>(i0, j0);
+    v = c.take<WVd>(i0, j0);
+    dN = c.take<WVd>(i0, j0);
+    g0 = c.take_col<WG>(i0);
+  }
+};
+
+// Final Jacobi value at a U/V unknown: FP64 the iterate, mixed u + delta.
+template <typename T>
+__device__ __forceinline__ double final_velocity(double vel, T xf) {
+  if (sizeof(T) == 4) return vel + (double)xf;
+  return (double)xf;
+}
+
+// Returns false when a wait failed.  rc: residU, residV, residMass,
+// residMassDof, non-finite flag (max); r.z, p.Ap (sum).
+template <typename T, class Group>
+__device__ bool mass_phase(const DesignView& d, Group& g, double* smem, char* tbuf, const T* xfU, const T* xfV,
+                           double (&rc)[7]) {
+  const Inner<T>& w = inner<T>(d);
+  const int M = d.M, N = d.N, P = d.P;
+  using L_t = LayoutC<T>;
+  char* ext = tbuf + (size_t)kStageDepth * L_t::kBytes;
+  const double mv = d.maxVel;
+  for_each_tile<L_t>(
+      d, g.rank, g.nblk, tbuf,
+      [&](const L_t& L) {
+        L.xu.stage(xfU, P, M);
+        L.u.stage(d.u, P, M);
+        L.dE.stage(d.dE, P, M);
+        L.xv.stage(xfV, P, M);
+        L.v.stage(d.v, P, M);
+        L.dN.stage(d.dN, P, M);
+        if (L.j0 <= 2) L.g0.stage(d.gamma, P, M - 1);
+      },
+      [&](const L_t& L, int i, int j, bool inside) {
+        Carver c{ext};
+        const auto us = c.take<typename L_t::WUd>(L.i0, L.j0);  // u* after scatter, clamp and BCs
+        const auto vs = c.take<typename L_t::WVd>(L.i0, L.j0);  // v*
+        const auto z0 = c.take<typename L_t::WZ>(L.i0, L.j0);   // z0 = r0/diag at the P-unknowns
+        // u*(ii, jj) as momentum_solver.cpp:326 + boundaries.cpp:57-103 leave it
+        for (int k = threadIdx.x; k < us.kElems; k += kThreads) {
+          int ii, jj;
+          us.coords(k, ii, jj);
+          double val = 0.0;
+          if (ii >= 1 && ii <= M - 1 && jj >= 0) {
+            if (jj == 0) {
+              val = (L.g0(ii - 1) > 0.5) ? d.Uin : 0.0;
+            } else {
+              const int jc = (jj >= N - 1) ? N - 2 : jj;
+              val = clampd(final_velocity<T>(L.u(ii, jc), L.xu(ii, jc)), -mv, mv);
+            }
+          }
+          us.s[k] = val;
+        }
+        for (int k = threadIdx.x; k < vs.kElems; k += kThreads) {
+          int ii, jj;
+          vs.coords(k, ii, jj);
+          double val = 0.0;
+          if (ii >= 1 && ii <= M - 2 && jj >= 1) {
+            const int jc = (jj >= N) ? N - 1 : jj;
+            val = clampd(final_velocity<T>(L.v(ii, jc), L.xv(ii, jc)), -mv, mv);
+          }
+          vs.s[k] = val;
+        }
+        __syncthreads();
+        // z0 at every P-unknown of the tile and its one-cell ring
+        for (int k = threadIdx.x; k < z0.kElems; k += kThreads) {
+          int ii, jj;
+          z0.coords(k, ii, jj);
+          double z = 0.0;
+          if (ii >= 1 && ii <= M - 1 && jj >= 1 && jj <= N - 2) {
+            const double mE = d.rho * us(ii, jj) * d.hy;
+            const double mW = d.rho * us(ii, jj - 1) * d.hy;
+            const double mN = d.rho * vs(ii, jj) * d.hx;
+            const double mS = d.rho * vs(ii - 1, jj) * d.hx;
+            const double b = mW - mE + mS - mN;
+            const double aE = (jj < N - 1) ? d.rho * L.dE(ii, jj) * d.hy : 0.0;
+            const double aW = (jj > 1) ? d.rho * L.dE(ii, jj - 1) * d.hy : 0.0;
+            const double aN = (ii < M - 1) ? d.rho * L.dN(ii, jj) * d.hx : 0.0;
+            const double aS = (ii > 1) ? d.rho * L.dN(ii - 1, jj) * d.hx : 0.0;
+            double aP = aE + aW + aN + aS;
+            if (aP < 1e-20) aP = 1.0;
+            const double rr = (double)(T)b, dd = (double)(T)aP;
+            z = (double)(T)((fabs(dd) > 1e-20) ? rr / dd : rr);
+          }
+          z0.s[k] = z;
+        }
+        __syncthreads();
+        if (!inside) return;
+        const size_t o = (size_t)i * P + j;
+        if (j <= N - 2) {
+          const double val = us(i, j);
+          d.us[o] = val;
+          rc[0] = maxd(rc[0], fabs(val - L.u(i, j)));
+          if (!isfinite(val)) rc[4] = 1.0;
+          if (j == N - 2) d.us[o + 1] = val;
+        }
+        if (j == 1) d.us[o - 1] = us(i, 0);
+        if (i <= M - 2) {
+          const double val = vs(i, j);
+          d.vs[o] = val;
+          rc[1] = maxd(rc[1], fabs(val - L.v(i, j)));
+          if (!isfinite(val)) rc[4] = 1.0;
+          if (j == N - 1) d.vs[o + 1] = val;
+        }
+        const double massE = d.rho * us(i, j) * d.hy;
+        const double massW = d.rho * us(i, j - 1) * d.hy;
+        const double massN = d.rho * vs(i, j) * d.hx;
+        const double massS = d.rho * vs(i - 1, j) * d.hx;
+        const double b = massW - massE + massS - massN;
+        const double ab = fabs(b);
+        if (!isfinite(ab)) rc[4] = 1.0;
+        if (ab > rc[2]) rc[2] = ab;
+        if (j <= N - 2) {
+          if (ab > rc[3]) rc[3] = ab;
+          // pressure_solver.cpp:698-703
+          const double aE = (j < N - 1) ? d.rho * L.dE(i, j) * d.hy : 0.0;
+          const double aW = (j > 1) ? d.rho * L.dE(i, j - 1) * d.hy : 0.0;
+          const double aN = (i < M - 1) ? d.rho * L.dN(i, j) * d.hx : 0.0;
+          const double aS = (i > 1) ? d.rho * L.dN(i - 1, j) * d.hx : 0.0;
+          double aP = aE + aW + aN + aS;
+          if (aP < 1e-20) aP = 1.0;
+          const T dg = (T)aP;
+          w.pdiag[o] = dg;
+          w.cx[o] = (T)aE;
+          w.cy[o] = (T)aN;
+          const T rt = (T)b;
+          w.pr[o] = rt;
+          w.px[o] = (T)0.0;
+          const double rr = (double)rt, dd = (double)dg;
+          const T z = (T)((fabs(dd) > 1e-20) ? rr / dd : rr);
+          if (d.pcgSingleReduction) {
+            w.cU[o + d.planeStride] = z;  // u0 = M^-1 r0 of the single-reduction recurrences
+          } else {
+            w.pz[o] = z;
+            w.pp0[o] = z;
+          }
+          rc[5] += rr * (double)z;
+          // first PCG product: A p0 with p0 = z0, in CSR order S, W, P, E, N
+          const double zc = (double)z;
+          double Ap = 0.0;
+          if (i > 1) Ap += -(double)(T)aS * z0(i - 1, j);
+          if (j > 1) Ap += -(double)(T)aW * z0(i, j - 1);
+          Ap += (double)dg * zc;
+          if (j + 1 <= N - 2) Ap += -(double)(T)aE * z0(i, j + 1);
+          if (i < M - 1) Ap += -(double)(T)aN * z0(i + 1, j);
+          const T apt = (T)Ap;
+          w.pAp[o] = apt;  // FP64: A p0; mixed: w0 = A u0 (the same plane)
+          rc[6] += zc * (double)apt;
+        }
+      });
+  return g.template sync_reduce<7, 0x1Fu>(rc, smem);
+}
+
+// Dynamic shared memory a persistent kernel needs for storage type T.
+template <typename T>
+constexpr size_t tile_smem_bytes() {
+  constexpr size_t a = kStageDepth * LayoutA::kBytes;
+  constexpr size_t c = kStageDepth * LayoutC<T>::kBytes + LayoutC<T>::kExtraBytes;
+  constexpr size_t dd = kStageDepth * LayoutD<T>::kBytes;
+  constexpr size_t m = a > c ? a : c;
+  return m > dd ? m : dd;
 }
 
 // ---------------------------------------------------------------------------
 // One outer iteration for one design on group g; out[8] receives the step
-// diagnostics.  Returns 0 to continue with another outer iteration, 1 when
-// this one is the last (iteration budget, convergence, or a non-finite
-// residual), -1 when the group must stop because a device-side wait failed.
+// diagnostics.  tbuf: tile_smem_bytes<T>() of shared memory.  Returns 0 to
+// continue with another outer iteration, 1 when this one is the last
+// (iteration budget, convergence, or a non-finite residual), -1 when the group
+// must stop because a device-side wait failed.
 // ---------------------------------------------------------------------------
 template <typename T, class Group>
-__device__ int outer_iteration(const DesignView& d, Group& g, double* smem, double (&out)[8], bool lastIter,
-                               bool stopOnConv, double eps) {
+__device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char* tbuf, double (&out)[8],
+                               bool lastIter, bool stopOnConv, double eps) {
   const Inner<T>& w = inner<T>(d);
   const int M = d.M, N = d.N, P = d.P;
   // ---- A: assembly + sweep 1 ----
   const bool anySweep = d.maxMomIter > 0;
   double red2[2] = {0.0, 0.0};
-  for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
-    if (j <= N - 2) red2[0] += assemble_point<true, T>(d, i, j, anySweep);
-    if (i <= M - 2) red2[1] += assemble_point<false, T>(d, i, j, anySweep);
-  });
+  for_each_tile<LayoutA>(
+      d, g.rank, g.nblk, tbuf,
+      [&](const LayoutA& L) {
+        L.u.stage(d.u, P, M);
+        L.v.stage(d.v, P, M);
+        L.p.stage(d.p, P, M);
+        L.a.stage(d.alpha, P, M - 1);
+      },
+      [&](const LayoutA& L, int i, int j, bool inside) {
+        if (!inside) return;
+        if (j <= N - 2) red2[0] += assemble_point<true, T>(d, L, i, j, anySweep);
+        if (i <= M - 2) red2[1] += assemble_point<false, T>(d, L, i, j, anySweep);
+      });
   if (!g.template sync_reduce<2, 0u>(red2, smem)) return -1;
   int kU = anySweep ? 1 : 0, kV = kU;
   bool actU = anySweep && !(red2[0] < d.thrU) && kU < d.maxMomIter;
@@ -908,96 +1177,8 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, doub
   const T* xfU = (kU & 1) ? w.xU1 : w.xU0;
   const T* xfV = (kV & 1) ? w.xV1 : w.xV0;
   // ---- C: scatter, BCs, mass residual, PCG set-up ----
-  // residU, residV, residMass, residMassDof, non-finite flag (max); r.z, p.Ap (sum)
   double rc[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  // Mass imbalance b and pressure diagonal of any P-cell, evaluated exactly as
-  // below for the cell's own thread, so that z0 = b/diag of the four
-  // neighbours -- and with it the first PCG product A z0 -- is formed here
-  // instead of in a phase of its own.
-  auto mass_b = [&](int ii, int jj) -> double {
-    const double mE = d.rho * ustar_at<T>(d, xfU, ii, jj) * d.hy;
-    const double mW = d.rho * ustar_at<T>(d, xfU, ii, jj - 1) * d.hy;
-    const double mN = d.rho * vstar_at<T>(d, xfV, ii, jj) * d.hx;
-    const double mS = d.rho * vstar_at<T>(d, xfV, ii - 1, jj) * d.hx;
-    return mW - mE + mS - mN;
-  };
-  auto p_diag = [&](int ii, int jj) -> double {
-    const double aE = (jj < N - 1) ? d.rho * AT(d.dE, ii, jj) * d.hy : 0.0;
-    const double aW = (jj > 1) ? d.rho * AT(d.dE, ii, jj - 1) * d.hy : 0.0;
-    const double aN = (ii < M - 1) ? d.rho * AT(d.dN, ii, jj) * d.hx : 0.0;
-    const double aS = (ii > 1) ? d.rho * AT(d.dN, ii - 1, jj) * d.hx : 0.0;
-    double aP = aE + aW + aN + aS;
-    if (aP < 1e-20) aP = 1.0;
-    return aP;
-  };
-  auto z0_at = [&](int ii, int jj) -> double {
-    const double rr = (double)(T)mass_b(ii, jj), dd = (double)(T)p_diag(ii, jj);
-    return (double)(T)((fabs(dd) > 1e-20) ? rr / dd : rr);
-  };
-  for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
-    const size_t o = (size_t)i * P + j;
-    if (j <= N - 2) {
-      const double val = clampd(final_velocity<T>(d.u, xfU, o), -d.maxVel, d.maxVel);
-      d.us[o] = val;
-      rc[0] = maxd(rc[0], fabs(val - d.u[o]));
-      if (!isfinite(val)) rc[4] = 1.0;
-      if (j == N - 2) d.us[o + 1] = val;
-    }
-    if (j == 1) d.us[o - 1] = ustar_at<T>(d, xfU, i, 0);
-    if (i <= M - 2) {
-      const double val = clampd(final_velocity<T>(d.v, xfV, o), -d.maxVel, d.maxVel);
-      d.vs[o] = val;
-      rc[1] = maxd(rc[1], fabs(val - d.v[o]));
-      if (!isfinite(val)) rc[4] = 1.0;
-      if (j == N - 1) d.vs[o + 1] = val;
-    }
-    const double massE = d.rho * ustar_at<T>(d, xfU, i, j) * d.hy;
-    const double massW = d.rho * ustar_at<T>(d, xfU, i, j - 1) * d.hy;
-    const double massN = d.rho * vstar_at<T>(d, xfV, i, j) * d.hx;
-    const double massS = d.rho * vstar_at<T>(d, xfV, i - 1, j) * d.hx;
-    const double b = massW - massE + massS - massN;
-    const double ab = fabs(b);
-    if (!isfinite(ab)) rc[4] = 1.0;
-    if (ab > rc[2]) rc[2] = ab;
-    if (j <= N - 2) {
-      if (ab > rc[3]) rc[3] = ab;
-      // pressure_solver.cpp:698-703
-      const double aE = (j < N - 1) ? d.rho * AT(d.dE, i, j) * d.hy : 0.0;
-      const double aW = (j > 1) ? d.rho * AT(d.dE, i, j - 1) * d.hy : 0.0;
-      const double aN = (i < M - 1) ? d.rho * AT(d.dN, i, j) * d.hx : 0.0;
-      const double aS = (i > 1) ? d.rho * AT(d.dN, i - 1, j) * d.hx : 0.0;
-      double aP = aE + aW + aN + aS;
-      if (aP < 1e-20) aP = 1.0;
-      const T dg = (T)aP;
-      w.pdiag[o] = dg;
-      w.cx[o] = (T)aE;
-      w.cy[o] = (T)aN;
-      const T rt = (T)b;
-      w.pr[o] = rt;
-      w.px[o] = (T)0.0;
-      const double rr = (double)rt, dd = (double)dg;
-      const T z = (T)((fabs(dd) > 1e-20) ? rr / dd : rr);
-      if (d.pcgSingleReduction) {
-        cg1_u(w, d.planeStride)[o] = z;  // u0 = M^-1 r0 of the single-reduction recurrences
-      } else {
-        w.pz[o] = z;
-        w.pp0[o] = z;
-      }
-      rc[5] += rr * (double)z;
-      // first PCG product: A p0 with p0 = z0 (pressure_solver.cpp:153-156), in CSR order S, W, P, E, N
-      const double zc = (double)z;
-      double Ap = 0.0;
-      if (i > 1) Ap += -(double)(T)aS * z0_at(i - 1, j);
-      if (j > 1) Ap += -(double)(T)aW * z0_at(i, j - 1);
-      Ap += (double)dg * zc;
-      if (j + 1 <= N - 2) Ap += -(double)(T)aE * z0_at(i, j + 1);
-      if (i < M - 1) Ap += -(double)(T)aN * z0_at(i + 1, j);
-      const T apt = (T)Ap;
-      w.pAp[o] = apt;  // FP64: A p0; mixed: w0 = A u0 (the same plane)
-      rc[6] += zc * (double)apt;
-    }
-  });
-  if (!g.template sync_reduce<7, 0x1Fu>(rc, smem)) return -1;
+  if (!mass_phase<T>(d, g, smem, tbuf, xfU, xfV, rc)) return -1;
   out[0] = rc[0];
   out[1] = rc[1];
   out[2] = rc[2];
@@ -1027,7 +1208,7 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, doub
     out[5] = its;
   }
   // ---- D: pressure and velocity correction ----
-  correct_fields<T>(d, g);
+  correct_fields<T>(d, g, tbuf);
   if (!stop) return g.sync() ? 0 : -1;
   return 1;
 }

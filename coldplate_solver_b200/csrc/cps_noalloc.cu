@@ -65,10 +65,12 @@ cps_status fail(cps_status s, const std::string& m) {
 __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_noalloc_kernel(cps::DesignView d, cps::RunControl rc,
                                                                       cps::GridBarrier* bar, double* red) {
   __shared__ double smem[cps::kRedWidth * 8];
+  extern __shared__ __align__(16) char tile_smem[];
   cps::GridGroup g{bar, red, rc.status, blockIdx.x, gridDim.x, 0u, 0ull};
   for (int it = 0; it < rc.n_outer; ++it) {
     double out[8];
-    const int r = cps::outer_iteration<double>(d, g, smem, out, it + 1 == rc.n_outer, rc.stop_on_conv != 0, rc.eps);
+    const int r = cps::outer_iteration<double>(d, g, smem, tile_smem, out, it + 1 == rc.n_outer,
+                                               rc.stop_on_conv != 0, rc.eps);
     if (r < 0) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       for (int k = 0; k < 8; ++k) rc.hist[(size_t)it * 8 + k] = out[k];
@@ -110,7 +112,11 @@ extern "C" cps_status cps_solve_noalloc(const cps_desc* desc, int pitch, const d
       cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
       if (e != cudaSuccess) return fail(CPS_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
       int per_sm = 0, sms = 0;
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cps_noalloc_kernel, cps::kThreads, 0);
+      e = cudaFuncSetAttribute((const void*)cps_noalloc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)cps::tile_smem_bytes<double>());
+      if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cps_noalloc_kernel, cps::kThreads,
+                                                          cps::tile_smem_bytes<double>());
       if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
       if (e != cudaSuccess || per_sm < 1) return fail(CPS_ERR_CUDA, "occupancy query failed");
       g_noalloc_ctas[dev] = std::min(sms * per_sm, kNoAllocMaxCtas);
@@ -179,7 +185,8 @@ extern "C" cps_status cps_solve_noalloc(const cps_desc* desc, int pitch, const d
   if (e != cudaSuccess) return fail(CPS_ERR_CUDA, std::string("memset: ") + cudaGetErrorString(e));
   cps::RunControl rc{max_outer, eps > 0.0 ? 1 : 0, eps, hist, done, status};
   void* args[] = {&w, &rc, &bar, &ring};
-  e = cudaLaunchCooperativeKernel((const void*)cps_noalloc_kernel, dim3(grid), dim3(cps::kThreads), args, 0, st);
+  e = cudaLaunchCooperativeKernel((const void*)cps_noalloc_kernel, dim3(grid), dim3(cps::kThreads), args,
+                                  cps::tile_smem_bytes<double>(), st);
   if (e != cudaSuccess) return fail(CPS_ERR_CUDA, std::string("cooperative launch: ") + cudaGetErrorString(e));
   int hflags[2] = {0, 0};
   e = cudaMemcpyAsync(hflags, status, sizeof(hflags), cudaMemcpyDeviceToHost, st);
