@@ -1,16 +1,18 @@
 """Batched solves of many designs of uneven size, and the project's autotuner.
 
-A batch places every design on a group of CTAs of one persistent launch
-(``cps_batch_solve``): either a group of K CTAs of a cooperative launch with a
-software group barrier, or one thread-block cluster with the hardware cluster
-barrier.  The knobs are the placement (CTAs per design: more CTAs shorten one
-design's phases, fewer CTAs let more designs run at once, and the designs in
-flight share the 126 MB L2) and the number of outer iterations a design runs
-per launch (its "visit": long visits amortise the launch, short ones let the
-host retire converged designs and admit new ones sooner).  :func:`autotune`
-times short visits of a sample of the actual designs for each candidate
-placement and keeps the fastest in cell-updates per second; results are
-cached per size bucket.
+A batch places every design on a group of CTAs of a persistent launch
+(``cps_batch_solve``): a group sized to the design (``tiles_per_cta``: each
+CTA takes that many 8 x 32 tiles per phase, and the groups run in waves that
+fill the device), a fixed group of K CTAs of one cooperative launch
+(``group_ctas``), or one thread-block cluster with the hardware cluster
+barrier (``cluster_ctas``).  The knobs are the placement (CTAs per design:
+more CTAs shorten one design's phases, fewer CTAs let more designs run at
+once, and the designs in flight share the 126 MB L2) and the number of outer
+iterations a design runs per launch (its "visit": long visits amortise the
+launch, short ones let the host retire converged designs and admit new ones
+sooner).  :func:`autotune` times short visits of a sample of the actual
+designs for each candidate placement and keeps the fastest in cell-updates
+per second; results are cached per size bucket.
 """
 from __future__ import annotations
 
@@ -25,16 +27,28 @@ from . import cps
 from .geometry import Design
 
 def mode_candidates(device: int = 0) -> List[dict]:
-    """Placements the autotuner tries: groups of 2x, 1x, 1/2x and 1/4x the SM
-    count of CTAs (2, 1, 2 ... designs in flight at 2 CTAs per SM) and
-    thread-block clusters of 8 and 16 CTAs."""
+    """Placements the autotuner tries: groups sized to each design at 2, 4, 8
+    and 16 tiles per CTA, fixed groups of 2x, 1x, 1/2x and 1/4x the SM count of
+    CTAs, and thread-block clusters of 8 and 16 CTAs."""
     try:
         import torch
         sms = torch.cuda.get_device_properties(device).multi_processor_count
     except Exception:  # noqa: BLE001 - no torch/GPU: B200 count
         sms = 148
     groups = [2 * sms, sms, sms // 2, sms // 4]
-    return [{"group_ctas": k} for k in groups if k >= 1] + [{"cluster_ctas": 8}, {"cluster_ctas": 16}]
+    return ([{"tiles_per_cta": t} for t in (2, 4, 8, 16)] + [{"group_ctas": k} for k in groups if k >= 1] +
+            [{"cluster_ctas": 8}, {"cluster_ctas": 16}])
+
+
+def default_mode(device: int = 0) -> dict:
+    """Placement used when none is given: groups of as many CTAs as the device
+    has SMs (two designs in flight at two CTAs per SM), which measured fastest
+    on the 16- and 64-design mixes; the autotuner picks per workload."""
+    try:
+        import torch
+        return {"group_ctas": torch.cuda.get_device_properties(device).multi_processor_count}
+    except Exception:  # noqa: BLE001 - no torch/GPU: B200 count
+        return {"group_ctas": 148}
 
 
 def mode_label(mode: dict) -> str:
@@ -100,6 +114,7 @@ class BatchRunner:
     all of them to ``eps`` in launches of at most ``visit`` outer iterations
     per design; designs that converge leave the batch between launches.
     ``mode`` is the keyword of :func:`cps.batch_solve` that places designs:
+    ``{"tiles_per_cta": R}`` (groups sized to each design, in waves),
     ``{"group_ctas": K}`` (groups of K CTAs of one cooperative launch) or
     ``{"cluster_ctas": C}`` (one thread-block cluster per design)."""
 
@@ -107,7 +122,7 @@ class BatchRunner:
                  mode: Optional[dict] = None):
         self.designs = list(designs)
         self.solvers = [cps.Solver(d, precision=precision, device=device) for d in self.designs]
-        self.mode = dict(mode or {"group_ctas": 74})
+        self.mode = dict(mode or default_mode(device))
 
     def close(self) -> None:
         for s in self.solvers:

@@ -68,7 +68,8 @@ class CpsPlane(ctypes.Structure):
 
 class CpsBatchOpts(ctypes.Structure):
     _fields_ = [("cluster_ctas", ctypes.c_int), ("max_clusters", ctypes.c_int), ("max_outer", ctypes.c_int),
-                ("eps", ctypes.c_double), ("order_by_size", ctypes.c_int), ("group_ctas", ctypes.c_int)]
+                ("eps", ctypes.c_double), ("order_by_size", ctypes.c_int), ("group_ctas", ctypes.c_int),
+                ("tiles_per_cta", ctypes.c_int)]
 
 
 class CpsBatchResult(ctypes.Structure):
@@ -289,10 +290,12 @@ def history_to_array(hist, n: int) -> np.ndarray:
 
 
 def batch_solve(solvers, max_outer: int, eps: float = 1e-6, cluster_ctas: int = 8, max_clusters: int = 0,
-                order_by_size: bool = True, inlet_velocities=None, group_ctas: int = 0):
-    """Run many resident designs in one persistent cluster launch
-    (cps_batch_solve).  Returns (results, kernel_ms); results[k] is a dict with
-    n_done, converged, status and the last step's diagnostics."""
+                order_by_size: bool = True, inlet_velocities=None, group_ctas: int = 0, tiles_per_cta: int = 0):
+    """Advance many resident designs together (cps_batch_solve): on
+    thread-block clusters of ``cluster_ctas``, on groups of ``group_ctas`` CTAs,
+    or (``tiles_per_cta`` > 0) on groups sized to each design, in waves.
+    Returns (results, kernel_ms); results[k] is a dict with n_done, converged,
+    status and the last step's diagnostics."""
     if not solvers:
         return [], 0.0
     lib = solvers[0].lib
@@ -301,7 +304,7 @@ def batch_solve(solvers, max_outer: int, eps: float = 1e-6, cluster_ctas: int = 
     uin = np.ascontiguousarray([s.inletVelocity if inlet_velocities is None else inlet_velocities[k]
                                 for k, s in enumerate(solvers)], dtype=np.float64)
     opts = CpsBatchOpts(cluster_ctas=cluster_ctas, max_clusters=max_clusters, max_outer=max_outer, eps=eps,
-                        order_by_size=int(order_by_size), group_ctas=group_ctas)
+                        order_by_size=int(order_by_size), group_ctas=group_ctas, tiles_per_cta=tiles_per_cta)
     res = (CpsBatchResult * n)()
     ms = ctypes.c_double(0.0)
     st = lib.cps_batch_solve(ctxs, n, _dptr(uin), ctypes.byref(opts), res, ctypes.byref(ms))

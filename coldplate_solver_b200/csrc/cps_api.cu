@@ -196,6 +196,54 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_group_kerne
   }
 }
 
+// Batched solves in waves: one design per group, groups sized to their
+// designs.  CTAs [first[g], first[g+1]) form group g and run design which[g]
+// to convergence or to its budget with the bounded software barrier of their
+// own counter; their reduction ring starts at first[g] ring rows.
+template <typename T>
+__global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_wave_kernel(const cps::BatchItem* __restrict__ items,
+                                                                   const int* __restrict__ first,
+                                                                   const int* __restrict__ which, int groups,
+                                                                   cps::BatchResult* results,
+                                                                   cps::GridBarrier* bars, double* rings) {
+  __shared__ double smem[cps::kRedWidth * 8];
+  __shared__ __align__(16) cps::BatchItem s_item;
+  extern __shared__ __align__(16) char tile_smem[];
+  int lo = 0, hi = groups;  // first[lo] <= blockIdx.x < first[lo + 1]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (first[mid] <= (int)blockIdx.x) lo = mid; else hi = mid;
+  }
+  const int grp = lo, K = first[grp + 1] - first[grp], id = which[grp];
+  {
+    const int* src = reinterpret_cast<const int*>(items + id);
+    int* dst = reinterpret_cast<int*>(&s_item);
+    for (int k = threadIdx.x; k < (int)(sizeof(cps::BatchItem) / sizeof(int)); k += blockDim.x) dst[k] = src[k];
+  }
+  __syncthreads();
+  const cps::BatchItem& item = s_item;
+  cps::BatchResult* res = results + id;
+  cps::GridGroup g{bars + grp, rings + (size_t)first[grp] * cps::kRedSlots * cps::kRedWidth, &res->status,
+                   blockIdx.x - (unsigned)first[grp], (unsigned)K, 0u, 0ull};
+  double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int done = 0;
+  for (int it = 0; it < item.n_outer; ++it) {
+    const int r = cps::outer_iteration<T>(item.view, g, smem, tile_smem, out, it + 1 == item.n_outer,
+                                          item.stop_on_conv != 0, item.eps);
+    if (r < 0) return;  // a bounded wait expired; the design's status says so
+    done = it + 1;
+    if (g.rank == 0 && threadIdx.x == 0 && item.hist && it < item.hist_cap)
+      for (int k = 0; k < 8; ++k) item.hist[(size_t)it * 8 + k] = out[k];
+    if (r != 0) break;
+  }
+  if (g.rank == 0 && threadIdx.x == 0) {
+    res->n_done = done;
+    const double conv = cps::maxd(cps::maxd(out[0], out[1]), out[3]);
+    res->converged = (done > 0 && conv <= item.eps) ? 1 : 0;
+    for (int k = 0; k < 8; ++k) res->last[k] = out[k];
+  }
+}
+
 // samplePlaneAtX (postprocessing.cpp:62-230) for one plane, one CTA: every row's
 // contribution is evaluated with the reference's expressions; the five sums are
 // combined in a fixed tree order.
@@ -420,6 +468,8 @@ struct BatchWorkspace {
   cps::GridBarrier* bars = nullptr;  // group kernel: one barrier, ring and slot pair per group
   double* rings = nullptr;
   int* slots = nullptr;
+  int* plan = nullptr;    // wave kernel: per wave, first[groups + 1] then which[groups]
+  int* h_plan = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 std::mutex g_batch_mutex;
@@ -442,15 +492,17 @@ BatchWorkspace* batch_workspace(int device, size_t n, std::string& err) {
     }
   }
   if (ws->cap < n) {
-    cudaFree(ws->items); cudaFree(ws->order); cudaFree(ws->queue); cudaFree(ws->results);
-    cudaFreeHost(ws->h_items); cudaFreeHost(ws->h_order); cudaFreeHost(ws->h_results);
-    ws->items = nullptr; ws->order = nullptr; ws->queue = nullptr; ws->results = nullptr;
-    ws->h_items = nullptr; ws->h_order = nullptr; ws->h_results = nullptr;
+    cudaFree(ws->items); cudaFree(ws->order); cudaFree(ws->queue); cudaFree(ws->results); cudaFree(ws->plan);
+    cudaFreeHost(ws->h_items); cudaFreeHost(ws->h_order); cudaFreeHost(ws->h_results); cudaFreeHost(ws->h_plan);
+    ws->items = nullptr; ws->order = nullptr; ws->queue = nullptr; ws->results = nullptr; ws->plan = nullptr;
+    ws->h_items = nullptr; ws->h_order = nullptr; ws->h_results = nullptr; ws->h_plan = nullptr;
     ws->cap = 0;
     const size_t cap = std::max<size_t>(n, 64);
     if (cudaMalloc(&ws->items, cap * sizeof(cps::BatchItem)) != cudaSuccess ||
         cudaMalloc(&ws->order, cap * sizeof(int)) != cudaSuccess || cudaMalloc(&ws->queue, 256) != cudaSuccess ||
         cudaMalloc(&ws->results, cap * sizeof(cps::BatchResult)) != cudaSuccess ||
+        cudaMalloc(&ws->plan, 3 * cap * sizeof(int)) != cudaSuccess ||
+        cudaMallocHost(&ws->h_plan, 3 * cap * sizeof(int)) != cudaSuccess ||
         cudaMallocHost(&ws->h_items, cap * sizeof(cps::BatchItem)) != cudaSuccess ||
         cudaMallocHost(&ws->h_order, cap * sizeof(int)) != cudaSuccess ||
         cudaMallocHost(&ws->h_results, cap * sizeof(cps::BatchResult)) != cudaSuccess) {
@@ -697,7 +749,68 @@ cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVeloc
       !cuda_ok(c0, cudaMemsetAsync(ws->queue, 0, sizeof(int), st), "memset") ||
       !cuda_ok(c0, cudaMemsetAsync(ws->results, 0, sizeof(cps::BatchResult) * n, st), "memset"))
     return CPS_ERR_CUDA;
-  if (opts->group_ctas > 0) {
+  if (opts->tiles_per_cta > 0) {
+    // Groups sized to their designs, packed into waves (first fit, largest
+    // first); one cooperative launch per wave, all CTAs of a wave co-resident.
+    const void* wk = c0->precision == CPS_MIXED ? (const void*)cps_wave_kernel<float>
+                                                : (const void*)cps_wave_kernel<double>;
+    int per_sm = 0, sms = 0;
+    const size_t tsm = tile_smem_for(c0->precision);
+    if (!allow_smem(c0, wk, tsm) ||
+        !cuda_ok(c0, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wk, cps::kThreads, tsm), "occupancy") ||
+        !cuda_ok(c0, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c0->device), "attribute"))
+      return CPS_ERR_CUDA;
+    const int max_ctas = std::min(sms * per_sm, kMaxGridCtas);
+    if (max_ctas < 1) return fail(c0, CPS_ERR_CUDA, "wave kernel does not fit on an SM");
+    std::vector<int> ctas(n);
+    for (int k = 0; k < n; ++k) {
+      const long long tiles = (long long)((ctxs[k]->M - 1 + cps::kTileI - 1) / cps::kTileI) *
+                              ((ctxs[k]->N - 1 + cps::kTileJ - 1) / cps::kTileJ);
+      ctas[k] = (int)std::max(1LL, std::min<long long>(max_ctas, (tiles + opts->tiles_per_cta - 1) / opts->tiles_per_cta));
+    }
+    std::vector<int> byc(n);
+    std::iota(byc.begin(), byc.end(), 0);
+    std::stable_sort(byc.begin(), byc.end(), [&](int a, int b) { return ctas[a] > ctas[b]; });
+    std::vector<std::vector<int>> waves;
+    std::vector<int> room;
+    for (int k : byc) {
+      size_t w = 0;
+      while (w < waves.size() && room[w] < ctas[k]) ++w;
+      if (w == waves.size()) { waves.emplace_back(); room.push_back(max_ctas); }
+      waves[w].push_back(k);
+      room[w] -= ctas[k];
+    }
+    // plan: for each wave, first[G + 1] then which[G]; at most 3n ints
+    std::vector<size_t> at(waves.size());
+    size_t pos = 0;
+    for (size_t w = 0; w < waves.size(); ++w) {
+      at[w] = pos;
+      int* f = ws->h_plan + pos;
+      const int G = (int)waves[w].size();
+      f[0] = 0;
+      for (int q = 0; q < G; ++q) {
+        f[q + 1] = f[q] + ctas[waves[w][q]];
+        f[G + 1 + q] = waves[w][q];
+      }
+      pos += 2 * (size_t)G + 1;
+    }
+    if (!cuda_ok(c0, cudaMemcpyAsync(ws->plan, ws->h_plan, sizeof(int) * pos, cudaMemcpyHostToDevice, st), "h2d"))
+      return CPS_ERR_CUDA;
+    const cps::BatchItem* items = ws->items;
+    cps::BatchResult* res = ws->results;
+    if (!cuda_ok(c0, cudaEventRecord(ws->ev0, st), "event")) return CPS_ERR_CUDA;
+    for (size_t w = 0; w < waves.size(); ++w) {
+      int G = (int)waves[w].size();
+      const int* first = ws->plan + at[w];
+      const int* which = first + G + 1;
+      const int grid = ws->h_plan[at[w] + G];
+      if (!cuda_ok(c0, cudaMemsetAsync(ws->bars, 0, sizeof(cps::GridBarrier) * G, st), "memset")) return CPS_ERR_CUDA;
+      void* args[] = {&items, &first, &which, &G, &res, &ws->bars, &ws->rings};
+      if (!cuda_ok(c0, cudaLaunchCooperativeKernel(wk, dim3(grid), dim3(cps::kThreads), args, tsm, st),
+                   "cooperative wave launch"))
+        return CPS_ERR_CUDA;
+    }
+  } else if (opts->group_ctas > 0) {
     // Groups of CTAs in one cooperative launch (all CTAs co-resident).
     const void* gk = c0->precision == CPS_MIXED ? (const void*)cps_group_kernel<float>
                                                 : (const void*)cps_group_kernel<double>;

@@ -5,11 +5,12 @@ as its device footprint (``cps_footprint``) fits in the HBM budget and an
 in-flight slot is free; admitted designs keep their fields resident until
 they converge.  The GPU runs epochs: one ``cps_batch_solve`` launch advances
 every in-flight design by at most ``visit`` outer iterations (each design on
-its own thread-block cluster, converged designs stop early).  Between epochs
+its own group of CTAs of a cooperative launch, or its own thread-block
+cluster; converged designs stop early).  Between epochs
 the host retires converged designs (freeing their memory) and admits the
 requests that arrived meanwhile, so new work overlaps with designs already on
 the device.  A design's result does not depend on the mix it ran in: its
-cluster computes exactly what it would compute alone.
+group computes exactly what it would compute alone.
 
 Latency of a request = time from its arrival to the end of the epoch in which
 it converged (queueing + admission + solve).
@@ -23,7 +24,7 @@ from typing import Deque, Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
 
-from . import cps
+from . import batch, cps
 from .geometry import Design
 
 
@@ -61,12 +62,17 @@ class ServeStats:
 
 
 class Server:
-    def __init__(self, budget_bytes: float = 120e9, visit: int = 300, cluster_ctas: int = 8,
+    def __init__(self, budget_bytes: float = 120e9, visit: int = 300, cluster_ctas: Optional[int] = None,
                  precision: int = cps.CPS_MIXED, device: int = 0, max_inflight: int = 256, eps: float = 1e-6,
-                 max_outer: int = 200000, keep_fields: bool = False):
+                 max_outer: int = 200000, keep_fields: bool = False, mode: Optional[dict] = None):
+        """``mode``: placement keyword of :func:`cps.batch_solve`
+        (default: :func:`batch.default_mode`); ``cluster_ctas`` is shorthand
+        for ``mode={"cluster_ctas": cluster_ctas}``."""
         self.budget = int(budget_bytes)
         self.visit = visit
-        self.cluster_ctas = cluster_ctas
+        if mode is None:
+            mode = {"cluster_ctas": cluster_ctas} if cluster_ctas else batch.default_mode(device)
+        self.mode = dict(mode)
         self.precision = precision
         self.device = device
         self.max_inflight = max_inflight
@@ -105,8 +111,7 @@ class Server:
                 if pending:
                     time.sleep(max(0.0, min(pending[0].arrival - (time.perf_counter() - t0), 0.05)))
                 continue
-            res, ms = cps.batch_solve([s for _, s, _ in inflight], self.visit, eps=self.eps,
-                                      cluster_ctas=self.cluster_ctas)
+            res, ms = cps.batch_solve([s for _, s, _ in inflight], self.visit, eps=self.eps, **self.mode)
             epochs += 1
             device_ms += ms
             end = time.perf_counter() - t0

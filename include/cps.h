@@ -160,6 +160,10 @@ typedef struct {
   int order_by_size;  /* start the largest designs first */
   int group_ctas;     /* > 0: run designs on groups of this many CTAs of one cooperative launch (software
                          group barrier, bounded waits) instead of on thread-block clusters */
+  int tiles_per_cta;  /* > 0 (overrides group_ctas and cluster_ctas): give each design a group of
+                         ceil(tiles / tiles_per_cta) CTAs (a tile is 8 x 32 points; at most the device's
+                         co-resident CTAs) and run the groups in waves, one cooperative launch per wave,
+                         packed largest first so that each wave fills the device */
 } cps_batch_opts;
 
 /* Per-design outcome of a batched solve. */
@@ -174,7 +178,9 @@ typedef struct {
  * cluster (hardware cluster barrier) or, with group_ctas > 0, on one group of
  * CTAs of a cooperative launch (software group barrier), until it meets eps
  * or spends max_outer outer iterations; clusters/groups take designs from a
- * device work queue, so designs of uneven size share the GPU.  Every context must be
+ * device work queue, so designs of uneven size share the GPU.  With
+ * tiles_per_cta > 0 each design's group is sized to the design instead, and
+ * the designs run in as few launches (waves) as the co-resident CTAs allow.  Every context must be
  * on the same device with the same precision.  Has no reference counterpart:
  * the reference solves one design per process (SIMPLE.cpp:638-642).
  * inletVelocity: n values or NULL to keep each context's last value.

@@ -95,7 +95,7 @@ def uneven_designs():
 
 
 @pytest.mark.parametrize("mode,size", [("cluster", 1), ("cluster", 4), ("cluster", 8), ("cluster", 16),
-                                       ("group", 3), ("group", 37), ("group", 74)])
+                                       ("group", 3), ("group", 37), ("group", 74), ("wave", 1), ("wave", 4)])
 def test_batch_matches_solo_solves(mode, size):
     designs = uneven_designs()
     n = 7
@@ -108,8 +108,10 @@ def test_batch_matches_solo_solves(mode, size):
     try:
         if mode == "cluster":
             res, ms = cps.batch_solve(solvers, n, eps=0.0, cluster_ctas=size)
-        else:
+        elif mode == "group":
             res, ms = cps.batch_solve(solvers, n, eps=0.0, group_ctas=size)
+        else:
+            res, ms = cps.batch_solve(solvers, n, eps=0.0, tiles_per_cta=size)
         assert ms > 0
         for k, s in enumerate(solvers):
             assert res[k]["n_done"] == n and res[k]["status"] == 0
@@ -125,7 +127,7 @@ def test_batch_matches_solo_solves(mode, size):
             s.close()
 
 
-@pytest.mark.parametrize("kw", [{"cluster_ctas": 8}, {"group_ctas": 37}])
+@pytest.mark.parametrize("kw", [{"cluster_ctas": 8}, {"group_ctas": 37}, {"tiles_per_cta": 2}])
 def test_batch_result_is_the_same_alone_and_in_the_mix(kw):
     designs = uneven_designs()
     target = 2
@@ -141,6 +143,37 @@ def test_batch_result_is_the_same_alone_and_in_the_mix(kw):
             s.close()
     for f in FIELDS:
         assert np.array_equal(fa[f], fm[f]), f
+
+
+def tiles(d):
+    return ((d.M - 1 + 7) // 8) * ((d.N - 1 + 31) // 32)
+
+
+@pytest.mark.parametrize("tpc", [1, 3, 8])
+@pytest.mark.parametrize("precision", [cps.CPS_FP64, cps.CPS_MIXED])
+def test_wave_batch_is_bitwise_the_solo_solve_on_as_many_ctas(tpc, precision):
+    """A design's group in a wave has ceil(tiles / tiles_per_cta) CTAs and then
+    computes exactly what the single-design kernel computes on that many CTAs."""
+    designs = uneven_designs() + [geometry.density_field(Nx=300, seed=4)]
+    n = 6
+    solo = []
+    for d in designs:
+        k = -(-tiles(d) // tpc)
+        with cps.Solver(d, precision=precision, grid_ctas=k) as s:
+            solo.append((s.solve(n, eps=0.0), s.download()))
+    solvers = [cps.Solver(d, precision=precision) for d in designs]
+    try:
+        res, _ = cps.batch_solve(solvers, n, eps=0.0, tiles_per_cta=tpc)
+        for k, s in enumerate(solvers):
+            assert res[k]["n_done"] == n and res[k]["status"] == 0
+            hs, fs = solo[k]
+            assert np.array_equal(cps.get_history(s, n), hs), k
+            fb = s.download()
+            for f in FIELDS:
+                assert np.array_equal(fb[f], fs[f]), (k, f)
+    finally:
+        for s in solvers:
+            s.close()
 
 
 def test_batch_stops_each_design_at_convergence():
@@ -162,7 +195,7 @@ def test_batch_stops_each_design_at_convergence():
         assert abs(r["n_done"] - solo_iters[k]) <= max(3, solo_iters[k] // 5), (r["n_done"], solo_iters[k])
 
 
-@pytest.mark.parametrize("kw", [{"cluster_ctas": 8}, {"group_ctas": 16}])
+@pytest.mark.parametrize("kw", [{"cluster_ctas": 8}, {"group_ctas": 16}, {"tiles_per_cta": 4}])
 def test_batch_mixed_precision_runs(kw):
     designs = uneven_designs()[:4]
     solvers = [cps.Solver(d, precision=cps.CPS_MIXED) for d in designs]

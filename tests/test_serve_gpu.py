@@ -1,10 +1,10 @@
 """Serving loop: continuous batching with HBM-footprint admission.
 
 The key property: each request's result is the same alone and in the mix.
-Within one cluster size a design's cluster computes exactly what it would
-compute alone, so the comparison is exact (bit for bit) on the fields and the
-iteration count; across precisions and modes the tolerances of the other
-tests apply."""
+Within one placement a design's group of CTAs (a thread-block cluster, or a
+group sized to the design) computes exactly what it would compute alone, so
+the comparison is exact (bit for bit) on the fields and the iteration count;
+across precisions and placements the tolerances of the other tests apply."""
 import numpy as np
 import pytest
 
@@ -28,15 +28,16 @@ def small_stream(n=6, seed=3):
     return out
 
 
+@pytest.mark.parametrize("mode", [{"cluster_ctas": 4}, {"tiles_per_cta": 2}])
 @pytest.mark.parametrize("precision", [cps.CPS_FP64, cps.CPS_MIXED])
-def test_each_result_is_the_same_alone_and_in_the_mix(precision):
+def test_each_result_is_the_same_alone_and_in_the_mix(precision, mode):
     stream = small_stream()
-    srv = serve.Server(visit=40, cluster_ctas=4, precision=precision, keep_fields=True, max_outer=30000)
+    srv = serve.Server(visit=40, mode=mode, precision=precision, keep_fields=True, max_outer=30000)
     stats = srv.run(stream, real_time=True)
     assert stats.completed == len(stream), [(r.converged, r.outer_iterations) for r in stats.requests]
     assert stats.max_inflight >= 2  # requests overlapped on the device
     for r in stats.requests:
-        alone = serve.Server(visit=40, cluster_ctas=4, precision=precision, keep_fields=True, max_outer=30000)
+        alone = serve.Server(visit=40, mode=mode, precision=precision, keep_fields=True, max_outer=30000)
         s1 = alone.run([(0.0, r.design)], real_time=False)
         a = s1.requests[0]
         assert a.outer_iterations == r.outer_iterations
@@ -58,7 +59,7 @@ def test_admission_respects_the_memory_budget():
 
 def test_latency_statistics():
     stream = small_stream(8, seed=11)
-    stats = serve.Server(visit=50, cluster_ctas=8, max_outer=30000).run(stream, real_time=True)
+    stats = serve.Server(visit=50, max_outer=30000).run(stream, real_time=True)
     lat = [r.latency for r in stats.requests]
     assert all(x > 0 for x in lat)
     assert stats.latency_p99_s >= stats.latency_p50_s > 0
