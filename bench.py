@@ -2,7 +2,7 @@
 """Benchmark: converged SIMPLE solves per second on one B200 (and N GPUs).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload network|straight|density|mix] [--precision fp64|mixed]
+                    [--workload network|straight|density|mix|served] [--precision fp64|mixed]
 
 A step is one converged solve (outer residual max(residU, residV,
 residMassDof) <= 1e-6) of the workload's design(s), started from the zero
@@ -15,6 +15,16 @@ u, v, p downloaded, every step (wall clock).
 Multi-GPU (torchrun, one rank per GPU): every rank solves its own copy of the
 workload (independent designs, no collective on the data path; weak scaling);
 the timed region is bracketed by barriers and the max over ranks is taken.
+
+--workload mix / served (one GPU): the many-design paths.  mix: the first
+--designs designs of the seeded 64-design density-field mix (Nx log-uniform
+in [256, 1024], Ny = Nx/2) solved together by the batched persistent kernel;
+a step is the whole batch.  served: --requests Poisson arrivals (20/s) of
+density-field designs (Nx in [128, 2048]) through the serving loop (HBM
+admission, continuous batching); latency is wall clock from arrival to
+convergence.  Both lines carry the plain FP64 single-design path on the same
+designs, one after another, as the comparison, and the relative dP
+difference of every design against it.
 
 --impl reference times the reference solver's own CPU implementation
 (oracle/_ref/ref_f64: its sources promoted to FP64, all host threads) on the
@@ -339,6 +349,11 @@ def run_reference(args) -> None:
     if rank != 0:
         return
     from oracle import reference
+    if args.workload in ("mix", "served"):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's converged iteration counts on the "
+                          "many-design workloads are not precomputed (hours of CPU); its arm runs on the "
+                          "single-design workloads"}))
+        return
     design, cfg = workload(args.workload)
     if not reference.available("f64"):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_f64 is not built (make -C oracle ref)"}))
@@ -367,6 +382,135 @@ def run_reference(args) -> None:
     }), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# many-design workloads: batched mix and served stream
+# ---------------------------------------------------------------------------
+def many_designs(args):
+    from coldplate_solver_b200 import geometry as g
+    if args.workload == "mix":
+        designs = g.batch_mix(64)[: args.designs]
+        cfg = {"workload": f"density_mix_{len(designs)}of64_nx256-1024", "designs": len(designs), "dx_um": 10,
+               "convection": "SOU", "two_point_five_d": True, "nx_range": [256, 1024]}
+        return designs, [0.0] * len(designs), cfg
+    stream = g.served_stream(args.requests, rate=20.0)
+    cfg = {"workload": f"served_stream_{args.requests}req_poisson20_nx128-2048", "requests": args.requests,
+           "arrival_rate_per_s": 20.0, "nx_range": [128, 2048], "hbm_budget_gb": 120}
+    return [d for _, d in stream], [t for t, _ in stream], cfg
+
+
+def plain_fp64_sequential(designs, arrivals, device):
+    """Every design alone on the single-design FP64 kernel, one after another
+    (device time per solve); FIFO latencies for the given arrival times."""
+    from coldplate_solver_b200 import cps
+    rows = []
+    for d in designs:
+        with cps.Solver(d, precision=cps.CPS_FP64, device=device) as s:
+            s.reset_fields()
+            s.kernel_timing(reset=True)
+            h = s.solve(MAX_OUTER, eps=EPS)
+            ms, launches, it = s.kernel_timing(reset=True)
+            rows.append({"ms": ms, "iters": int(it), "dp": s.full_dp(), "launches": launches,
+                         "converged": bool(max(h[-1, 0], h[-1, 1], h[-1, 3]) <= EPS)})
+    t, lat = 0.0, []
+    for a, r in zip(arrivals, rows):
+        t = max(t, a * 1e3) + r["ms"]
+        lat.append(t - a * 1e3)
+    return rows, lat
+
+
+def run_many(args) -> None:
+    import torch
+
+    from coldplate_solver_b200 import batch, cps, serve
+    rank, local, world = dist_init(args.gpus)
+    device = local
+    torch.cuda.set_device(device)
+    designs, arrivals, cfg = many_designs(args)
+    precision = cps.CPS_MIXED if args.precision == "mixed" else cps.CPS_FP64
+    mode = batch.default_mode(device) if args.placement == "default" else json.loads(args.placement)
+    n = len(designs)
+    seq, seq_lat = plain_fp64_sequential(designs, arrivals, device)
+    seq_ms = sum(r["ms"] for r in seq)
+    clocks = None
+    if args.workload == "mix":
+        with batch.BatchRunner(designs, precision=precision, device=device, mode=mode) as br:
+            for _ in range(args.warmup):  # module load, first touch; short visits from the zero state
+                br.run(eps=EPS, max_outer=100, visit=100)
+            with ClockSampler(device) as clocks:
+                ms_total, launches, lat = 0.0, 0, []
+                t0 = time.perf_counter()
+                for _ in range(args.steps):
+                    res, ms, nl = br.run(eps=EPS, max_outer=MAX_OUTER, visit=args.visit)
+                    ms_total += ms
+                    launches += nl
+                    lat += [r["finished_ms"] for r in res]
+                wall = time.perf_counter() - t0
+            dps = [s.full_dp() for s in br.solvers]
+            # e2e: designs from host memory to converged fields back on the host
+            t1 = time.perf_counter()
+            br2 = batch.BatchRunner(designs, precision=precision, device=device, mode=mode)
+            res2, _, _ = br2.run(eps=EPS, max_outer=MAX_OUTER, visit=args.visit, reset=False)
+            fields = [s.download() for s in br2.solvers]
+            e2e_s = time.perf_counter() - t1
+            br2.close()
+        iters = [r["outer_iterations"] for r in res]
+        converged = sum(bool(r["converged"]) for r in res)
+        value = args.steps * n / (ms_total / 1e3)
+        h2d = sum(d.alpha.nbytes + d.gamma.nbytes for d in designs)
+        d2h = sum(sum(f[k].nbytes for k in ("u", "v", "p")) for f in fields)
+        e2e = {"value": n / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+        timing = {"device_ms_per_step": ms_total / args.steps, "wall_s_per_step": wall / args.steps}
+    else:
+        srv = serve.Server(mode=mode, precision=precision, device=device, visit=args.visit, max_outer=MAX_OUTER)
+        warm = [(0.0, d) for d in designs[: min(4, n)]]
+        for _ in range(args.warmup):
+            serve.Server(mode=mode, precision=precision, device=device, visit=100, max_outer=100).run(
+                warm, real_time=False)
+        with ClockSampler(device) as clocks:
+            st = srv.run(list(zip(arrivals, designs)), real_time=True)
+        dps = [r.dp for r in st.requests]
+        iters = [r.outer_iterations for r in st.requests]
+        converged = st.completed
+        lat = [1e3 * r.latency for r in st.requests]
+        launches = st.epochs
+        value = st.solves_per_s
+        e2e = {"value": st.solves_per_s, "unit": "solves/s",
+               "h2d_bytes_per_step": sum(d.alpha.nbytes + d.gamma.nbytes for d in designs),
+               "d2h_bytes_per_step": 8 * n}
+        timing = {"makespan_s": st.makespan_s, "device_ms": st.device_ms, "max_inflight": st.max_inflight,
+                  "peak_bytes": st.peak_bytes}
+    errs = [abs(a - r["dp"]) / abs(r["dp"]) for a, r in zip(dps, seq) if r["dp"] != 0]
+    seq_value = n / (seq_ms / 1e3) if args.workload == "mix" else n / (max(seq_lat[k] + 1e3 * arrivals[k]
+                                                                         for k in range(n)) / 1e3 - arrivals[0])
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if precision == cps.CPS_FP64 else "f32+f64", "data": "synthetic (seeded generator)",
+        "impl": "b200",
+        "config": dict(cfg, precision=args.precision, placement=mode, visit=args.visit, eps=EPS,
+                       converged=f"{converged}/{n}", warmup="visits of 100 outer iterations per design",
+                       l2="working set larger than L2 (all designs resident)"),
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "timing": timing,
+        "outer_iterations": {"total": int(sum(iters)), "min": int(min(iters)), "max": int(max(iters))},
+        "vs_plain_fp64_sequential": {
+            "value": seq_value, "speedup": value / seq_value if seq_value > 0 else None,
+            "device_ms": seq_ms, "latency_ms": {"p50": float(np.percentile(seq_lat, 50)),
+                                                "p99": float(np.percentile(seq_lat, 99))},
+            "outer_iterations_total": int(sum(r["iters"] for r in seq)),
+            "converged": f"{sum(r['converged'] for r in seq)}/{n}"},
+        "dp_rel_diff_vs_plain_fp64": {"max": float(max(errs)) if errs else None,
+                                      "median": float(np.median(errs)) if errs else None,
+                                      "note": "both stopped at the 1e-6 outer residual; see the parity tests "
+                                              "for the 1e-10 comparison"},
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary() if clocks is not None else None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 # Outer iterations of a converged FP64 solve of each workload, measured by the
 # bit-exact FP64 oracle (the reference's own arithmetic, 1e-6 outer residual).
 REFERENCE_ITERS = {"straight": 5564, "network": 9814}
@@ -378,11 +522,16 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="network", choices=["straight", "network", "density"])
+    ap.add_argument("--workload", default="network", choices=["straight", "network", "density", "mix", "served"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--cpu-sample-iters", type=int, default=200)
     ap.add_argument("--ref-sample-iters", type=int, default=300)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--designs", type=int, default=64, help="mix: designs of the 64-design mix to solve")
+    ap.add_argument("--requests", type=int, default=32, help="served: requests in the stream")
+    ap.add_argument("--visit", type=int, default=4096, help="mix/served: outer iterations per design per launch")
+    ap.add_argument("--placement", default="default",
+                    help='mix/served: JSON placement, e.g. \'{"group_ctas": 148}\' or \'{"tiles_per_cta": 8}\'')
     ap.add_argument("--max-outer", type=int, default=MAX_OUTER,
                     help="cap on outer iterations per solve (small profiling captures; the line then says converged=false)")
     args = ap.parse_args()
@@ -390,6 +539,8 @@ def main() -> None:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload in ("mix", "served"):
+        run_many(args)
     else:
         run_b200(args)
 

@@ -136,7 +136,10 @@ class BatchRunner:
         self.close()
 
     def run(self, eps: float = 1e-6, max_outer: int = 200000, visit: int = 4096, reset: bool = True):
-        """Returns (per-design results with total outer_iterations, device ms, launches)."""
+        """Returns (per-design results, device ms, launches).  Each result has
+        the design's total outer_iterations and finished_ms, the device time
+        from the start of the run to the end of the launch in which the design
+        left the batch (converged, failed or out of budget)."""
         if reset:
             for s in self.solvers:
                 s.reset_fields()
@@ -153,7 +156,7 @@ class BatchRunner:
             still = []
             for k, r in zip(active, res):
                 done[k] += r["n_done"]
-                results[k] = dict(r, outer_iterations=done[k])
+                results[k] = dict(r, outer_iterations=done[k], finished_ms=total_ms)
                 if not r["converged"] and r["status"] == 0 and done[k] < max_outer:
                     still.append(k)
             active = still
