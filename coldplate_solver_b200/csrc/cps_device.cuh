@@ -72,6 +72,10 @@ constexpr int kRedSlots = 4;    // ring of reduction slots (grid group)
 #define CPS_MIN_BLOCKS 2
 #endif
 constexpr int kStageDepth = 3;  // tiles whose shared-memory copies are in flight at once
+#ifndef CPS_RESIDENT_TILES
+#define CPS_RESIDENT_TILES 2
+#endif
+constexpr int kResidentTiles = CPS_RESIDENT_TILES;  // register-resident PCG up to this many tiles per CTA
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
 
 enum DeviceStatus : int { kStatusOk = 0, kStatusTimeout = 1, kStatusDiverged = 2 };
@@ -733,6 +737,119 @@ __device__ int pcg_two_reductions(const DesignView& d, Group& g, double* smem, d
 }
 
 // ---------------------------------------------------------------------------
+// The same PCG for groups in which a thread owns at most R unknowns (every
+// CTA has at most R tiles): each thread keeps its unknowns' x, r, z, p, Ap,
+// diagonal and face conductances in registers for the whole solve, so P2
+// reads no memory (it stores x for phase D and z for the neighbours) and P1
+// loads only the neighbours' z and p_{k-1} (and stores p_k for them).  The
+// arithmetic, the points' order and so every sum are those of
+// pcg_two_reductions.
+// ---------------------------------------------------------------------------
+template <typename T, int R, class Group>
+__device__ int pcg_resident(const DesignView& d, Group& g, double* smem, double rz0, double pAp0) {
+  const Inner<T>& w = inner<T>(d);
+  const int M = d.M, N = d.N, P = d.P;
+  const int tilesJ = (N - 1 + kTileJ - 1) / kTileJ;
+  const int tilesI = (M - 1 + kTileI - 1) / kTileI;
+  const int nt = tilesI * tilesJ;
+  const int ty = threadIdx.x >> 5, tx = threadIdx.x & 31;
+  bool on[R];
+  int ii[R], jj[R];
+  size_t oo[R];
+  T x[R], r[R], z[R], p[R], ap[R], dg[R], cE[R], cW[R], cN[R], cS[R];
+#pragma unroll
+  for (int u = 0; u < R; ++u) {
+    const int t = (int)g.rank + u * (int)g.nblk;
+    ii[u] = 1 + (t / tilesJ) * kTileI + ty;
+    jj[u] = 1 + (t % tilesJ) * kTileJ + tx;
+    on[u] = t < nt && ii[u] <= M - 1 && jj[u] <= N - 2;
+    oo[u] = on[u] ? (size_t)ii[u] * P + jj[u] : 0;
+    x[u] = r[u] = z[u] = p[u] = ap[u] = dg[u] = cE[u] = cW[u] = cN[u] = cS[u] = (T)0;
+    if (on[u]) {
+      const size_t o = oo[u];
+      x[u] = w.px[o];
+      r[u] = w.pr[o];
+      z[u] = w.pz[o];
+      p[u] = w.pp0[o];
+      ap[u] = w.pAp[o];
+      dg[u] = w.pdiag[o];
+      cE[u] = w.cx[o];
+      cN[u] = w.cy[o];
+      if (jj[u] > 1) cW[u] = w.cx[o - 1];
+      if (ii[u] > 1) cS[u] = w.cy[o - P];
+    }
+  }
+  double rz = rz0, beta = 0.0;
+  int it = 0;
+  for (; it < d.maxPIter; ++it) {
+    const T* pold = (it & 1) ? w.pp0 : w.pp1;  // p_{it-1}
+    T* pcur = (it & 1) ? w.pp1 : w.pp0;        // p_it
+    const double bt = beta;
+    double s1[1] = {pAp0};  // iteration 0's p = z, A p and p.Ap come from phase C
+    if (it > 0) {
+      s1[0] = 0.0;
+      T zn[R][4], pn[R][4];  // z and p_{k-1} at the S, W, E, N neighbours
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) zn[u][q] = pn[u][q] = (T)0;
+        if (on[u]) {
+          const size_t o = oo[u];
+          if (ii[u] > 1) { zn[u][0] = w.pz[o - P]; pn[u][0] = pold[o - P]; }
+          if (jj[u] > 1) { zn[u][1] = w.pz[o - 1]; pn[u][1] = pold[o - 1]; }
+          if (jj[u] + 1 <= N - 2) { zn[u][2] = w.pz[o + 1]; pn[u][2] = pold[o + 1]; }
+          if (ii[u] < M - 1) { zn[u][3] = w.pz[o + P]; pn[u][3] = pold[o + P]; }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < R; ++u) {
+        if (!on[u]) continue;
+        const int i = ii[u], j = jj[u];
+        // p = z + beta p (pressure_solver.cpp:181) at the point and its unknown neighbours
+        auto pk = [&](T zq, T pq) -> double { return (double)(T)((double)zq + bt * (double)pq); };
+        const double pc0 = pk(z[u], p[u]);
+        double Ap = 0.0;
+        if (i > 1) Ap += -(double)cS[u] * pk(zn[u][0], pn[u][0]);
+        if (j > 1) Ap += -(double)cW[u] * pk(zn[u][1], pn[u][1]);
+        Ap += (double)dg[u] * pc0;
+        if (j + 1 <= N - 2) Ap += -(double)cE[u] * pk(zn[u][2], pn[u][2]);
+        if (i < M - 1) Ap += -(double)cN[u] * pk(zn[u][3], pn[u][3]);
+        p[u] = (T)pc0;
+        pcur[oo[u]] = p[u];
+        ap[u] = (T)Ap;
+        s1[0] += pc0 * (double)ap[u];
+      }
+      if (!g.template sync_reduce<1, 0u>(s1, smem)) return -1;
+    }
+    const double pAp = s1[0];
+    if (fabs(pAp) < 1e-20) break;
+    const double alpha = rz / pAp;
+    double s2[2] = {0.0, 0.0};  // |r|^2, r.z
+#pragma unroll
+    for (int u = 0; u < R; ++u) {
+      if (!on[u]) continue;
+      x[u] = (T)((double)x[u] + alpha * (double)p[u]);
+      w.px[oo[u]] = x[u];
+      const T rt = (T)((double)r[u] - alpha * (double)ap[u]);
+      r[u] = rt;
+      const double rr = (double)rt;
+      s2[0] += rr * rr;
+      const double dgd = (double)dg[u];
+      const T zz = (T)((fabs(dgd) > 1e-20) ? rr / dgd : rr);
+      z[u] = zz;
+      w.pz[oo[u]] = zz;
+      s2[1] += rr * (double)zz;
+    }
+    if (!g.template sync_reduce<2, 0u>(s2, smem)) return -1;
+    if (sqrt(s2[0]) < d.pTol) break;
+    const double rzPrev = rz;
+    rz = s2[1];
+    beta = rz / rzPrev;
+  }
+  return it;
+}
+
+// ---------------------------------------------------------------------------
 // Single-reduction Jacobi-PCG (Chronopoulos-Gear recurrences), selected per
 // design by pcgSingleReduction: the same Krylov iterates as the reference's PCG in exact
 // arithmetic, with one grid-wide reduction per iteration instead of two.
@@ -1203,7 +1320,10 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
     if (its < 0) return -1;
     out[5] = its;
   } else {
-    const int its = pcg_two_reductions<T>(d, g, smem, rc[5], rc[6]);
+    const int tiles = ((M - 1 + kTileI - 1) / kTileI) * ((N - 1 + kTileJ - 1) / kTileJ);
+    const int its = (tiles <= kResidentTiles * (int)g.nblk)
+                        ? pcg_resident<T, kResidentTiles>(d, g, smem, rc[5], rc[6])
+                        : pcg_two_reductions<T>(d, g, smem, rc[5], rc[6]);
     if (its < 0) return -1;
     out[5] = its;
   }
