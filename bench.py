@@ -370,7 +370,10 @@ def run_b200(args) -> None:
         "e2e": {"value": world * e2e_steps / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "frac": (achieved / peak) if achieved else None,
+                     "traffic": MEASURED_TRAFFIC.get((args.workload, args.precision)),
+                     "traffic_source": "ncu launch list of the full workload (dram bytes per launch)"
+                     if (args.workload, args.precision) in MEASURED_TRAFFIC else None,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s",
                      "kernel": "cps_grid_kernel", "kernel_ms_per_launch": kernel_ms / max(1, launches),
                      "algorithmic_bytes_per_launch": alg_bytes / max(1, launches)},
@@ -388,10 +391,12 @@ def run_reference(args) -> None:
     if rank != 0:
         return
     from oracle import reference
-    if args.workload in ("mix", "served"):
-        print(json.dumps({"impl": "reference", "unavailable": "the reference's converged iteration counts on the "
-                          "many-design workloads are not precomputed (hours of CPU); its arm runs on the "
-                          "single-design workloads"}))
+    if args.workload == "served":
+        print(json.dumps({"impl": "reference", "unavailable": "a served stream is a GPU serving loop; the "
+                          "reference's CPU rate on the same designs is the mix arm's (--workload mix)"}))
+        return
+    if args.workload == "mix":
+        run_reference_mix(args)
         return
     design, cfg = workload(args.workload)
     if not reference.available("f64"):
@@ -409,6 +414,43 @@ def run_reference(args) -> None:
         "impl": "reference",
         "config": dict(cfg, outer_iterations_per_solve=done, converged=r["converged"],
                        ms_per_outer_iteration=r["ms_per_outer_iteration"]),
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_reference_mix(args) -> None:
+    """The reference on the seeded subsample of the mix whose converged counts
+    oracle/mix_counts.py recorded: each design solved from the zero state to
+    its 1e-6 stop on all host cores, or, past --ref-design-cap seconds,
+    extrapolated to its recorded count; solves/s = designs / summed time."""
+    from coldplate_solver_b200 import geometry as g
+    from oracle import reference
+    path = os.path.join(REPO, "oracle", "mix_reference_counts.json")
+    if not reference.available("f64") or not os.path.exists(path):
+        print(json.dumps({"impl": "reference", "unavailable": "needs oracle/_ref/ref_f64 and "
+                          "oracle/mix_reference_counts.json (python oracle/mix_counts.py)"}))
+        return
+    counts = json.load(open(path))
+    mix = g.batch_mix(64)
+    threads = host_cores()
+    reference.run(mix[counts["designs"][0]["k"]], 10, precision="f64", threads=threads)  # warm-up
+    rows, total = [], 0.0
+    for row in counts["designs"]:
+        r = reference_solve(mix[row["k"]], threads, row["iters"], 4, args.ref_design_cap)
+        t = 1.0 / r["value"]
+        total += t
+        rows.append({"k": row["k"], "M": row["M"], "N": row["N"], "seconds": t, "converged": r["converged"],
+                     "iters": r["iters"]})
+    value = len(rows) / total
+    sample = (f"{len(rows)} designs of the 64-design mix (seed {counts['subsample_seed']}), each solved to its own "
+              f"1e-6 stop or extrapolated after {args.ref_design_cap:.0f} s to the count recorded by "
+              f"oracle/mix_counts.py; solves/s = designs / summed time")
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 1, "steps": len(rows),
+        "warmup": 1, "ms_per_step": 1e3 * total / len(rows), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)", "impl": "reference",
+        "config": {"workload": "density_mix_subsample_of_64_nx256-1024", "designs": rows, "eps": EPS},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -543,6 +585,12 @@ def run_many(args) -> None:
         print(json.dumps(line), flush=True)
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
+# single-design kernel, from the one-pass ncu launch list of the full default
+# workload (`bench.py --steps 2 --warmup 3 --no-cpu-baseline`, 14 launches,
+# FP64); profiles/cps_grid_kernel_network_500x250_fp64.txt has the command.
+MEASURED_TRAFFIC = {("network", "fp64"): 1.249e9}
+
 # Outer iterations of a converged FP64 solve of each workload, measured by the
 # bit-exact FP64 oracle (the reference's own arithmetic, 1e-6 outer residual).
 REFERENCE_ITERS = {"straight": 5564, "network": 9814}
@@ -562,6 +610,8 @@ def main() -> None:
                     help="CPU baseline: seconds after which the reference's solve is extrapolated")
     ap.add_argument("--ref-time-cap", type=float, default=600.0,
                     help="reference arm: seconds after which an unfinished solve is extrapolated")
+    ap.add_argument("--ref-design-cap", type=float, default=45.0,
+                    help="reference arm, mix: seconds per design after which its solve is extrapolated")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--designs", type=int, default=64, help="mix: designs of the 64-design mix to solve")
     ap.add_argument("--requests", type=int, default=32, help="served: requests in the stream")
