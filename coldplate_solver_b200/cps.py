@@ -72,6 +72,12 @@ class CpsBatchOpts(ctypes.Structure):
                 ("tiles_per_cta", ctypes.c_int)]
 
 
+class CpsDpMonitor(ctypes.Structure):
+    _fields_ = [("gate", ctypes.c_int), ("window", ctypes.c_int), ("percent", ctypes.c_double),
+                ("slope_gate", ctypes.c_int), ("slope_window", ctypes.c_int), ("slope_max_delta", ctypes.c_double),
+                ("ramp_steps", ctypes.c_int), ("x_core_in", ctypes.c_double), ("x_core_out", ctypes.c_double)]
+
+
 class CpsBatchResult(ctypes.Structure):
     _fields_ = [("n_done", ctypes.c_int), ("converged", ctypes.c_int), ("status", ctypes.c_int),
                 ("last", CpsStepOut)]
@@ -101,6 +107,10 @@ SIGNATURES = {
     "cps_solve_noalloc": (ctypes.c_int, [ctypes.POINTER(CpsDesc), ctypes.c_int, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
                                          ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.POINTER(CpsStepOut),
                                          ctypes.POINTER(ctypes.c_int), _P]),
+    "cps_set_dp_monitor": (ctypes.c_int, [_P, ctypes.POINTER(CpsDpMonitor)]),
+    "cps_solve_monitored": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                           ctypes.POINTER(CpsStepOut), _D, ctypes.POINTER(ctypes.c_int),
+                                           ctypes.POINTER(ctypes.c_int)]),
     "cps_last_error": (ctypes.c_char_p, [_P]),
     "cps_version": (ctypes.c_char_p, []),
 }
@@ -260,6 +270,34 @@ class Solver:
             h = hist[k]
             out[k] = (h.residU, h.residV, h.residMass, h.residMassDof, h.err, h.pIters, h.uSweeps, h.vSweeps)
         return out
+
+    def set_dp_monitor(self, gate: bool = True, window: int = 500, percent: float = 1.0, slope_gate: bool = False,
+                       slope_window: int = 1000, slope_max_delta: float = 10.0, ramp_steps: int = 1000,
+                       x_core_in: float = 0.01, x_core_out: float = 0.05, enabled: bool = True) -> None:
+        """Attach the pressure-drop monitor/gate (cps_set_dp_monitor); the
+        defaults are the reference's (SIMPLE.h:88-89, 98-103, 346)."""
+        if not enabled:
+            self._check(self.lib.cps_set_dp_monitor(self.ctx, None))
+            return
+        m = CpsDpMonitor(gate=int(gate), window=window, percent=percent, slope_gate=int(slope_gate),
+                         slope_window=slope_window, slope_max_delta=slope_max_delta, ramp_steps=ramp_steps,
+                         x_core_in=x_core_in, x_core_out=x_core_out)
+        self._check(self.lib.cps_set_dp_monitor(self.ctx, ctypes.byref(m)))
+
+    def solve_monitored(self, max_outer: int, eps: float = 1e-6, inletVelocity: Optional[float] = None):
+        """cps_solve_monitored: returns (history (n, 8), pressure drops (n, 4):
+        core total, full total, core static, full static, dp_converged)."""
+        hist = (CpsStepOut * max(1, max_outer))()
+        dp = np.zeros((max(1, max_outer), 4))
+        nd, conv = ctypes.c_int(0), ctypes.c_int(0)
+        uin = self.inletVelocity if inletVelocity is None else inletVelocity
+        self._check(self.lib.cps_solve_monitored(self.ctx, uin, max_outer, eps, hist, _dptr(dp), ctypes.byref(nd),
+                                                 ctypes.byref(conv)))
+        out = np.zeros((nd.value, 8))
+        for k in range(nd.value):
+            h = hist[k]
+            out[k] = (h.residU, h.residV, h.residMass, h.residMassDof, h.err, h.pIters, h.uSweeps, h.vSweeps)
+        return out, dp[: nd.value].copy(), bool(conv.value)
 
     def sample_plane(self, x: float) -> np.ndarray:
         pl = CpsPlane()

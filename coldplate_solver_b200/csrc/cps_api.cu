@@ -64,7 +64,11 @@ struct cps_ctx {
   double* dplane = nullptr;
   double* hstage = nullptr;  // pinned, one plane of (M+1) x (N+1) doubles
   double* hhist = nullptr;   // pinned, kHistChunk * 8
-  int* hflags = nullptr;     // pinned: status, n_done
+  int* hflags = nullptr;     // pinned: status, n_done, pressure-drop gate
+  double* dplog = nullptr;   // device, kHistChunk x 4 pressure drops of the last launch
+  double* hdplog = nullptr;  // pinned copy
+  double* ddphist = nullptr; // device, the pressure-drop gate's windows (cudaMalloc'd by cps_set_dp_monitor)
+  int iter = 0;              // outer-loop iteration index of the next iteration (monitor and gate)
   int grid = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double kernel_ms = 0.0;
@@ -72,16 +76,20 @@ struct cps_ctx {
   std::string err;
 };
 
-template <typename T>
+// Monitor: the outer loop's pressure-drop monitor and gate compiled in (a
+// separate instantiation: compiling it into the plain kernel slowed every
+// outer iteration by 60 % on B200).
+template <typename T, bool Monitor>
 __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_grid_kernel(cps::DesignView d, cps::RunControl rc,
                                                                 cps::GridBarrier* bar, double* red) {
-  __shared__ double smem[cps::kRedWidth * 8];
+  __shared__ double smem[(Monitor ? cps::kPlaneSums : cps::kRedWidth) * 8];
   extern __shared__ __align__(16) char tile_smem[];
   cps::GridGroup g{bar, red, rc.status, blockIdx.x, gridDim.x, 0u, 0ull};
   for (int it = 0; it < rc.n_outer; ++it) {
     double out[8];
-    const int r = cps::outer_iteration<T>(d, g, smem, tile_smem, out, it + 1 == rc.n_outer, rc.stop_on_conv != 0,
-                                          rc.eps);
+    const int r = cps::outer_iteration<T, cps::GridGroup, Monitor>(
+        d, g, smem, tile_smem, out, it + 1 == rc.n_outer, rc.stop_on_conv != 0, rc.eps, rc.iter0 + it,
+        rc.dplog ? rc.dplog + (size_t)4 * it : nullptr, rc.dp_converged);
     if (r < 0) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       for (int k = 0; k < 8; ++k) rc.hist[(size_t)it * 8 + k] = out[k];
@@ -249,55 +257,11 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_wave_kernel
 // combined in a fixed tree order.
 __global__ void __launch_bounds__(cps::kThreads) cps_plane_kernel(cps::DesignView d, double xPhysical, double* out) {
   __shared__ double smem[cps::kRedWidth * 8];
-  const int M = d.M, N = d.N, P = d.P;
-  const double hx = d.hx, hy = d.hy, rho = d.rho;
-  const double xMin = 0.5 * hx, xMax = ((double)N - 0.5) * hx;
-  const double xClamped = cps::maxd(xMin, cps::mind(xPhysical, xMax));
-  const double jFloat = xClamped / hx - 0.5;
-  int colLeft = (int)floor(jFloat);
-  colLeft = colLeft < N - 2 ? colLeft : N - 2;
-  colLeft = 0 < colLeft ? colLeft : 0;
-  const int colRight = colLeft + 1;
-  const double xLeft = ((double)colLeft + 0.5) * hx, xRight = ((double)colRight + 0.5) * hx;
-  double t = (fabs(xRight - xLeft) < 1e-12) ? 0.0 : (xClamped - xLeft) / (xRight - xLeft);
-  t = cps::maxd(0.0, cps::mind(1.0, t));
+  const cps::PlaneSetup ps = cps::plane_setup(d, xPhysical);
   double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // staticAreaSum, dynAreaSum, totalWeighted, area, fluxSum
-  auto cl = [](int a, int lo, int hi) { return a < lo ? lo : (a > hi ? hi : a); };
-  for (int i = 1 + threadIdx.x; i < M; i += blockDim.x) {
-    const int cellRow = i - 1;
-    if (d.gamma[(size_t)cellRow * P + colLeft] < 1.0 - 1e-6 || d.gamma[(size_t)cellRow * P + colRight] < 1.0 - 1e-6)
-      continue;
-    const double faceArea = hy;
-    acc[3] += faceArea;
-    const int pL = cl(colLeft + 1, 0, N), pR = cl(colRight + 1, 0, N);
-    const double staticP = (1.0 - t) * d.p[(size_t)i * P + pL] + t * d.p[(size_t)i * P + pR];
-    const int uL = cl(colLeft, 0, N - 1), uR = cl(colRight, 0, N - 1);
-    const double uNormal = (1.0 - t) * d.u[(size_t)i * P + uL] + t * d.u[(size_t)i * P + uR];
-    const int vL = cl(colLeft, 0, N), vR = cl(colRight, 0, N);
-    const int vT = cl(i - 1, 0, M - 1), vB = cl(i, 0, M - 1);
-    const double vTop = (1.0 - t) * d.v[(size_t)vT * P + vL] + t * d.v[(size_t)vT * P + vR];
-    const double vBottom = (1.0 - t) * d.v[(size_t)vB * P + vL] + t * d.v[(size_t)vB * P + vR];
-    const double vTangential = 0.5 * (vTop + vBottom);
-    const double velMag = sqrt(uNormal * uNormal + vTangential * vTangential);
-    const double dynP = 0.5 * rho * velMag * velMag;
-    const double totalPAbs = staticP + dynP;
-    acc[0] += staticP * faceArea;
-    acc[1] += dynP * faceArea;
-    const double fluxAbs = fabs(rho * uNormal * faceArea);
-    if (fluxAbs > 0.0) {
-      acc[4] += fluxAbs;
-      acc[2] += totalPAbs * fluxAbs;
-    }
-  }
+  for (int i = 1 + threadIdx.x; i < d.M; i += blockDim.x) cps::plane_row(d, ps, i, acc);
   cps::block_reduce<5, 0u>(acc, smem);
-  if (threadIdx.x == 0) {
-    const double area = acc[3], fluxSum = acc[4];
-    double avgStatic = 0.0, avgDynamic = 0.0, avgTotal = 0.0, valid = 0.0;
-    if (area > 0.0) { avgStatic = acc[0] / area; avgDynamic = acc[1] / area; valid = 1.0; }
-    if (fluxSum > 0.0) avgTotal = acc[2] / fluxSum;
-    else if (area > 0.0) avgTotal = avgStatic + avgDynamic;
-    out[0] = area; out[1] = fluxSum; out[2] = avgStatic; out[3] = avgDynamic; out[4] = avgTotal; out[5] = valid;
-  }
+  if (threadIdx.x == 0) cps::plane_metrics(acc, out);
 }
 
 namespace {
@@ -324,8 +288,9 @@ size_t footprint_bytes(int M, int N, int precision, size_t* plane_elems_out, int
   size_t bytes = plane * sizeof(double) * kFieldPlanes;
   bytes += round_up(plane * elem_bytes(precision) * kInnerPlanes, 256);
   bytes += 256;                                                           // barrier + flags
-  bytes += (size_t)cps::kRedSlots * kMaxGridCtas * cps::kRedWidth * 8;    // reduction ring
+  bytes += (size_t)(cps::kRedSlots * cps::kRedWidth + cps::kPlaneSums) * kMaxGridCtas * 8;  // reduction ring
   bytes += (size_t)kHistChunk * 8 * 8 + 64;                               // history + plane metrics
+  bytes += (size_t)kHistChunk * 4 * 8;                                    // pressure-drop log
   return round_up(bytes, 256);
 }
 
@@ -393,8 +358,10 @@ void set_step_inputs(cps_ctx* c, double Uin) {
   c->view.maxVel = 3.0 * std::max(std::fabs(Uin), 0.1);  // iterations.cpp:104
 }
 
-const void* grid_kernel_for(int precision) {
-  return precision == CPS_MIXED ? (const void*)cps_grid_kernel<float> : (const void*)cps_grid_kernel<double>;
+const void* grid_kernel_for(int precision, bool monitor = false) {
+  if (monitor)
+    return precision == CPS_MIXED ? (const void*)cps_grid_kernel<float, true> : (const void*)cps_grid_kernel<double, true>;
+  return precision == CPS_MIXED ? (const void*)cps_grid_kernel<float, false> : (const void*)cps_grid_kernel<double, false>;
 }
 
 // Dynamic shared memory of the persistent kernels (tile staging buffers).
@@ -412,21 +379,29 @@ void to_step_out(const double* h, cps_step_out* o) {
   o->pIters = (int)h[5]; o->uSweeps = (int)h[6]; o->vSweeps = (int)h[7];
 }
 
-cps_status run(cps_ctx* c, int n_outer, int stop_on_conv, double eps, cps_step_out* hist, int* n_done) {
+cps_status run(cps_ctx* c, int n_outer, int stop_on_conv, double eps, cps_step_out* hist, int* n_done,
+               double* dp_history = nullptr, int* dp_converged = nullptr) {
   int done_total = 0;
+  const bool monitor = c->view.dpMonitor != 0;
+  if (dp_converged) *dp_converged = 0;
   while (done_total < n_outer) {
     const int chunk = std::min(kHistChunk, n_outer - done_total);
-    cps::RunControl rc{chunk, stop_on_conv, eps, c->dhist, c->dndone, c->dstatus};
-    if (!cuda_ok(c, cudaMemsetAsync(c->dndone, 0, sizeof(int), c->stream), "memset") ||
+    cps::RunControl rc{chunk, stop_on_conv, eps, c->dhist, c->dndone, c->dstatus, c->iter,
+                       monitor ? c->dplog : nullptr, c->dstatus + 2};
+    if (!cuda_ok(c, cudaMemsetAsync(c->dndone, 0, 2 * sizeof(int), c->stream), "memset") ||
         !cuda_ok(c, cudaMemsetAsync(c->bar, 0, sizeof(cps::GridBarrier), c->stream), "memset"))
       return CPS_ERR_CUDA;
     void* args[] = {&c->view, &rc, &c->bar, &c->red};
     if (!cuda_ok(c, cudaEventRecord(c->ev0, c->stream), "event")) return CPS_ERR_CUDA;
-    if (!cuda_ok(c, cudaLaunchCooperativeKernel(grid_kernel_for(c->precision), dim3(c->grid), dim3(cps::kThreads),
+    if (!cuda_ok(c, cudaLaunchCooperativeKernel(grid_kernel_for(c->precision, monitor), dim3(c->grid), dim3(cps::kThreads),
                                                 args, tile_smem_for(c->precision), c->stream), "cooperative launch"))
       return CPS_ERR_CUDA;
     if (!cuda_ok(c, cudaEventRecord(c->ev1, c->stream), "event")) return CPS_ERR_CUDA;
-    if (!cuda_ok(c, cudaMemcpyAsync(c->hflags, c->dstatus, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream), "d2h"))
+    if (!cuda_ok(c, cudaMemcpyAsync(c->hflags, c->dstatus, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->stream), "d2h"))
+      return CPS_ERR_CUDA;
+    if (monitor && dp_history &&
+        !cuda_ok(c, cudaMemcpyAsync(c->hdplog, c->dplog, sizeof(double) * 4 * chunk, cudaMemcpyDeviceToHost,
+                                    c->stream), "d2h"))
       return CPS_ERR_CUDA;
     if (!cuda_ok(c, cudaMemcpyAsync(c->hhist, c->dhist, sizeof(double) * 8 * chunk, cudaMemcpyDeviceToHost, c->stream),
                  "d2h"))
@@ -439,6 +414,9 @@ cps_status run(cps_ctx* c, int n_outer, int stop_on_conv, double eps, cps_step_o
     c->outer_done += nd;
     if (hist)
       for (int k = 0; k < nd; ++k) to_step_out(c->hhist + (size_t)8 * k, &hist[done_total + k]);
+    if (monitor && dp_history) std::memcpy(dp_history + (size_t)4 * done_total, c->hdplog, sizeof(double) * 4 * nd);
+    if (dp_converged && c->hflags[2]) *dp_converged = 1;
+    c->iter += nd;
     done_total += nd;
     if (n_done) *n_done = done_total;
     if (status != cps::kStatusOk) {
@@ -560,7 +538,8 @@ cps_status cps_create(const cps_desc* d, cps_ctx** out) {
   const size_t stage = (size_t)(d->M + 1) * (d->N + 1);
   if (!cuda_ok(c, cudaMallocHost(&c->hstage, stage * sizeof(double)), "pinned alloc") ||
       !cuda_ok(c, cudaMallocHost(&c->hhist, (size_t)kHistChunk * 8 * sizeof(double)), "pinned alloc") ||
-      !cuda_ok(c, cudaMallocHost(&c->hflags, 4 * sizeof(int)), "pinned alloc"))
+      !cuda_ok(c, cudaMallocHost(&c->hflags, 4 * sizeof(int)), "pinned alloc") ||
+      !cuda_ok(c, cudaMallocHost(&c->hdplog, sizeof(double) * 4 * kHistChunk), "pinned alloc"))
     return bail(CPS_ERR_OOM);
 
   char* tail = c->slab + c->plane_elems * sizeof(double) * kFieldPlanes +
@@ -569,8 +548,9 @@ cps_status cps_create(const cps_desc* d, cps_ctx** out) {
   c->dstatus = reinterpret_cast<int*>(tail + 64);  // [0] status, [1] n_done
   c->dndone = c->dstatus + 1;
   c->red = reinterpret_cast<double*>(tail + 256);
-  c->dhist = c->red + (size_t)cps::kRedSlots * kMaxGridCtas * cps::kRedWidth;
+  c->dhist = c->red + (size_t)(cps::kRedSlots * cps::kRedWidth + cps::kPlaneSums) * kMaxGridCtas;
   c->dplane = c->dhist + (size_t)kHistChunk * 8;
+  c->dplog = c->dplane + 8;
 
   cps::DesignView& v = c->view;
   v.M = d->M; v.N = d->N; v.P = c->P;
@@ -609,6 +589,7 @@ cps_status cps_create(const cps_desc* d, cps_ctx** out) {
   // Persistent grid: co-resident CTAs, at most one per tile of the design.
   int per_sm = 0, sms = 0;
   if (!allow_smem(c, grid_kernel_for(d->precision), tile_smem_for(d->precision)) ||
+      !allow_smem(c, grid_kernel_for(d->precision, true), tile_smem_for(d->precision)) ||
       !cuda_ok(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_kernel_for(d->precision),
                                                                 cps::kThreads, tile_smem_for(d->precision)),
                "occupancy") ||
@@ -635,6 +616,8 @@ void cps_destroy(cps_ctx* c) {
   if (c->hstage) cudaFreeHost(c->hstage);
   if (c->hhist) cudaFreeHost(c->hhist);
   if (c->hflags) cudaFreeHost(c->hflags);
+  if (c->hdplog) cudaFreeHost(c->hdplog);
+  if (c->ddphist) cudaFree(c->ddphist);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -657,6 +640,7 @@ cps_status cps_reset_fields(cps_ctx* c) {
   // Planes u .. dN are contiguous at the start of the slab.
   if (!cuda_ok(c, cudaMemsetAsync(c->slab, 0, c->plane_elems * sizeof(double) * (kDN + 1), c->stream), "memset"))
     return CPS_ERR_CUDA;
+  c->iter = 0;
   return CPS_OK;
 }
 
@@ -706,6 +690,55 @@ cps_status cps_solve(cps_ctx* c, double inletVelocity, int max_outer, double eps
   return run(c, max_outer, eps > 0.0 ? 1 : 0, eps, history, n_done);
 }
 
+cps_status cps_set_dp_monitor(cps_ctx* c, const cps_dp_monitor* m) {
+  if (!c) return fail(nullptr, CPS_ERR_ARG, "ctx is NULL");
+  if (!cuda_ok(c, cudaSetDevice(c->device), "cudaSetDevice")) return CPS_ERR_CUDA;
+  c->iter = 0;
+  if (!m) {
+    c->view.dpMonitor = 0;
+    c->view.dpGate = 0;
+    return CPS_OK;
+  }
+  if (m->window < 1 || m->slope_window < 0 || m->ramp_steps < 0 || !(m->percent >= 0.0))
+    return fail(c, CPS_ERR_ARG, "dp monitor: window >= 1, slope_window >= 0, ramp_steps >= 0, percent >= 0");
+  const size_t slots = (size_t)m->window + (size_t)(m->slope_gate ? m->slope_window : 0);
+  if (slots * sizeof(double) > tile_smem_for(c->precision))
+    return fail(c, CPS_ERR_ARG, "dp monitor: window + slope_window exceeds " +
+                                    std::to_string(tile_smem_for(c->precision) / sizeof(double)) + " values");
+  if (c->ddphist) cudaFree(c->ddphist);
+  c->ddphist = nullptr;
+  if (!cuda_ok(c, cudaMalloc(&c->ddphist, std::max<size_t>(slots, 1) * sizeof(double)), "cudaMalloc")) return CPS_ERR_OOM;
+  if (!cuda_ok(c, cudaMemset(c->ddphist, 0, std::max<size_t>(slots, 1) * sizeof(double)), "memset")) return CPS_ERR_CUDA;
+  cps::DesignView& v = c->view;
+  v.dpMonitor = 1;
+  v.dpGate = m->gate ? 1 : 0;
+  v.dpWindow = m->window;
+  v.dpSlopeGate = m->slope_gate ? 1 : 0;
+  v.dpSlopeWindow = m->slope_gate ? m->slope_window : 0;
+  v.dpRampSteps = m->ramp_steps;
+  v.dpPercent = m->percent;
+  v.dpSlopeMaxDelta = m->slope_max_delta;
+  v.xPlane[0] = m->x_core_in;
+  v.xPlane[1] = m->x_core_out;
+  v.xPlane[2] = 0.0;
+  v.xPlane[3] = (double)c->N * v.hx;  // domainXMax = N * hx (SIMPLE.cpp:250)
+  v.dpHist = c->ddphist;
+  return CPS_OK;
+}
+
+cps_status cps_solve_monitored(cps_ctx* c, double inletVelocity, int max_outer, double eps, cps_step_out* history,
+                               double* dp_history, int* n_done, int* dp_converged) {
+  if (!c) return fail(nullptr, CPS_ERR_ARG, "ctx is NULL");
+  if (max_outer < 0) return fail(c, CPS_ERR_ARG, "max_outer < 0");
+  if (!c->view.dpMonitor) return fail(c, CPS_ERR_ARG, "no pressure-drop monitor set (cps_set_dp_monitor)");
+  if (n_done) *n_done = 0;
+  if (dp_converged) *dp_converged = 0;
+  if (max_outer == 0) return CPS_OK;
+  if (!cuda_ok(c, cudaSetDevice(c->device), "cudaSetDevice")) return CPS_ERR_CUDA;
+  set_step_inputs(c, inletVelocity);
+  return run(c, max_outer, eps > 0.0 ? 1 : 0, eps, history, n_done, dp_history, dp_converged);
+}
+
 cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVelocity, const cps_batch_opts* opts,
                            cps_batch_result* results, double* kernel_ms) {
   if (!ctxs || n <= 0 || !opts || !results) return fail(nullptr, CPS_ERR_ARG, "ctxs, n > 0, opts and results required");
@@ -729,6 +762,7 @@ cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVeloc
     cps::BatchItem& it = ws->h_items[k];
     std::memset(&it, 0, sizeof(it));
     it.view = c->view;
+    it.view.dpMonitor = 0;  // the pressure-drop monitor runs in cps_solve/cps_solve_monitored only
     it.n_outer = opts->max_outer;
     it.stop_on_conv = opts->eps > 0.0 ? 1 : 0;
     it.eps = opts->eps;

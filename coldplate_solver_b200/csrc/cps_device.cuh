@@ -64,7 +64,8 @@ namespace cg = cooperative_groups;
 constexpr int kThreads = 256;   // 8 warps
 constexpr int kTileI = 8;       // tile rows (one warp per row)
 constexpr int kTileJ = 32;      // tile columns (one lane per column)
-constexpr int kRedWidth = 8;    // doubles per CTA per reduction
+constexpr int kRedWidth = 8;    // doubles per CTA per reduction slot
+constexpr int kPlaneSums = 20;  // the pressure-drop monitor's reduction (own ring region)
 constexpr int kRedSlots = 4;    // ring of reduction slots (grid group)
 // CTAs per SM the persistent kernels are compiled for (128 registers per
 // thread at 2).
@@ -108,6 +109,18 @@ struct DesignView {
   long long planeStride;                          // elements between coefficient planes
   Inner<double> f64;
   Inner<float> f32;
+  // Pressure-drop monitor and convergence gate of the outer loop (SIMPLE.cpp:269-408);
+  // dpMonitor = 0 leaves the iteration as calculateStep alone.
+  int dpMonitor;          // sample the four planes after every outer iteration
+  int dpGate;             // usePressureDropConvergence
+  int dpWindow;           // dpConvergenceWindow
+  int dpSlopeGate;        // usePressureDropSlopeGate
+  int dpSlopeWindow;      // dpSlopeWindowIters
+  int dpRampSteps;        // rampSteps: the dP history starts at this iteration
+  double dpPercent;       // dpConvergencePercent
+  double dpSlopeMaxDelta; // dpSlopeMaxDelta
+  double xPlane[4];       // core inlet, core outlet, x = 0, x = N hx
+  double* dpHist;         // dpWindow circular slots, then dpSlopeWindow slots (slot = iter mod window)
 };
 
 template <typename T> __device__ __forceinline__ const Inner<T>& inner(const DesignView& d);
@@ -122,6 +135,9 @@ struct RunControl {
   double* hist;       // n_outer x 8: residU, residV, residMass, residMassDof, err, pIters, uSweeps, vSweeps
   int* n_done;        // outer iterations completed by this launch
   int* status;        // DeviceStatus
+  int iter0;          // the outer loop's iteration index of this launch's first iteration
+  double* dplog;      // n_outer x 4 (core total, full total, core static, full static dP) or null
+  int* dp_converged;  // set when the pressure-drop gate stopped the loop
 };
 
 // One entry of the batched (cluster) kernel's work list.
@@ -272,7 +288,17 @@ struct GridGroup {
   // __syncwarp in warp 0) to the whole CTA.
   template <int K, unsigned MaxMask>
   __device__ bool sync_reduce(double (&v)[K], double* smem) {
-    __shared__ double s_res[kRedWidth];
+    static_assert(K <= kRedWidth, "ring slots hold kRedWidth values per CTA");
+    double* slot = red + (size_t)(redCount % kRedSlots) * nblk * kRedWidth;
+    ++redCount;
+    return sync_reduce_at<K, MaxMask>(v, smem, slot);
+  }
+
+  // The same with the CTA partials in a region of K * nblk values of the
+  // caller's choosing (one that no reduction in flight can be using).
+  template <int K, unsigned MaxMask>
+  __device__ bool sync_reduce_at(double (&v)[K], double* smem, double* slot) {
+    __shared__ double s_res[kPlaneSums];
     __shared__ int s_ok;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
@@ -287,8 +313,6 @@ struct GridGroup {
 #pragma unroll
       for (int k = 0; k < K; ++k) smem[k * 8 + warp] = v[k];
     }
-    double* slot = red + (size_t)(redCount % kRedSlots) * nblk * kRedWidth;
-    ++redCount;
     ++epoch;
     __syncthreads();
     if (warp == 0) {
@@ -1232,6 +1256,184 @@ __device__ bool mass_phase(const DesignView& d, Group& g, double* smem, char* tb
   return g.template sync_reduce<7, 0x1Fu>(rc, smem);
 }
 
+// ---------------------------------------------------------------------------
+// samplePlaneAtX (postprocessing.cpp:62-230), split into the interpolation
+// set-up of a plane, one row's five contributions and the metrics from the
+// five sums (staticAreaSum, dynAreaSum, totalWeighted, area, fluxSum).
+// ---------------------------------------------------------------------------
+struct PlaneSetup {
+  int colLeft, colRight;
+  double t;
+};
+
+__device__ __forceinline__ PlaneSetup plane_setup(const DesignView& d, double xPhysical) {
+  const int N = d.N;
+  const double hx = d.hx;
+  const double xMin = 0.5 * hx, xMax = ((double)N - 0.5) * hx;
+  const double xClamped = maxd(xMin, mind(xPhysical, xMax));
+  const double jFloat = xClamped / hx - 0.5;
+  int colLeft = (int)floor(jFloat);
+  colLeft = colLeft < N - 2 ? colLeft : N - 2;
+  colLeft = 0 < colLeft ? colLeft : 0;
+  const int colRight = colLeft + 1;
+  const double xLeft = ((double)colLeft + 0.5) * hx, xRight = ((double)colRight + 0.5) * hx;
+  double t = (fabs(xRight - xLeft) < 1e-12) ? 0.0 : (xClamped - xLeft) / (xRight - xLeft);
+  t = maxd(0.0, mind(1.0, t));
+  return PlaneSetup{colLeft, colRight, t};
+}
+
+// Row i (1..M-1) of the plane, added into acc in the reference's order.
+__device__ __forceinline__ void plane_row(const DesignView& d, const PlaneSetup& s, int i, double* acc) {
+  const int M = d.M, N = d.N, P = d.P;
+  const double hy = d.hy, rho = d.rho, t = s.t;
+  const int colLeft = s.colLeft, colRight = s.colRight;
+  auto cl = [](int a, int lo, int hi) { return a < lo ? lo : (a > hi ? hi : a); };
+  const int cellRow = i - 1;
+  if (d.gamma[(size_t)cellRow * P + colLeft] < 1.0 - 1e-6 || d.gamma[(size_t)cellRow * P + colRight] < 1.0 - 1e-6)
+    return;
+  const double faceArea = hy;
+  acc[3] += faceArea;
+  const int pL = cl(colLeft + 1, 0, N), pR = cl(colRight + 1, 0, N);
+  const double staticP = (1.0 - t) * d.p[(size_t)i * P + pL] + t * d.p[(size_t)i * P + pR];
+  const int uL = cl(colLeft, 0, N - 1), uR = cl(colRight, 0, N - 1);
+  const double uNormal = (1.0 - t) * d.u[(size_t)i * P + uL] + t * d.u[(size_t)i * P + uR];
+  const int vL = cl(colLeft, 0, N), vR = cl(colRight, 0, N);
+  const int vT = cl(i - 1, 0, M - 1), vB = cl(i, 0, M - 1);
+  const double vTop = (1.0 - t) * d.v[(size_t)vT * P + vL] + t * d.v[(size_t)vT * P + vR];
+  const double vBottom = (1.0 - t) * d.v[(size_t)vB * P + vL] + t * d.v[(size_t)vB * P + vR];
+  const double vTangential = 0.5 * (vTop + vBottom);
+  const double velMag = sqrt(uNormal * uNormal + vTangential * vTangential);
+  const double dynP = 0.5 * rho * velMag * velMag;
+  const double totalPAbs = staticP + dynP;
+  acc[0] += staticP * faceArea;
+  acc[1] += dynP * faceArea;
+  const double fluxAbs = fabs(rho * uNormal * faceArea);
+  if (fluxAbs > 0.0) {
+    acc[4] += fluxAbs;
+    acc[2] += totalPAbs * fluxAbs;
+  }
+}
+
+// out: area, fluxSum, avgStatic, avgDynamic, avgTotal, valid (PlaneMetrics)
+__device__ __forceinline__ void plane_metrics(const double* acc, double* out) {
+  const double area = acc[3], fluxSum = acc[4];
+  double avgStatic = 0.0, avgDynamic = 0.0, avgTotal = 0.0, valid = 0.0;
+  if (area > 0.0) { avgStatic = acc[0] / area; avgDynamic = acc[1] / area; valid = 1.0; }
+  if (fluxSum > 0.0) avgTotal = acc[2] / fluxSum;
+  else if (area > 0.0) avgTotal = avgStatic + avgDynamic;
+  out[0] = area; out[1] = fluxSum; out[2] = avgStatic; out[3] = avgDynamic; out[4] = avgTotal; out[5] = valid;
+}
+
+// ---------------------------------------------------------------------------
+// After an outer iteration: the four planes (core inlet/outlet, x = 0 and
+// x = N hx, SIMPLE.cpp:338-344) sampled by the whole group, the four
+// pressure drops (:347-353) and the pressure-drop convergence gate
+// (:356-408).  Rows are spread over the group's threads and the twenty sums
+// reduced once, so every CTA holds the same drops and evaluates the gate
+// identically: the history slots are a function of the iteration index
+// (value k of the window goes to slot k mod window, the slope window holds
+// the last dpSlopeWindow iterations) and CTA 0 writes this iteration's slots.
+// The window statistics are the reference's formulas; their sums are grouped
+// in a fixed lane-strided order, as the plane sums are.  Returns false when a
+// wait failed.
+// ---------------------------------------------------------------------------
+template <class Group>
+__device__ bool dp_phase(const DesignView& d, Group& g, double* smem, char* tbuf, int iter, double* dplog,
+                         bool& converged) {
+  PlaneSetup ps[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) ps[q] = plane_setup(d, d.xPlane[q]);
+  double acc[kPlaneSums];
+#pragma unroll
+  for (int k = 0; k < kPlaneSums; ++k) acc[k] = 0.0;
+  const int first = (int)g.rank * kThreads + (int)threadIdx.x, step = (int)g.nblk * kThreads;
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    for (int i = 1 + first; i <= d.M - 1; i += step) plane_row(d, ps[q], i, acc + 5 * q);
+  // the plane sums use the ring region after the kRedSlots slots, which no
+  // other reduction touches
+  if (!g.template sync_reduce_at<kPlaneSums, 0u>(acc, smem, g.red + (size_t)kRedSlots * g.nblk * kRedWidth))
+    return false;
+  double m[4][6];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) plane_metrics(acc + 5 * q, m[q]);
+  const double coreTotal = m[0][4] - m[1][4], fullTotal = m[2][4] - m[3][4];
+  const double coreStatic = m[0][2] - m[1][2], fullStatic = m[2][2] - m[3][2];
+  const bool writer = g.rank == 0 && threadIdx.x == 0;
+  if (writer && dplog) {
+    dplog[0] = coreTotal;
+    dplog[1] = fullTotal;
+    dplog[2] = coreStatic;
+    dplog[3] = fullStatic;
+  }
+  converged = false;
+  const int W = d.dpWindow, S = d.dpSlopeWindow;
+  const bool slope = d.dpSlopeGate && S > 0;
+  const double v = coreTotal;
+  if (d.dpGate && iter >= d.dpRampSteps && iter - d.dpRampSteps + 1 >= W) {
+    // Warp 0 evaluates the statistics: lane-strided sums in a fixed order and a
+    // warp tree (deterministic, the same in every CTA), the window values staged
+    // in shared memory once; the other warps wait at one barrier.
+    __shared__ int s_conv;
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x < 32) {
+      double* win = reinterpret_cast<double*>(tbuf);
+      double* sl = win + W;
+      const int cur = (iter - d.dpRampSteps) % W;
+      const bool slopeFull = slope && iter + 1 >= S;
+      for (int k = lane; k < W; k += 32) win[k] = (k == cur) ? v : __ldcg(d.dpHist + k);
+      if (slopeFull)
+        for (int k = lane; k < S; k += 32) sl[k] = (k == S - 1) ? v : __ldcg(d.dpHist + W + (iter - S + 1 + k) % S);
+      __syncwarp();
+      auto warp_sum = [](double x) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+        return x;
+      };
+      double sum = 0.0;
+      for (int k = lane; k < W; k += 32) sum += win[k];
+      const double mean = warp_sum(sum) / double(W);
+      double varSum = 0.0;
+      for (int k = lane; k < W; k += 32) {
+        const double diff = win[k] - mean;
+        varSum += diff * diff;
+      }
+      const double stdDev = sqrt(warp_sum(varSum) / double(W));
+      const double denom = maxd(fabs(mean), 1.0);
+      const double stdPercent = (stdDev / denom) * 100.0;
+      const double latestDeltaPercent = (fabs(v - mean) / denom) * 100.0;
+      bool slopeGatePassed = true;
+      if (slopeFull) {
+        // least-squares slope over (iteration - first iteration, dP), SIMPLE.cpp:276-294
+        double sumX = 0.0, sumY = 0.0, sumXX = 0.0, sumXY = 0.0;
+        for (int k = lane; k < S; k += 32) {
+          const double x = (double)k, y = sl[k];
+          sumX += x;
+          sumY += y;
+          sumXX += x * x;
+          sumXY += x * y;
+        }
+        sumX = warp_sum(sumX);
+        sumY = warp_sum(sumY);
+        sumXX = warp_sum(sumXX);
+        sumXY = warp_sum(sumXY);
+        const double n = (double)S;
+        const double den = n * sumXX - sumX * sumX;
+        const double slopeVal = (fabs(den) < 1e-12) ? 0.0 : (n * sumXY - sumX * sumY) / den;
+        slopeGatePassed = fabs(slopeVal) <= d.dpSlopeMaxDelta / (double)S;
+      }
+      if (lane == 0) s_conv = (stdPercent < d.dpPercent && latestDeltaPercent < d.dpPercent && slopeGatePassed) ? 1 : 0;
+    }
+    __syncthreads();
+    converged = s_conv != 0;
+  }
+  if (writer) {
+    if (slope) d.dpHist[W + iter % S] = v;
+    if (d.dpGate && iter >= d.dpRampSteps) d.dpHist[(iter - d.dpRampSteps) % W] = v;
+  }
+  return true;
+}
+
 // Dynamic shared memory a persistent kernel needs for storage type T.
 template <typename T>
 constexpr size_t tile_smem_bytes() {
@@ -1244,14 +1446,19 @@ constexpr size_t tile_smem_bytes() {
 
 // ---------------------------------------------------------------------------
 // One outer iteration for one design on group g; out[8] receives the step
-// diagnostics.  tbuf: tile_smem_bytes<T>() of shared memory.  Returns 0 to
-// continue with another outer iteration, 1 when this one is the last
-// (iteration budget, convergence, or a non-finite residual), -1 when the group
-// must stop because a device-side wait failed.
+// diagnostics.  tbuf: tile_smem_bytes<T>() of shared memory.  With Monitor
+// (compiled in for the single-design kernel only) and d.dpMonitor, iter is the
+// outer loop's iteration index, dplog (may be null)
+// receives its four pressure drops and *dpConverged is set when the
+// pressure-drop gate ends the loop.  Returns 0 to continue with another outer
+// iteration, 1 when this one is the last (iteration budget, convergence, the
+// pressure-drop gate, or a non-finite residual), -1 when the group must stop
+// because a device-side wait failed.
 // ---------------------------------------------------------------------------
-template <typename T, class Group>
+template <typename T, class Group, bool Monitor = false>
 __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char* tbuf, double (&out)[8],
-                               bool lastIter, bool stopOnConv, double eps) {
+                               bool lastIter, bool stopOnConv, double eps, int iter = 0, double* dplog = nullptr,
+                               int* dpConverged = nullptr) {
   const Inner<T>& w = inner<T>(d);
   const int M = d.M, N = d.N, P = d.P;
   // ---- A: assembly + sweep 1 ----
@@ -1329,6 +1536,15 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
   }
   // ---- D: pressure and velocity correction ----
   correct_fields<T>(d, g, tbuf);
+  if constexpr (Monitor) {
+    if (d.dpMonitor) {
+      // ---- pressure-drop monitor and gate; its reduction is the barrier before the next A ----
+      bool gateStop = false;
+      if (!g.sync() || !dp_phase(d, g, smem, tbuf, iter, dplog, gateStop)) return -1;
+      if (gateStop && dpConverged && g.rank == 0 && threadIdx.x == 0) *dpConverged = 1;
+      return (stop || gateStop) ? 1 : 0;
+    }
+  }
   if (!stop) return g.sync() ? 0 : -1;
   return 1;
 }

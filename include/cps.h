@@ -151,6 +151,42 @@ cps_status cps_get_stream(cps_ctx* ctx, void** stream);
 cps_status cps_kernel_timing(cps_ctx* ctx, double* kernel_ms, long long* launches, long long* outer_iterations,
                              int reset);
 
+/* Pressure-drop monitor and convergence gate of the outer loop
+ * (SIMPLE::runIterations, SIMPLE.cpp:269-408): after every outer iteration the
+ * four planes core inlet/outlet, x = 0 and x = N hx are sampled as
+ * samplePlaneAtX does (postprocessing.cpp:97-230) and, with gate set, the loop
+ * stops once the core total-pressure drop settles: over the last `window`
+ * values (collected from iteration ramp_steps on) std/|mean| and
+ * |latest - mean|/|mean| (|mean| floored at 1) are both below percent %, and,
+ * with slope_gate, the least-squares slope over the last slope_window
+ * iterations is at most slope_max_delta / slope_window. */
+typedef struct {
+  int    gate;             /* usePressureDropConvergence (SIMPLE.h:98) */
+  int    window;           /* dpConvergenceWindow (SIMPLE.h:99) */
+  double percent;          /* dpConvergencePercent (SIMPLE.h:100) */
+  int    slope_gate;       /* usePressureDropSlopeGate (SIMPLE.h:101) */
+  int    slope_window;     /* dpSlopeWindowIters (SIMPLE.h:102) */
+  double slope_max_delta;  /* dpSlopeMaxDelta (SIMPLE.h:103) */
+  int    ramp_steps;       /* rampSteps (SIMPLE.h:346): the window starts at this iteration */
+  double x_core_in;        /* xPlaneCoreInlet [m] */
+  double x_core_out;       /* xPlaneCoreOutlet [m] */
+} cps_dp_monitor;
+
+/* Attach (m != NULL) or detach (NULL) the pressure-drop monitor of ctx and
+ * restart the outer-loop iteration count at 0 (as does cps_reset_fields).
+ * window + slope_window is limited by the kernel's shared memory (reported in
+ * the error message when exceeded). */
+cps_status cps_set_dp_monitor(cps_ctx* ctx, const cps_dp_monitor* m);
+
+/* cps_solve with the monitor attached: also fills dp_history (may be NULL;
+ * max_outer x 4 doubles: core total, full total, core static, full static
+ * pressure drop of each iteration, the columns of the reference's
+ * pressure_drop_history.txt) and sets *dp_converged when the gate ended the
+ * loop.  The residual stop (eps > 0) and the gate both apply, as in the
+ * reference's loop condition. */
+cps_status cps_solve_monitored(cps_ctx* ctx, double inletVelocity, int max_outer, double eps, cps_step_out* history,
+                               double* dp_history, int* n_done, int* dp_converged);
+
 /* Options of a batched solve. */
 typedef struct {
   int cluster_ctas;   /* CTAs of the thread-block cluster that runs one design (1..16; 0 = 8) */

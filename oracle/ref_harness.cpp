@@ -163,7 +163,7 @@ int main(int argc, char** argv) {
   try {
     auto recs = read_records(argv[1]);
     const int M = geti(recs, "M"), N = geti(recs, "N");
-    const int mode = geti(recs, "mode");  // 0 = iterate, 1 = build alpha from gamma only
+    const int mode = geti(recs, "mode");  // 0 = iterate, 1 = build alpha from gamma only, 2 = runIterations
     // The constructor reads these two files from ./ExportFiles (SIMPLE.cpp:19-21).
     mkdir("ExportFiles", 0755);
     {
@@ -231,7 +231,42 @@ int main(int argc, char** argv) {
     std::vector<double> hU, hV, hMass, hMassDof, hErr;
     std::vector<int32_t> hP, hJu, hJv;
     double elapsed = 0.0;
-    for (int it = 0; it < maxOuter; ++it) {
+    if (mode == 2) {
+      // The reference's own outer loop with its pressure-drop gate (SIMPLE.cpp:237-449); the
+      // residual test is switched off (epsilon = 0) so that only the gate or maxIterations ends it.
+      s.usePressureDropConvergence = true;
+      s.dpConvergenceWindow = geti(recs, "dpWindow");
+      s.dpConvergencePercent = static_cast<real>(getd(recs, "dpPercent"));
+      s.usePressureDropSlopeGate = geti(recs, "dpSlopeGate") != 0;
+      s.dpSlopeWindowIters = geti(recs, "dpSlopeWindow");
+      s.dpSlopeMaxDelta = static_cast<real>(getd(recs, "dpSlopeMaxDelta"));
+      s.rampSteps = geti(recs, "rampSteps");
+      s.enableInletRamp = false;
+      s.xPlaneCoreInlet = static_cast<real>(getd(recs, "xCoreIn"));
+      s.xPlaneCoreOutlet = static_cast<real>(getd(recs, "xCoreOut"));
+      s.maxIterations = maxOuter;
+      s.epsilon = 0;
+      auto t0 = std::chrono::steady_clock::now();
+      s.runIterations();
+      elapsed = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      // its per-iteration log: iter, core total, full total, core static, full static dP
+      std::vector<int32_t> dpIter;
+      std::vector<double> dp;
+      FILE* f = std::fopen("ExportFiles/pressure_drop_history.txt", "r");
+      if (!f) throw std::runtime_error("no pressure_drop_history.txt");
+      char line[512];
+      if (!std::fgets(line, sizeof line, f)) line[0] = 0;  // header
+      int it;
+      double a, b, c, e;
+      while (std::fscanf(f, "%d %lf %lf %lf %lf", &it, &a, &b, &c, &e) == 5) {
+        dpIter.push_back(it);
+        dp.insert(dp.end(), {a, b, c, e});
+      }
+      std::fclose(f);
+      w.i("dpIter", dpIter);
+      w.d("dp", dp);
+    }
+    for (int it = 0; mode == 0 && it < maxOuter; ++it) {
       s.inletVelocity = s.targetVel;  // SIMPLE.cpp:303-307 with the inlet ramp off
       g_sweep_counts.clear();
       int pIt = 0;

@@ -78,6 +78,37 @@ def run(design, max_outer: int, precision: str = "f64", eps: float = 1e-6, stop_
     return out
 
 
+def run_iterations(design, max_iterations: int, window: int, percent: float, ramp_steps: int,
+                   slope_gate: bool = False, slope_window: int = 0, slope_max_delta: float = 0.0,
+                   x_core=(0.01, 0.05), precision: str = "f64", threads: int = 1,
+                   timeout: float = 3600) -> Dict[str, np.ndarray]:
+    """The reference's own SIMPLE::runIterations (SIMPLE.cpp:237-449) with its
+    pressure-drop gate on and the residual test off (epsilon = 0): returns its
+    per-iteration pressure-drop log (``dpIter``; ``dp`` (n, 4): core total,
+    full total, core static, full static, as pressure_drop_history.txt prints
+    them, 6 significant digits) and the final fields."""
+    if not available(precision):
+        raise FileNotFoundError(f"{binary(precision)} not built (make -C oracle ref)")
+    with tempfile.TemporaryDirectory(prefix="cps_ref_") as tmp:
+        cpath, opath = os.path.join(tmp, "case.bin"), os.path.join(tmp, "out.bin")
+        rec = case_records(design, max_iterations, 0.0, False, threads, None, mode=2, x_core=x_core)
+        rec.update({"dpWindow": [int(window)], "dpPercent": [float(percent)], "dpSlopeGate": [int(slope_gate)],
+                    "dpSlopeWindow": [int(slope_window)], "dpSlopeMaxDelta": [float(slope_max_delta)],
+                    "rampSteps": [int(ramp_steps)]})
+        casefile.write_records(cpath, rec)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        proc = subprocess.run([binary(precision), cpath, opath], cwd=tmp, env=env, stdout=subprocess.DEVNULL,
+                              stderr=subprocess.PIPE, timeout=timeout)
+        if proc.returncode != 0:
+            raise RuntimeError(f"reference harness failed: {proc.stderr.decode()[-2000:]}")
+        out = casefile.read_records(opath)
+    M, N = design.M, design.N
+    for k, s in {"u": (M + 1, N), "v": (M, N + 1), "p": (M + 1, N + 1)}.items():
+        out[k] = out[k].reshape(s)
+    out["dp"] = out["dp"].reshape(-1, 4)
+    return out
+
+
 def build_alpha(gamma: np.ndarray, kmin: float = 1e-14, q: float = 1.0, precision: str = "f64", eta: float = 0.00089):
     """The reference's own buildAlphaFromDensity (SIMPLE.cpp:589-630) on
     ``gamma`` with alpha_max = eta / kmin (SIMPLE.cpp:65-66); returns (alpha, gamma)."""

@@ -9,6 +9,7 @@ reference's index space: u/uStar/dE (M+1, N), v/vStar/dN (M, N+1), p/pStar
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 import subprocess
 from typing import Dict, Optional
@@ -123,3 +124,63 @@ def build_alpha(gamma: np.ndarray, alpha_max: float, q: float, precision: str = 
     fn(ctypes.c_int(g.shape[0]), ctypes.c_int(g.shape[1]), ctypes.c_double(alpha_max), ctypes.c_double(q),
        _ptr(g), _ptr(a))
     return a, g
+
+
+def dp_gate_solve(design, fields: Dict[str, np.ndarray], max_outer: int, window: int, percent: float,
+                  ramp_steps: int, slope_gate: bool = False, slope_window: int = 0, slope_max_delta: float = 0.0,
+                  x_core=(0.01, 0.05), precision: str = "f64"):
+    """The outer loop of SIMPLE::runIterations (SIMPLE.cpp:269-408) with the
+    residual test off: one outer iteration, the four planes (core inlet and
+    outlet, x = 0, x = N hx), the four pressure drops, then the pressure-drop
+    window and slope gate, until the gate passes or ``max_outer``.  Returns
+    (dp (n, 4): core total, full total, core static, full static; converged)."""
+    xs = (x_core[0], x_core[1], 0.0, design.N * design.hx)
+    hist = [0.0] * window      # dpHistory, slot k
+    idx, filled = 0, False
+    slope_buf = []             # (iter, value), oldest first
+    rows = []
+    for it in range(max_outer):
+        step(design, fields, precision, stop_after=3)
+        m = [sample_plane(design, fields, x, precision) for x in xs]
+        core, full = m[0][4] - m[1][4], m[2][4] - m[3][4]
+        rows.append((core, full, m[0][2] - m[1][2], m[2][2] - m[3][2]))
+        if slope_gate and slope_window > 0:
+            slope_buf.append((it, core))
+            if len(slope_buf) > slope_window:
+                slope_buf.pop(0)
+        if it >= ramp_steps:
+            hist[idx] = core
+            idx = (idx + 1) % window
+            if idx == 0:
+                filled = True
+            if filled:
+                s = 0.0
+                for k in range(window):
+                    s += hist[k]
+                mean = s / float(window)
+                var = 0.0
+                for k in range(window):
+                    dd = hist[k] - mean
+                    var += dd * dd
+                std = math.sqrt(var / float(window))
+                denom = max(abs(mean), 1.0)
+                std_pct = (std / denom) * 100.0
+                latest = hist[(idx - 1 + window) % window]
+                delta_pct = (abs(latest - mean) / denom) * 100.0
+                ok = True
+                if slope_gate and slope_window > 0 and len(slope_buf) >= slope_window:
+                    x0 = float(slope_buf[0][0])
+                    sx = sy = sxx = sxy = 0.0
+                    n = float(len(slope_buf))
+                    for (xi, yi) in slope_buf:
+                        x = float(xi) - x0
+                        sx += x
+                        sy += yi
+                        sxx += x * x
+                        sxy += x * yi
+                    den = n * sxx - sx * sx
+                    slope = 0.0 if abs(den) < 1e-12 else (n * sxy - sx * sy) / den
+                    ok = abs(slope) <= slope_max_delta / float(slope_window)
+                if std_pct < percent and delta_pct < percent and ok:
+                    return np.array(rows), True
+    return np.array(rows), False

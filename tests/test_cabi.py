@@ -43,6 +43,8 @@ def test_struct_layout_matches_c():
 int main(void) {
   printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(cps_desc), offsetof(cps_desc, precision), offsetof(cps_desc, alpha),
          offsetof(cps_desc, grid_ctas), sizeof(cps_step_out), offsetof(cps_step_out, vSweeps), sizeof(cps_plane));
+  printf("%zu %zu %zu %zu %zu\n", sizeof(cps_batch_opts), offsetof(cps_batch_opts, tiles_per_cta),
+         sizeof(cps_dp_monitor), offsetof(cps_dp_monitor, ramp_steps), offsetof(cps_dp_monitor, x_core_out));
   return 0;
 }'''
     with tempfile.TemporaryDirectory() as t:
@@ -52,7 +54,8 @@ int main(void) {
         vals = list(map(int, subprocess.run([exe], capture_output=True, text=True).stdout.split()))
     py = [ctypes.sizeof(cps.CpsDesc), cps.CpsDesc.precision.offset, cps.CpsDesc.alpha.offset,
           cps.CpsDesc.grid_ctas.offset, ctypes.sizeof(cps.CpsStepOut), cps.CpsStepOut.vSweeps.offset,
-          ctypes.sizeof(cps.CpsPlane)]
+          ctypes.sizeof(cps.CpsPlane), ctypes.sizeof(cps.CpsBatchOpts), cps.CpsBatchOpts.tiles_per_cta.offset,
+          ctypes.sizeof(cps.CpsDpMonitor), cps.CpsDpMonitor.ramp_steps.offset, cps.CpsDpMonitor.x_core_out.offset]
     assert vals == py
 
 
