@@ -78,6 +78,12 @@ class CpsDpMonitor(ctypes.Structure):
                 ("ramp_steps", ctypes.c_int), ("x_core_in", ctypes.c_double), ("x_core_out", ctypes.c_double)]
 
 
+class CpsCaseParams(ctypes.Structure):
+    _fields_ = [("M", ctypes.c_int), ("N", ctypes.c_int), ("hx", ctypes.c_double), ("hy", ctypes.c_double),
+                ("U_in", ctypes.c_double), ("N_in_buffer", ctypes.c_int), ("N_out_buffer", ctypes.c_int),
+                ("Ht", ctypes.c_double), ("has_Ht", ctypes.c_int)]
+
+
 class CpsBatchResult(ctypes.Structure):
     _fields_ = [("n_done", ctypes.c_int), ("converged", ctypes.c_int), ("status", ctypes.c_int),
                 ("last", CpsStepOut)]
@@ -111,6 +117,14 @@ SIGNATURES = {
     "cps_solve_monitored": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                            ctypes.POINTER(CpsStepOut), _D, ctypes.POINTER(ctypes.c_int),
                                            ctypes.POINTER(ctypes.c_int)]),
+    "cps_read_case_params": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(CpsCaseParams)]),
+    "cps_read_geometry": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _D, _D,
+                                         ctypes.POINTER(ctypes.c_int)]),
+    "cps_read_restart": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _D, _D, _D,
+                                        ctypes.POINTER(ctypes.c_int)]),
+    "cps_save_all": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D, _D, ctypes.c_int]),
+    "cps_io_last_error": (ctypes.c_char_p, []),
     "cps_last_error": (ctypes.c_char_p, [_P]),
     "cps_version": (ctypes.c_char_p, []),
 }

@@ -257,6 +257,44 @@ cps_status cps_solve_noalloc(const cps_desc* desc, int pitch, const double* alph
 /* Device bytes held by a context created from desc (admission control). */
 cps_status cps_footprint(const cps_desc* desc, unsigned long long* bytes);
 
+/* ---- The reference's files at the boundary (host code, no GPU) ---- */
+
+/* fluid_params.txt as SIMPLE::loadParameters reads it (SIMPLE.cpp:31-47):
+ * "M N hy hx U_in N_in_buffer N_out_buffer [Ht ...]". */
+typedef struct {
+  int M, N;
+  double hx, hy, U_in;
+  int N_in_buffer, N_out_buffer;
+  double Ht;       /* the optional out-of-plane height */
+  int has_Ht;
+} cps_case_params;
+cps_status cps_read_case_params(const char* path, cps_case_params* out);
+
+/* geometry_fluid.txt as loadTopology + loadDensityField read it
+ * (SIMPLE.cpp:517-584): M x N cellType values (0 fluid, 1 solid), row-major
+ * into cellType and/or gamma = 1 - cellType (either may be NULL); a missing
+ * file means all fluid (CPS_OK, message in cps_io_last_error) and a short
+ * one stops at its end (*values_read, may be NULL, counts what was read). */
+cps_status cps_read_geometry(const char* path, int M, int N, double* cellType, double* gamma, int* values_read);
+
+/* Restart matrices dir/u.txt ((M+1) x N), v.txt (M x (N+1)), p.txt
+ * ((M+1) x (N+1)), row-major, as the restart loader reads them
+ * (SIMPLE.cpp:203-226): a missing or incomplete file leaves its matrix zero;
+ * *loaded (may be NULL) counts the complete ones. */
+cps_status cps_read_restart(const char* dir, int M, int N, double* u, double* v, double* p, int* loaded);
+
+/* SIMPLE::saveAll (output.cpp:73-266) into dir: u, v, p (staggered),
+ * u_full, v_full, pressure_full (cell-centred), u_thermal, v_thermal,
+ * pressure_thermal, p_gradient (without the inlet/outlet buffer columns) as
+ * tab-separated text, and fluid_results.vtk; numbers printed as the
+ * reference prints them.  cellType may be NULL (then 1 - gamma). */
+cps_status cps_save_all(const char* dir, int M, int N, double hx, double hy, int N_in_buffer, int N_out_buffer,
+                        const double* u, const double* v, const double* p, const double* cellType,
+                        const double* gamma, const double* alpha, int layout);
+
+/* Message of the last failed (or warning) file call on this thread. */
+const char* cps_io_last_error(void);
+
 /* Message of the last failed call on ctx (or of the last failed cps_create
  * on this thread when ctx is NULL). */
 const char* cps_last_error(const cps_ctx* ctx);

@@ -163,7 +163,39 @@ int main(int argc, char** argv) {
   try {
     auto recs = read_records(argv[1]);
     const int M = geti(recs, "M"), N = geti(recs, "N");
-    const int mode = geti(recs, "mode");  // 0 = iterate, 1 = build alpha from gamma only, 2 = runIterations
+    const int mode = geti(recs, "mode");  // 0 = iterate, 1 = alpha from gamma, 2 = runIterations, 3 = files
+    if (mode == 3) {
+      // The reference's own file handling on files the caller put in ./ExportFiles:
+      // the constructor reads fluid_params.txt and geometry_fluid.txt and builds
+      // gamma and alpha (SIMPLE.cpp:18-29); with a "restart" record the restart
+      // loader reads ./restart/{u,v,p}.txt (SIMPLE.cpp:203-232); with "save" the
+      // fields given as records are written by saveAll (output.cpp:73-266).
+      SIMPLE s;
+      Writer w(argv[2]);
+      w.matrix("cellType", s.cellType);
+      w.matrix("gamma", s.gamma);  // after buildAlphaFromDensity's wall rows
+      w.matrix("alpha", s.alpha);
+      if (recs.count("restart")) {
+        s.reuseInitialFields = true;
+        s.restartDirectory = "restart";
+        s.initializeMemory();
+      }
+      if (recs.count("save")) {
+        load_grid(recs, "u0", s.u);
+        load_grid(recs, "v0", s.v);
+        load_grid(recs, "p0", s.p);
+        s.saveAll();
+      }
+      w.i("MN", {s.M, s.N, s.N_in_buffer, s.N_out_buffer});
+      w.d("params", {static_cast<double>(s.hx), static_cast<double>(s.hy), static_cast<double>(s.targetVel),
+                     static_cast<double>(s.Ht_channel)});
+      s.loadDensityField();  // gamma as the file gives it (SIMPLE.cpp:556-584)
+      w.matrix("gammaLoaded", s.gamma);
+      w.matrix("u", s.u);
+      w.matrix("v", s.v);
+      w.matrix("p", s.p);
+      return 0;
+    }
     // The constructor reads these two files from ./ExportFiles (SIMPLE.cpp:19-21).
     mkdir("ExportFiles", 0755);
     {

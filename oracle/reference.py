@@ -109,6 +109,55 @@ def run_iterations(design, max_iterations: int, window: int, percent: float, ram
     return out
 
 
+def run_io(files: Dict[str, str], restart: Optional[Dict[str, str]] = None,
+           save: Optional[Dict[str, np.ndarray]] = None, precision: str = "f64", timeout: float = 600) -> dict:
+    """The reference's own file handling (harness mode 3): ``files``
+    (ExportFiles/fluid_params.txt, geometry_fluid.txt as text) are read by its
+    constructor; ``restart`` ({u,v,p}.txt texts) by its restart loader; with
+    ``save`` (u, v, p arrays) its saveAll writes ExportFiles.  Returns what it
+    read (M, N, buffers, hx, hy, U_in, Ht, cellType, gamma after the wall rows
+    of buildAlphaFromDensity, gammaLoaded = as loadDensityField leaves it,
+    alpha, u, v, p)
+    and ``written``: every file left in ExportFiles, as text."""
+    if not available(precision):
+        raise FileNotFoundError(f"{binary(precision)} not built (make -C oracle ref)")
+    with tempfile.TemporaryDirectory(prefix="cps_ref_io_") as tmp:
+        os.makedirs(os.path.join(tmp, "ExportFiles"))
+        for name, text in files.items():
+            with open(os.path.join(tmp, "ExportFiles", name), "w") as f:
+                f.write(text)
+        rec = {"M": [0], "N": [0], "mode": [3], "threads": [1]}
+        if restart is not None:
+            os.makedirs(os.path.join(tmp, "restart"))
+            for name, text in restart.items():
+                with open(os.path.join(tmp, "restart", name), "w") as f:
+                    f.write(text)
+            rec["restart"] = [1]
+        if save is not None:
+            rec["save"] = [1]
+            rec["u0"], rec["v0"], rec["p0"] = save["u"], save["v"], save["p"]
+        cpath, opath = os.path.join(tmp, "case.bin"), os.path.join(tmp, "out.bin")
+        casefile.write_records(cpath, rec)
+        proc = subprocess.run([binary(precision), cpath, opath], cwd=tmp, stdout=subprocess.DEVNULL,
+                              stderr=subprocess.PIPE, timeout=timeout, env=dict(os.environ, OMP_NUM_THREADS="1"))
+        if proc.returncode != 0:
+            raise RuntimeError(f"reference harness failed: {proc.stderr.decode()[-2000:]}")
+        out = casefile.read_records(opath)
+        written = {}
+        for name in sorted(os.listdir(os.path.join(tmp, "ExportFiles"))):
+            if name not in files:
+                with open(os.path.join(tmp, "ExportFiles", name)) as f:
+                    written[name] = f.read()
+    M, N, nin, nout = (int(x) for x in out["MN"])
+    hx, hy, uin, ht = (float(x) for x in out["params"])
+    res = {"M": M, "N": N, "N_in_buffer": nin, "N_out_buffer": nout, "hx": hx, "hy": hy, "U_in": uin, "Ht": ht,
+           "written": written}
+    for k, shape in {"cellType": (M, N), "gamma": (M, N), "gammaLoaded": (M, N), "alpha": (M, N),
+                     "u": (M + 1, N), "v": (M, N + 1), "p": (M + 1, N + 1)}.items():
+        res[k] = out[k].reshape(shape)
+    return res
+
+
 def build_alpha(gamma: np.ndarray, kmin: float = 1e-14, q: float = 1.0, precision: str = "f64", eta: float = 0.00089):
     """The reference's own buildAlphaFromDensity (SIMPLE.cpp:589-630) on
     ``gamma`` with alpha_max = eta / kmin (SIMPLE.cpp:65-66); returns (alpha, gamma)."""

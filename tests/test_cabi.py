@@ -45,6 +45,8 @@ int main(void) {
          offsetof(cps_desc, grid_ctas), sizeof(cps_step_out), offsetof(cps_step_out, vSweeps), sizeof(cps_plane));
   printf("%zu %zu %zu %zu %zu\n", sizeof(cps_batch_opts), offsetof(cps_batch_opts, tiles_per_cta),
          sizeof(cps_dp_monitor), offsetof(cps_dp_monitor, ramp_steps), offsetof(cps_dp_monitor, x_core_out));
+  printf("%zu %zu %zu\n", sizeof(cps_case_params), offsetof(cps_case_params, N_in_buffer),
+         offsetof(cps_case_params, has_Ht));
   return 0;
 }'''
     with tempfile.TemporaryDirectory() as t:
@@ -55,7 +57,8 @@ int main(void) {
     py = [ctypes.sizeof(cps.CpsDesc), cps.CpsDesc.precision.offset, cps.CpsDesc.alpha.offset,
           cps.CpsDesc.grid_ctas.offset, ctypes.sizeof(cps.CpsStepOut), cps.CpsStepOut.vSweeps.offset,
           ctypes.sizeof(cps.CpsPlane), ctypes.sizeof(cps.CpsBatchOpts), cps.CpsBatchOpts.tiles_per_cta.offset,
-          ctypes.sizeof(cps.CpsDpMonitor), cps.CpsDpMonitor.ramp_steps.offset, cps.CpsDpMonitor.x_core_out.offset]
+          ctypes.sizeof(cps.CpsDpMonitor), cps.CpsDpMonitor.ramp_steps.offset, cps.CpsDpMonitor.x_core_out.offset,
+          ctypes.sizeof(cps.CpsCaseParams), cps.CpsCaseParams.N_in_buffer.offset, cps.CpsCaseParams.has_Ht.offset]
     assert vals == py
 
 
