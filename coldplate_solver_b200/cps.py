@@ -48,6 +48,7 @@ class CpsDesc(ctypes.Structure):
         ("alpha", ctypes.POINTER(ctypes.c_double)), ("gamma", ctypes.POINTER(ctypes.c_double)),
         ("layout", ctypes.c_int), ("device", ctypes.c_int), ("grid_ctas", ctypes.c_int),
         ("pcg_variant", ctypes.c_int),
+        ("momentum_explicit", ctypes.c_int),
     ]
 
 
@@ -173,7 +174,7 @@ def make_desc(design: Design, precision: int = CPS_FP64, device: int = 0, grid_c
                 enableConvectionScaling=int(design.enableConvectionScaling), Ht_channel=design.Ht_channel,
                 twoPointFiveDSinkMultiplier=design.twoPointFiveDSinkMultiplier, precision=precision,
                 alpha=_dptr(alpha), gamma=_dptr(gamma), layout=CPS_ROW_MAJOR, device=device, grid_ctas=grid_ctas,
-                pcg_variant=pcg_variant)
+                pcg_variant=pcg_variant, momentum_explicit=int(design.momentumSolverType == 0))
     return d, (alpha, gamma)
 
 

@@ -308,6 +308,8 @@ cps_status validate(const cps_desc* d) {
   if (d->grid_ctas < 0) return fail(nullptr, CPS_ERR_ARG, "grid_ctas < 0");
   if (d->pcg_variant != CPS_PCG_REFERENCE && d->pcg_variant != CPS_PCG_SINGLE_REDUCTION)
     return fail(nullptr, CPS_ERR_ARG, "bad pcg_variant");
+  if (d->momentum_explicit != 0 && d->momentum_explicit != 1)
+    return fail(nullptr, CPS_ERR_ARG, "momentum_explicit must be 0 (implicit Jacobi) or 1 (explicit)");
   return CPS_OK;
 }
 
@@ -556,6 +558,7 @@ cps_status cps_create(const cps_desc* d, cps_ctx** out) {
   v.M = d->M; v.N = d->N; v.P = c->P;
   v.conv = d->convectionScheme; v.maxPIter = d->maxPressureIter; v.maxMomIter = d->maxMomentumIter;
   v.pcgSingleReduction = d->pcg_variant == CPS_PCG_SINGLE_REDUCTION ? 1 : 0;
+  v.momExplicit = d->momentum_explicit;
   v.hx = d->hx; v.hy = d->hy; v.rho = d->rho; v.uvAlpha = d->uvAlpha; v.pAlpha = d->pAlpha; v.pTol = d->pTol;
   // Derived constants, evaluated in the reference's operation order
   // (momentum_solver.cpp:166-191, 220-222, 261; jacobi_solver.cpp:41, 63).

@@ -101,6 +101,7 @@ struct DesignView {
   int M, N, P;
   int conv, maxPIter, maxMomIter;
   int pcgSingleReduction;  // 1: single-reduction PCG recurrences; 0: the reference's two-reduction PCG
+  int momExplicit;         // 1: explicit point update of the momentum (momentumSolverType = 0)
   double hx, hy, rho, uvAlpha, pAlpha, pTol;
   double vol, De, Dn, sinkDiag, Fcx, Fcy, relax;  // Fcx = cs*rho*hy, Fcy = cs*rho*hx, relax = (1-uvA)/uvA
   double thrU, thrV;                              // momTol^2 * nU, momTol^2 * nV
@@ -663,6 +664,65 @@ __device__ __forceinline__ double assemble_point(const DesignView& d, const Layo
   }
   (IsU ? w.xU1 : w.xV1)[o] = (T)(velCur + r / aP);
   return r * r;
+}
+
+// The explicit momentum update at one unknown (momentumSolverType = 0,
+// iterations.cpp:254-412, pseudo-transient off so the transient coefficient
+// is rho vol / inf = 0): the full coefficients, one point update from the
+// current velocities, clamped to +-maxVel; d = h / max(aP0, 1e-12).  Its
+// result goes where phase C reads the final Jacobi iterate (FP64: the value;
+// mixed: its difference to the current velocity).
+template <bool IsU, typename T>
+__device__ __forceinline__ void explicit_point(const DesignView& d, const LayoutA& L, int i, int j) {
+  constexpr bool kMixed = sizeof(T) == 4;
+  const Inner<T>& w = inner<T>(d);
+  const int P = d.P;
+  const auto& u = L.u;
+  const auto& v = L.v;
+  const double mv = d.maxVel;
+  auto clampv = [&](double x) { return maxd(-mv, mind(mv, x)); };  // std::max(-maxVel, std::min(maxVel, x))
+  double alphaLocal, ue, uw, vn, vs;
+  if (IsU) {
+    alphaLocal = 0.5 * (L.a(i - 1, j - 1) + L.a(i - 1, j));
+    ue = clampv(0.5 * (u(i, j) + u(i, j + 1)));
+    uw = clampv(0.5 * (u(i, j - 1) + u(i, j)));
+    vn = clampv(0.5 * (v(i, j) + v(i, j + 1)));
+    vs = clampv(0.5 * (v(i - 1, j) + v(i - 1, j + 1)));
+  } else {
+    alphaLocal = 0.5 * (L.a(i - 1, j - 1) + L.a(i, j - 1));
+    ue = clampv(0.5 * (u(i, j) + u(i + 1, j)));
+    uw = clampv(0.5 * (u(i, j - 1) + u(i + 1, j - 1)));
+    vn = clampv(0.5 * (v(i, j) + v(i + 1, j)));
+    vs = clampv(0.5 * (v(i - 1, j) + v(i, j)));
+  }
+  const double Fe = d.Fcx * ue, Fw = d.Fcx * uw, Fn = d.Fcy * vn, Fs = d.Fcy * vs;
+  const double aE = d.De + maxd(0.0, -Fe), aW = d.De + maxd(0.0, Fw);
+  const double aN = d.Dn + maxd(0.0, -Fn), aS = d.Dn + maxd(0.0, Fs);
+  const auto& X = IsU ? u : v;
+  const double Sdc = (d.conv == 1) ? sou_correction<IsU>(d, X, i, j, Fe, Fw, Fn, Fs) : 0.0;
+  const double sumA = aE + aW + aN + aS;
+  const double transCoeffLocal = 0.0;
+  const double brinkmanDrag = alphaLocal * d.vol;
+  double aP0 = sumA + (Fe - Fw + Fn - Fs) + transCoeffLocal + d.sinkDiag + brinkmanDrag;
+  aP0 = maxd(aP0, 1e-10);
+  const double dDenom = maxd(aP0, 1e-12);
+  const size_t o = (size_t)i * P + j;
+  const double velCur = X(i, j);
+  double Sp;
+  if (IsU) {
+    d.dE[o] = d.hy / dDenom;
+    Sp = (L.p(i, j) - L.p(i, j + 1)) * d.hy;
+  } else {
+    d.dN[o] = d.hx / dDenom;
+    Sp = (L.p(i, j) - L.p(i + 1, j)) * d.hx;
+  }
+  Sp += transCoeffLocal * velCur;
+  Sp += Sdc;
+  const double aP = aP0 / d.uvAlpha;
+  Sp += d.relax * aP0 * velCur;
+  double xNew = (aE * X(i, j + 1) + aW * X(i, j - 1) + aN * X(i + 1, j) + aS * X(i - 1, j) + Sp) / aP;
+  xNew = clampv(xNew);
+  (IsU ? w.xU0 : w.xV0)[o] = kMixed ? (T)(xNew - velCur) : (T)xNew;
 }
 
 // ---------------------------------------------------------------------------
@@ -1461,8 +1521,9 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
                                int* dpConverged = nullptr) {
   const Inner<T>& w = inner<T>(d);
   const int M = d.M, N = d.N, P = d.P;
-  // ---- A: assembly + sweep 1 ----
-  const bool anySweep = d.maxMomIter > 0;
+  // ---- A: assembly + sweep 1 (or the explicit update) ----
+  const bool expl = d.momExplicit != 0;
+  const bool anySweep = !expl && d.maxMomIter > 0;
   double red2[2] = {0.0, 0.0};
   for_each_tile<LayoutA>(
       d, g.rank, g.nblk, tbuf,
@@ -1474,6 +1535,11 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
       },
       [&](const LayoutA& L, int i, int j, bool inside) {
         if (!inside) return;
+        if (expl) {
+          if (j <= N - 2) explicit_point<true, T>(d, L, i, j);
+          if (i <= M - 2) explicit_point<false, T>(d, L, i, j);
+          return;
+        }
         if (j <= N - 2) red2[0] += assemble_point<true, T>(d, L, i, j, anySweep);
         if (i <= M - 2) red2[1] += assemble_point<false, T>(d, L, i, j, anySweep);
       });

@@ -132,6 +132,7 @@ extern "C" cps_status cps_solve_noalloc(const cps_desc* desc, int pitch, const d
   cps::DesignView w = {};
   w.M = d.M; w.N = d.N; w.P = pitch;
   w.conv = d.convectionScheme; w.maxPIter = d.maxPressureIter; w.maxMomIter = d.maxMomentumIter;
+  w.momExplicit = d.momentum_explicit != 0 ? 1 : 0;
   w.hx = d.hx; w.hy = d.hy; w.rho = d.rho; w.uvAlpha = d.uvAlpha; w.pAlpha = d.pAlpha; w.pTol = d.pTol;
   w.vol = d.hx * d.hy;
   w.De = d.eta * d.hy / d.hx;

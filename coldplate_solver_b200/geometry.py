@@ -70,6 +70,7 @@ class Design:
     maxPressureIter: int = 20  # SIMPLE.h:152
     momentumTol: float = 1e-5  # SIMPLE.h:176
     maxMomentumIter: int = 200  # SIMPLE.h:177
+    momentumSolverType: int = 1  # SIMPLE.h:172 (0 explicit point update, 1 implicit Jacobi)
     name: str = "design"
 
     def __post_init__(self) -> None:
@@ -99,8 +100,8 @@ class Design:
 
     def int_params(self) -> np.ndarray:
         return np.array([self.M, self.N, self.convectionScheme, int(self.enableTwoPointFiveD),
-                         int(self.enableConvectionScaling), self.maxPressureIter, self.maxMomentumIter],
-                        dtype=np.int32)
+                         int(self.enableConvectionScaling), self.maxPressureIter, self.maxMomentumIter,
+                         self.momentumSolverType], dtype=np.int32)
 
     def real_params(self) -> np.ndarray:
         return np.array([self.hx, self.hy, self.rho, self.eta, self.uvAlpha, self.pAlpha, self.inletVelocity,

@@ -59,6 +59,7 @@ void ensure_device(SIMPLE& s) {
   d.momentumTol = s.momentumTol;
   d.maxMomentumIter = s.maxMomentumIter;
   d.convectionScheme = s.convectionScheme;
+  d.momentum_explicit = s.momentumSolverType == 0 ? 1 : 0;
   d.enableTwoPointFiveD = s.enableTwoPointFiveD ? 1 : 0;
   d.enableConvectionScaling = s.enableConvectionScaling ? 1 : 0;
   d.Ht_channel = s.Ht_channel;

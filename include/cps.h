@@ -73,6 +73,9 @@ typedef struct {
   int pcg_variant;                /* CPS_PCG_REFERENCE (two reductions per iteration, as
                                      pressure_solver.cpp:121-184) or CPS_PCG_SINGLE_REDUCTION
                                      (Chronopoulos-Gear recurrences: one reduction per iteration) */
+  int momentum_explicit;          /* 0: implicit Jacobi momentum (momentumSolverType = 1, SIMPLE.h:172);
+                                     1: the explicit point update (momentumSolverType = 0,
+                                     iterations.cpp:176-441, pseudo-transient off) */
 } cps_desc;
 
 /* PCG recurrences (same Krylov iterates in exact arithmetic). */

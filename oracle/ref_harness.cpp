@@ -244,7 +244,7 @@ int main(int argc, char** argv) {
     s.momentumTol = static_cast<real>(getd(recs, "momTol"));
     s.maxMomentumIter = geti(recs, "maxMomIter");
     s.pressureSolverType = recs.count("solverType") ? geti(recs, "solverType") : 1;  // 1 = Parallel CG
-    s.momentumSolverType = 1;           // implicit Jacobi (iterations.cpp:109)
+    s.momentumSolverType = recs.count("momType") ? geti(recs, "momType") : 1;  // iterations.cpp:109
     s.enablePseudoTimeStepping = false; // SIMPLE.h:262 default
     s.usePressureDropConvergence = false;
     s.saveStateInterval = 0;

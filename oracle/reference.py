@@ -42,7 +42,8 @@ def case_records(design, max_outer: int, eps: float = 1e-6, stop_on_conv: bool =
         "convScale": [int(design.enableConvectionScaling)], "sinkMult": [design.twoPointFiveDSinkMultiplier],
         "uvAlpha": [design.uvAlpha], "pAlpha": [design.pAlpha], "pTol": [design.pTol],
         "maxPIter": [design.maxPressureIter], "momTol": [design.momentumTol],
-        "maxMomIter": [design.maxMomentumIter], "maxOuter": [max_outer], "stopOnConv": [int(stop_on_conv)],
+        "maxMomIter": [design.maxMomentumIter], "momType": [int(design.momentumSolverType)],
+        "maxOuter": [max_outer], "stopOnConv": [int(stop_on_conv)],
         "eps": [eps], "xCoreIn": [x_core[0]], "xCoreOut": [x_core[1]],
         "alpha": design.alpha, "gamma": design.gamma,
     }

@@ -30,13 +30,13 @@ static inline REAL FN(min_)(REAL a, REAL b) { return (b < a) ? b : a; }
 static inline REAL FN(clamp_)(REAL v, REAL lo, REAL hi) { return (v < lo) ? lo : (hi < v) ? hi : v; }
 
 typedef struct {
-  int M, N, conv, twoFiveD, convScale, maxPIter, maxMomIter;
+  int M, N, conv, twoFiveD, convScale, maxPIter, maxMomIter, momType;
   REAL hx, hy, rho, eta, uvAlpha, pAlpha, Uin, Ht, sinkMult, pTol, momTol;
 } FN(params);
 
 static void FN(unpack)(const int* ip, const double* dp, FN(params) * s) {
   s->M = ip[0]; s->N = ip[1]; s->conv = ip[2]; s->twoFiveD = ip[3]; s->convScale = ip[4];
-  s->maxPIter = ip[5]; s->maxMomIter = ip[6];
+  s->maxPIter = ip[5]; s->maxMomIter = ip[6]; s->momType = ip[7];
   s->hx = (REAL)dp[0]; s->hy = (REAL)dp[1]; s->rho = (REAL)dp[2]; s->eta = (REAL)dp[3];
   s->uvAlpha = (REAL)dp[4]; s->pAlpha = (REAL)dp[5]; s->Uin = (REAL)dp[6]; s->Ht = (REAL)dp[7];
   s->sinkMult = (REAL)dp[8]; s->pTol = (REAL)dp[9]; s->momTol = (REAL)dp[10];
@@ -238,6 +238,78 @@ static int FN(momentum)(const FN(params) * s, int isU, const REAL* u, const REAL
   return iter;
 }
 
+/* The explicit momentum update of calculateStep with momentumSolverType = 0
+ * and the pseudo-transient term off (iterations.cpp:176-441): one point update
+ * per unknown from the current velocities with the full coefficients, clamped
+ * to +-maxVel; d = h / max(aP0, 1e-12).  Writes xStar and d at the unknowns;
+ * *resid = max |xNew - vel|. */
+static void FN(momentum_explicit)(const FN(params) * s, int isU, const REAL* u, const REAL* v, const REAL* p,
+                                  const REAL* alpha, REAL* xStar, REAL* d, REAL* resid) {
+  const int M = s->M, N = s->N;
+  const REAL hx = s->hx, hy = s->hy, vol = hx * hy, rho = s->rho, eta = s->eta;
+  const int i1 = isU ? M - 1 : M - 2, j1 = isU ? N - 2 : N - 1;
+  const int xc = isU ? N : N + 1;
+  const REAL* x_old = isU ? u : v;
+#define U_(a, b) u[(a) * N + (b)]
+#define V_(a, b) v[(a) * (N + 1) + (b)]
+#define P_(a, b) p[(a) * (N + 1) + (b)]
+#define A_(a, b) alpha[(a) * N + (b)]
+  const REAL maxVel = (REAL)3 * FN(max_)((REAL)fabs(s->Uin), (REAL)0.1);
+  const REAL convScale = s->convScale ? ((REAL)6 / (REAL)7) : (REAL)1;                 /* :233 */
+  const REAL sinkCoeff = (s->twoFiveD && s->Ht > 0) ? s->sinkMult * ((REAL)5 * eta / ((REAL)2 * s->Ht * s->Ht)) : (REAL)0;
+  const REAL sinkDiag = sinkCoeff * vol;                                                 /* :240 */
+  REAL res = 0;
+  for (int i = 1; i <= i1; ++i)
+    for (int j = 1; j <= j1; ++j) {
+      REAL alphaLocal, ue, uw, vn, vs;
+      if (isU) { /* :262-271 */
+        alphaLocal = (REAL)0.5 * (A_(i - 1, j - 1) + A_(i - 1, j));
+        ue = FN(max_)(-maxVel, FN(min_)(maxVel, (REAL)0.5 * (U_(i, j) + U_(i, j + 1))));
+        uw = FN(max_)(-maxVel, FN(min_)(maxVel, (REAL)0.5 * (U_(i, j - 1) + U_(i, j))));
+        vn = FN(max_)(-maxVel, FN(min_)(maxVel, (REAL)0.5 * (V_(i, j) + V_(i, j + 1))));
+        vs = FN(max_)(-maxVel, FN(min_)(maxVel, (REAL)0.5 * (V_(i - 1, j) + V_(i - 1, j + 1))));
+      } else { /* :350-359 */
+        alphaLocal = (REAL)0.5 * (A_(i - 1, j - 1) + A_(i, j - 1));
+        ue = FN(max_)(-maxVel, FN(min_)(maxVel, (REAL)0.5 * (U_(i, j) + U_(i + 1, j))));
+        uw = FN(max_)(-maxVel, FN(min_)(maxVel, (REAL)0.5 * (U_(i, j - 1) + U_(i + 1, j - 1))));
+        vn = FN(max_)(-maxVel, FN(min_)(maxVel, (REAL)0.5 * (V_(i, j) + V_(i + 1, j))));
+        vs = FN(max_)(-maxVel, FN(min_)(maxVel, (REAL)0.5 * (V_(i - 1, j) + V_(i, j))));
+      }
+      const REAL De = eta * hy / hx, Dn = eta * hx / hy;
+      const REAL Fe = convScale * rho * hy * ue, Fw = convScale * rho * hy * uw;
+      const REAL Fn = convScale * rho * hx * vn, Fs = convScale * rho * hx * vs;
+      const REAL aE = De + FN(max_)(0, -Fe), aW = De + FN(max_)(0, Fw);
+      const REAL aN = Dn + FN(max_)(0, -Fn), aS = Dn + FN(max_)(0, Fs);
+      const REAL Sdc = (s->conv == 1) ? (isU ? FN(sou_u)(s, u, i, j, Fe, Fw, Fn, Fs) : FN(sou_v)(s, v, i, j, Fe, Fw, Fn, Fs))
+                                      : (REAL)0;
+      const REAL sumA = aE + aW + aN + aS;
+      const REAL transCoeffLocal = 0; /* rho vol / dt with dt = +inf (pseudo-transient off, :212) */
+      const REAL brinkmanDrag = alphaLocal * vol;
+      REAL aP0 = sumA + (Fe - Fw + Fn - Fs) + transCoeffLocal + sinkDiag + brinkmanDrag;
+      aP0 = FN(max_)(aP0, (REAL)1e-10);
+      const REAL dDenom = FN(max_)(aP0, (REAL)1e-12);
+      const REAL velCur = x_old[i * xc + j];
+      REAL Sp;
+      if (isU) { d[i * N + j] = hy / dDenom; Sp = (P_(i, j) - P_(i, j + 1)) * hy; }
+      else     { d[i * (N + 1) + j] = hx / dDenom; Sp = (P_(i, j) - P_(i + 1, j)) * hx; }
+      Sp += transCoeffLocal * velCur; /* uOld == u (:220) */
+      Sp += Sdc;
+      const REAL aP = aP0 / s->uvAlpha;
+      Sp += ((REAL)1 - s->uvAlpha) / s->uvAlpha * aP0 * velCur;
+      REAL xNew = (aE * x_old[i * xc + j + 1] + aW * x_old[i * xc + j - 1] + aN * x_old[(i + 1) * xc + j] +
+                   aS * x_old[(i - 1) * xc + j] + Sp) / aP;
+      xNew = FN(max_)(-maxVel, FN(min_)(maxVel, xNew));
+      const REAL diff = (REAL)fabs(xNew - velCur);
+      if (diff > res) res = diff;
+      xStar[i * xc + j] = xNew;
+    }
+  *resid = res;
+#undef U_
+#undef V_
+#undef P_
+#undef A_
+}
+
 /* boundaries.cpp:48-106 setVelocityBoundaryConditions. */
 void FN(velocity_bc)(int M, int N, double Uin_d, const REAL* gamma, REAL* uIn, REAL* vIn) {
   const REAL Uin = (REAL)Uin_d;
@@ -355,8 +427,8 @@ static int FN(pressure)(const FN(params) * s, const REAL* uStar, const REAL* vSt
   return iter;
 }
 
-/* iterations.cpp:82-526 calculateStep with momentumSolverType=1 and the
- * Parallel-CG pressure solver.  `stop_after`: 1 = after the momentum solve and
+/* iterations.cpp:82-526 calculateStep with momentumSolverType 1 (implicit
+ * Jacobi) or 0 (explicit point update) and the Parallel-CG pressure solver.  `stop_after`: 1 = after the momentum solve and
  * its BCs (uStar, vStar, dE, dN final), 2 = after the pressure solve (pStar
  * final), 3 = whole step.  diag[0..7] = residU, residV, residMass,
  * residMassDof, returned error, PCG count, U sweeps, V sweeps. */
@@ -369,8 +441,14 @@ int FN(step)(const int* ip, const double* dp, int stop_after, REAL* u, REAL* v, 
   if (M < 3 || N < 3) return -1;
   const REAL maxVel = (REAL)3 * FN(max_)((REAL)fabs(s.Uin), (REAL)0.1); /* :104 */
   REAL residU, residV, residMass, residMassDof;
-  const int su = FN(momentum)(&s, 1, u, v, p, alpha, uStar, dE, &residU);
-  const int sv = FN(momentum)(&s, 0, u, v, p, alpha, vStar, dN, &residV);
+  int su = -1, sv = -1; /* no Jacobi solve in the explicit path */
+  if (s.momType == 0) {
+    FN(momentum_explicit)(&s, 1, u, v, p, alpha, uStar, dE, &residU);
+    FN(momentum_explicit)(&s, 0, u, v, p, alpha, vStar, dN, &residV);
+  } else {
+    su = FN(momentum)(&s, 1, u, v, p, alpha, uStar, dE, &residU);
+    sv = FN(momentum)(&s, 0, u, v, p, alpha, vStar, dN, &residV);
+  }
   FN(velocity_bc)(M, N, dp[6], gamma, uStar, vStar); /* :134 */
   diag[0] = residU; diag[1] = residV; diag[6] = su; diag[7] = sv;
   if (stop_after == 1) return 0;
