@@ -72,6 +72,31 @@ class Design:
     maxMomentumIter: int = 200  # SIMPLE.h:177
     momentumSolverType: int = 1  # SIMPLE.h:172 (0 explicit point update, 1 implicit Jacobi)
     name: str = "design"
+    # Pseudo-transient term and its CFL controllers (SIMPLE.h:255-313; all off by default).
+    enablePseudoTimeStepping: bool = False
+    useLocalPseudoTime: bool = True
+    timeStepMultiplier: float = 0.01  # timeStep = multiplier * N hx / max(inletVelocity, 1e-6)
+    minPseudoSpeed: float = 0.05
+    pseudoCFL: float = 0.1  # the CFL number when the ramp does not set it
+    enableSER: bool = True
+    serCFLMin: float = 0.1
+    serCFLMax: float = 5.0
+    serSmooth: float = 0.5
+    serMinIter: int = 10
+    serMaxIncrease: float = 1.1
+    serMaxDecrease: float = 0.7
+    serUseMaxResid: bool = False
+    enableLineSearch: bool = True
+    lsAlphaMin: float = 0.1
+    lsAlphaReduce: float = 0.3
+    lsMaxTries: int = 4
+    lsResidIncreaseTol: float = 1.01
+    enableCflRamp: bool = True
+    pseudoCFLInitial: float = 0.1
+    pseudoCFLMax: float = 30.0
+    cflRampStartRes: float = 1e-4
+    cflRampExponent: float = 0.8
+    cflRampSmooth: float = 0.1
 
     def __post_init__(self) -> None:
         self.gamma = np.ascontiguousarray(self.gamma, dtype=np.float64)
@@ -98,15 +123,27 @@ class Design:
     def nP(self) -> int:
         return (self.M - 1) * (self.N - 2)
 
+    def pseudo_cfl_start(self) -> float:
+        """The CFL number of the first step: the constructor starts the ramp
+        at pseudoCFLInitial when enableCflRamp (SIMPLE.cpp:78-82)."""
+        return self.pseudoCFLInitial if self.enableCflRamp else self.pseudoCFL
+
     def int_params(self) -> np.ndarray:
         return np.array([self.M, self.N, self.convectionScheme, int(self.enableTwoPointFiveD),
                          int(self.enableConvectionScaling), self.maxPressureIter, self.maxMomentumIter,
-                         self.momentumSolverType], dtype=np.int32)
+                         self.momentumSolverType, int(self.enablePseudoTimeStepping), int(self.useLocalPseudoTime),
+                         int(self.enableSER), int(self.enableLineSearch), int(self.enableCflRamp),
+                         int(self.serUseMaxResid), self.serMinIter, self.lsMaxTries], dtype=np.int32)
 
-    def real_params(self) -> np.ndarray:
+    def real_params(self, pseudo_cfl: Optional[float] = None) -> np.ndarray:
+        """dp[27] is the CFL number the step uses (default: the first step's)."""
         return np.array([self.hx, self.hy, self.rho, self.eta, self.uvAlpha, self.pAlpha, self.inletVelocity,
-                         self.Ht_channel, self.twoPointFiveDSinkMultiplier, self.pTol, self.momentumTol],
-                        dtype=np.float64)
+                         self.Ht_channel, self.twoPointFiveDSinkMultiplier, self.pTol, self.momentumTol,
+                         self.timeStepMultiplier, self.minPseudoSpeed, self.pseudoCFLInitial, self.pseudoCFLMax,
+                         self.cflRampStartRes, self.cflRampExponent, self.cflRampSmooth, self.serCFLMin,
+                         self.serCFLMax, self.serSmooth, self.serMaxIncrease, self.serMaxDecrease, self.lsAlphaMin,
+                         self.lsAlphaReduce, self.lsResidIncreaseTol, self.inletVelocity,
+                         self.pseudo_cfl_start() if pseudo_cfl is None else pseudo_cfl], dtype=np.float64)
 
     def replace(self, **kw) -> "Design":
         return dataclasses.replace(self, **kw)

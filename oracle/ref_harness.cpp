@@ -246,6 +246,44 @@ int main(int argc, char** argv) {
     s.pressureSolverType = recs.count("solverType") ? geti(recs, "solverType") : 1;  // 1 = Parallel CG
     s.momentumSolverType = recs.count("momType") ? geti(recs, "momType") : 1;  // iterations.cpp:109
     s.enablePseudoTimeStepping = false; // SIMPLE.h:262 default
+    if (recs.count("pseudoI")) {
+      // The pseudo-transient term and its CFL controllers (SIMPLE.h:255-313), in the
+      // layout of oracle/simple_oracle_impl.h (ip[8..15], dp[11..27]).
+      const std::vector<int32_t>& pi = recs["pseudoI"].i;
+      const std::vector<double>& pd = recs["pseudoD"].d;
+      if (pi.size() != 8 || pd.size() != 17) throw std::runtime_error("bad pseudo records");
+      s.enablePseudoTimeStepping = pi[0] != 0;
+      s.useLocalPseudoTime = pi[1] != 0;
+      s.enableSER = pi[2] != 0;
+      s.enableLineSearch = pi[3] != 0;
+      s.enableCflRamp = pi[4] != 0;
+      s.serUseMaxResid = pi[5] != 0;
+      s.serMinIter = pi[6];
+      s.lsMaxTries = pi[7];
+      s.timeStepMultiplier = static_cast<real>(pd[0]);
+      s.minPseudoSpeed = static_cast<real>(pd[1]);
+      s.pseudoCFLInitial = static_cast<real>(pd[2]);
+      s.pseudoCFLMax = static_cast<real>(pd[3]);
+      s.cflRampStartRes = static_cast<real>(pd[4]);
+      s.cflRampExponent = static_cast<real>(pd[5]);
+      s.cflRampSmooth = static_cast<real>(pd[6]);
+      s.serCFLMin = static_cast<real>(pd[7]);
+      s.serCFLMax = static_cast<real>(pd[8]);
+      s.serSmooth = static_cast<real>(pd[9]);
+      s.serMaxIncrease = static_cast<real>(pd[10]);
+      s.serMaxDecrease = static_cast<real>(pd[11]);
+      s.lsAlphaMin = static_cast<real>(pd[12]);
+      s.lsAlphaReduce = static_cast<real>(pd[13]);
+      s.lsResidIncreaseTol = static_cast<real>(pd[14]);
+      // The constructor's set-up with these values (SIMPLE.cpp:68-82): the global
+      // pseudo time step from the domain length and the target velocity; the
+      // starting CFL number.
+      real domainLength = s.N * s.hx;
+      real velRef = std::max(s.targetVel, static_cast<real>(1e-6));
+      s.timeStep = s.timeStepMultiplier * domainLength / velRef;
+      s.pseudoCFL = static_cast<real>(pd[16]);
+      if (s.enableCflRamp) s.pseudoCFL = s.pseudoCFLInitial;
+    }
     s.usePressureDropConvergence = false;
     s.saveStateInterval = 0;
 
@@ -260,7 +298,7 @@ int main(int argc, char** argv) {
     const int maxOuter = geti(recs, "maxOuter");
     const int stopOnConv = geti(recs, "stopOnConv");
     const double eps = getd(recs, "eps");
-    std::vector<double> hU, hV, hMass, hMassDof, hErr;
+    std::vector<double> hU, hV, hMass, hMassDof, hErr, hCfl, hSer;
     std::vector<int32_t> hP, hJu, hJv;
     double elapsed = 0.0;
     if (mode == 2) {
@@ -304,7 +342,15 @@ int main(int argc, char** argv) {
       int pIt = 0;
       auto t0 = std::chrono::steady_clock::now();
       real err = s.calculateStep(pIt);
+      // the CFL controllers after the step (SIMPLE.cpp:321-327); no-ops with the
+      // pseudo-transient term off
+      real monitoringResid = s.serUseMaxResid ? err : s.residMass;
+      s.updateCflSER(monitoringResid, it);
+      s.applyLineSearch(monitoringResid);
+      s.updateCflRamp(monitoringResid);
       elapsed += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      hCfl.push_back(s.pseudoCFL);
+      hSer.insert(hSer.end(), {(double)s.serResidPrev, (double)s.lsCurrentAlpha, (double)s.lsBacktrackCount});
 #ifdef CPS_DROPIN
       if (s.pressureSolverType == 5) b200SyncFieldsToHost(s);  // uStar/vStar for the residual below
 #endif
@@ -332,6 +378,8 @@ int main(int argc, char** argv) {
     w.i("uSweeps", hJu);
     w.i("vSweeps", hJv);
     w.d("elapsed", {elapsed});
+    w.d("pseudoCFL", hCfl);  // after each step's controllers
+    w.d("pseudoState", hSer);  // serResidPrev, lsCurrentAlpha, lsBacktrackCount after each step
     w.matrix("u", s.u);
     w.matrix("v", s.v);
     w.matrix("p", s.p);

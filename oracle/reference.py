@@ -49,6 +49,10 @@ def case_records(design, max_outer: int, eps: float = 1e-6, stop_on_conv: bool =
     }
     if init is not None:
         rec["u0"], rec["v0"], rec["p0"] = init["u"], init["v"], init["p"]
+    if design.enablePseudoTimeStepping:
+        ip, dp = design.int_params(), design.real_params(design.pseudoCFL)
+        rec["pseudoI"] = [int(x) for x in ip[8:16]]
+        rec["pseudoD"] = [float(x) for x in dp[11:28]]
     return rec
 
 

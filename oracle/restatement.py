@@ -61,15 +61,17 @@ def _check(fields: Dict[str, np.ndarray], design, dt) -> None:
             raise ValueError(f"field {k}: expected {s} {dt} C-contiguous, got {a.shape} {a.dtype}")
 
 
-def step(design, fields: Dict[str, np.ndarray], precision: str = "f64", stop_after: int = 3) -> Dict[str, float]:
-    """One outer iteration in place (iterations.cpp:82-526)."""
+def step(design, fields: Dict[str, np.ndarray], precision: str = "f64", stop_after: int = 3,
+         pseudo_cfl: Optional[float] = None) -> Dict[str, float]:
+    """One outer iteration in place (iterations.cpp:82-526); ``pseudo_cfl``:
+    the CFL number of the pseudo-transient term (default: the first step's)."""
     dt = np.float64 if precision == "f64" else np.float32
     _check(fields, design, dt)
     alpha = np.ascontiguousarray(design.alpha, dtype=dt)
     gamma = np.ascontiguousarray(design.gamma, dtype=dt)
     diag = np.zeros(8, dtype=np.float64)
     fn = lib().orc64_step if precision == "f64" else lib().orc32_step
-    rc = fn(_ptr(design.int_params()), _ptr(design.real_params()), ctypes.c_int(stop_after),
+    rc = fn(_ptr(design.int_params()), _ptr(design.real_params(pseudo_cfl)), ctypes.c_int(stop_after),
             *[_ptr(fields[k]) for k in FIELD_NAMES], _ptr(alpha), _ptr(gamma), _ptr(diag))
     if rc != 0:
         raise RuntimeError(f"oracle step failed ({rc})")
@@ -92,6 +94,26 @@ def solve(design, fields: Dict[str, np.ndarray], max_outer: int, eps: float = 1e
     if n < 0:
         raise RuntimeError("oracle solve failed")
     return hist[:n]
+
+
+def pseudo_start(design) -> np.ndarray:
+    """The CFL controllers' state before the first step: pseudoCFL,
+    serResidPrev, lsCurrentAlpha, lsBacktrackCount (SIMPLE.cpp:78-82,
+    SIMPLE.h:255-313)."""
+    return np.array([design.pseudo_cfl_start(), 0.0, 1.0, 0.0], dtype=np.float64)
+
+
+def pseudo_update(design, state: np.ndarray, diag: Dict[str, float], iteration: int,
+                  precision: str = "f64") -> np.ndarray:
+    """The outer loop's CFL controllers after the step with index
+    ``iteration`` (SIMPLE.cpp:321-327, time_control.cpp:43-166); returns the
+    new state."""
+    st = np.array(state, dtype=np.float64, copy=True)
+    resid = diag["err"] if design.serUseMaxResid else diag["residMass"]
+    fn = lib().orc64_pseudo_update if precision == "f64" else lib().orc32_pseudo_update
+    fn(_ptr(design.int_params()), _ptr(design.real_params(float(st[0]))), _ptr(st), ctypes.c_double(resid),
+       ctypes.c_int(iteration))
+    return st
 
 
 def sample_plane(design, fields: Dict[str, np.ndarray], x: float, precision: str = "f64") -> np.ndarray:

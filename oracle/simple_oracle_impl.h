@@ -29,17 +29,137 @@ static inline REAL FN(max_)(REAL a, REAL b) { return (a < b) ? b : a; }
 static inline REAL FN(min_)(REAL a, REAL b) { return (b < a) ? b : a; }
 static inline REAL FN(clamp_)(REAL v, REAL lo, REAL hi) { return (v < lo) ? lo : (hi < v) ? hi : v; }
 
+/* Parameter layout (ip, dp), shared with coldplate_solver_b200/geometry.py:
+ *   ip[0..7]   M N conv twoFiveD convScale maxPIter maxMomIter momType
+ *   ip[8..15]  pseudo-transient (SIMPLE.h:255-313): enablePseudoTimeStepping useLocalPseudoTime
+ *              enableSER enableLineSearch enableCflRamp serUseMaxResid serMinIter lsMaxTries
+ *   dp[0..10]  hx hy rho eta uvAlpha pAlpha Uin Ht sinkMult pTol momTol
+ *   dp[11..26] timeStepMultiplier minPseudoSpeed pseudoCFLInitial pseudoCFLMax cflRampStartRes
+ *              cflRampExponent cflRampSmooth serCFLMin serCFLMax serSmooth serMaxIncrease
+ *              serMaxDecrease lsAlphaMin lsAlphaReduce lsResidIncreaseTol targetVel
+ *   dp[27]     pseudoCFL: the CFL number the step uses (the controllers' current state) */
 typedef struct {
   int M, N, conv, twoFiveD, convScale, maxPIter, maxMomIter, momType;
+  int pseudo, pseudoLocal, serOn, lsOn, rampOn, serUseMax, serMinIter, lsMaxTries;
   REAL hx, hy, rho, eta, uvAlpha, pAlpha, Uin, Ht, sinkMult, pTol, momTol;
+  REAL timeStep, minPseudoSpeed, cflInitial, cflMax, rampStartRes, rampExponent, rampSmooth;
+  REAL serCFLMin, serCFLMax, serSmooth, serMaxIncrease, serMaxDecrease, lsAlphaMin, lsAlphaReduce, lsTol;
+  REAL pseudoCFL;
 } FN(params);
 
 static void FN(unpack)(const int* ip, const double* dp, FN(params) * s) {
   s->M = ip[0]; s->N = ip[1]; s->conv = ip[2]; s->twoFiveD = ip[3]; s->convScale = ip[4];
   s->maxPIter = ip[5]; s->maxMomIter = ip[6]; s->momType = ip[7];
+  s->pseudo = ip[8]; s->pseudoLocal = ip[9]; s->serOn = ip[10]; s->lsOn = ip[11]; s->rampOn = ip[12];
+  s->serUseMax = ip[13]; s->serMinIter = ip[14]; s->lsMaxTries = ip[15];
   s->hx = (REAL)dp[0]; s->hy = (REAL)dp[1]; s->rho = (REAL)dp[2]; s->eta = (REAL)dp[3];
   s->uvAlpha = (REAL)dp[4]; s->pAlpha = (REAL)dp[5]; s->Uin = (REAL)dp[6]; s->Ht = (REAL)dp[7];
   s->sinkMult = (REAL)dp[8]; s->pTol = (REAL)dp[9]; s->momTol = (REAL)dp[10];
+  s->minPseudoSpeed = (REAL)dp[12]; s->cflInitial = (REAL)dp[13]; s->cflMax = (REAL)dp[14];
+  s->rampStartRes = (REAL)dp[15]; s->rampExponent = (REAL)dp[16]; s->rampSmooth = (REAL)dp[17];
+  s->serCFLMin = (REAL)dp[18]; s->serCFLMax = (REAL)dp[19]; s->serSmooth = (REAL)dp[20];
+  s->serMaxIncrease = (REAL)dp[21]; s->serMaxDecrease = (REAL)dp[22]; s->lsAlphaMin = (REAL)dp[23];
+  s->lsAlphaReduce = (REAL)dp[24]; s->lsTol = (REAL)dp[25]; s->pseudoCFL = (REAL)dp[27];
+  { /* SIMPLE.cpp:68-70: the global pseudo time step from the domain length and the target velocity */
+    const REAL domainLength = (REAL)s->N * s->hx;
+    const REAL velRef = FN(max_)((REAL)dp[26], (REAL)1e-6);
+    s->timeStep = (REAL)dp[11] * domainLength / velRef;
+  }
+}
+
+/* The pseudo-transient coefficient rho vol / dt of the implicit assembly at a
+ * point whose current velocity is vel (momentum_solver.cpp:231-241); 0 with
+ * the pseudo-transient term off. */
+static REAL FN(trans_implicit)(const FN(params) * s, REAL vel) {
+  if (!s->pseudo) return 0;
+  const REAL vol = s->hx * s->hy, hChar = FN(min_)(s->hx, s->hy);
+  REAL dtLocal = FN(max_)(s->timeStep, (REAL)1e-20);
+  if (s->pseudoLocal) {
+    const REAL speed = FN(max_)((REAL)fabs(vel), s->minPseudoSpeed);
+    dtLocal = FN(min_)(dtLocal, s->pseudoCFL * hChar / speed);
+    dtLocal = FN(max_)(dtLocal, (REAL)1e-20);
+  }
+  return s->rho * vol / dtLocal;
+}
+
+/* The same coefficient in the explicit update, from computeLocalDt
+ * (iterations.cpp:189-217, 290-294): dt = +inf with the term off. */
+static REAL FN(trans_explicit)(const FN(params) * s, REAL vel) {
+  const REAL vol = s->hx * s->hy, hChar = FN(min_)(s->hx, s->hy);
+  REAL dtLocal;
+  if (!s->pseudo) dtLocal = (REAL)INFINITY;
+  else if (!s->pseudoLocal) dtLocal = s->timeStep;
+  else {
+    const REAL speed = FN(max_)((REAL)fabs(vel), s->minPseudoSpeed);
+    const REAL dtCfl = s->pseudoCFL * hChar / speed;
+    dtLocal = FN(min_)(s->timeStep, dtCfl);
+  }
+  return s->rho * vol / dtLocal;
+}
+
+/* The outer loop's CFL controllers after one step (SIMPLE.cpp:321-327):
+ * updateCflSER (time_control.cpp:82-118), applyLineSearch (:127-166) and
+ * updateCflRamp (:43-63), in that order.  st = {pseudoCFL, serResidPrev,
+ * lsCurrentAlpha, lsBacktrackCount}; resid = the monitoring residual
+ * (serUseMaxResid ? the step's error : residMass); iteration = the outer
+ * loop's index of the step. */
+void FN(pseudo_update)(const int* ip, const double* dp, double* st, double resid_d, int iteration) {
+  FN(params) s;
+  FN(unpack)(ip, dp, &s);
+  if (!s.pseudo) return;
+  REAL cfl = (REAL)st[0], prev = (REAL)st[1], alpha = (REAL)st[2];
+  int count = (int)st[3];
+  const REAL resid = (REAL)resid_d;
+  if (s.serOn && iteration >= s.serMinIter) {
+    const REAL cur = FN(max_)(resid, (REAL)1e-15);
+    if (prev <= 0) {
+      prev = cur;
+    } else {
+      REAL ratio = prev / cur;
+      ratio = FN(max_)(ratio, s.serMaxDecrease);
+      ratio = FN(min_)(ratio, s.serMaxIncrease);
+      REAL target = cfl * ratio;
+      target = FN(max_)(target, s.serCFLMin);
+      target = FN(min_)(target, s.serCFLMax);
+      cfl = ((REAL)1 - s.serSmooth) * cfl + s.serSmooth * target;
+      if (!isfinite(cfl) || cfl <= 0) cfl = s.serCFLMin;
+      prev = cur;
+    }
+  }
+  if (s.lsOn && s.serOn) {
+    if (prev <= 0) {
+      alpha = 1;
+      count = 0;
+    } else {
+      const REAL ratio = resid / prev;
+      if (ratio > s.lsTol) {
+        count++;
+        if (count <= s.lsMaxTries) {
+          alpha *= s.lsAlphaReduce;
+          alpha = FN(max_)(alpha, s.lsAlphaMin);
+          cfl *= s.lsAlphaReduce;
+          cfl = FN(max_)(cfl, s.serCFLMin);
+        }
+      } else {
+        if (alpha < 1) alpha = FN(min_)(alpha * (REAL)1.1, (REAL)1);
+        count = 0;
+      }
+    }
+  }
+  if (s.rampOn && !s.serOn) {
+    const REAL cur = FN(max_)(resid, (REAL)1e-12);
+    if (cur > s.rampStartRes) {
+      cfl = s.cflInitial;
+    } else {
+      const REAL ratio = s.rampStartRes / cur;
+      const REAL rawFactor = sizeof(REAL) == 4 ? (REAL)powf((float)ratio, (float)s.rampExponent)
+                                               : (REAL)pow((double)ratio, (double)s.rampExponent);
+      const REAL target = FN(min_)(s.cflInitial * rawFactor, s.cflMax);
+      cfl = ((REAL)1 - s.rampSmooth) * cfl + s.rampSmooth * target;
+      if (!isfinite(cfl) || cfl <= 0) cfl = s.cflInitial;
+    }
+  }
+  st[0] = cfl; st[1] = prev; st[2] = alpha; st[3] = count;
 }
 
 /* SIMPLE.cpp:589-630 buildAlphaFromDensity: RAMP alpha from gamma, then rows 0
@@ -172,14 +292,15 @@ static int FN(momentum)(const FN(params) * s, int isU, const REAL* u, const REAL
       const REAL aE = De + FN(max_)(0, -Fe), aW = De + FN(max_)(0, Fw);
       const REAL aN = Dn + FN(max_)(0, -Fn), aS = Dn + FN(max_)(0, Fs);
       const REAL sumA = aE + aW + aN + aS;
-      const REAL transCoeff = 0; /* pseudo-transient off (SIMPLE.h:262) */
+      const REAL velCur = isU ? U_(i, j) : V_(i, j);
+      const REAL transCoeff = FN(trans_implicit)(s, velCur); /* :231-241 */
       const REAL brinkmanDrag = alphaLocal * vol;
       REAL aP0 = sumA + (Fe - Fw + Fn - Fs) + transCoeff + sinkDiag + brinkmanDrag; /* :246 */
       aP0 = FN(max_)(aP0, (REAL)1e-10);
       const REAL aP = aP0 / s->uvAlpha;
-      REAL Sp, velCur;
-      if (isU) { Sp = (P_(i, j) - P_(i, j + 1)) * hy; velCur = U_(i, j); }
-      else     { Sp = (P_(i, j) - P_(i + 1, j)) * hx; velCur = V_(i, j); }
+      REAL Sp;
+      if (isU) Sp = (P_(i, j) - P_(i, j + 1)) * hy;
+      else     Sp = (P_(i, j) - P_(i + 1, j)) * hx;
       Sp += transCoeff * velCur; /* uOld == u at this point (iterations.cpp:118) */
       Sp += ((REAL)1 - s->uvAlpha) / s->uvAlpha * aP0 * velCur;
       if (s->conv == 1) Sp += isU ? FN(sou_u)(s, u, i, j, Fe, Fw, Fn, Fs) : FN(sou_v)(s, v, i, j, Fe, Fw, Fn, Fs);
@@ -239,7 +360,7 @@ static int FN(momentum)(const FN(params) * s, int isU, const REAL* u, const REAL
 }
 
 /* The explicit momentum update of calculateStep with momentumSolverType = 0
- * and the pseudo-transient term off (iterations.cpp:176-441): one point update
+ * (iterations.cpp:176-441): one point update
  * per unknown from the current velocities with the full coefficients, clamped
  * to +-maxVel; d = h / max(aP0, 1e-12).  Writes xStar and d at the unknowns;
  * *resid = max |xNew - vel|. */
@@ -283,12 +404,12 @@ static void FN(momentum_explicit)(const FN(params) * s, int isU, const REAL* u, 
       const REAL Sdc = (s->conv == 1) ? (isU ? FN(sou_u)(s, u, i, j, Fe, Fw, Fn, Fs) : FN(sou_v)(s, v, i, j, Fe, Fw, Fn, Fs))
                                       : (REAL)0;
       const REAL sumA = aE + aW + aN + aS;
-      const REAL transCoeffLocal = 0; /* rho vol / dt with dt = +inf (pseudo-transient off, :212) */
+      const REAL velCur = x_old[i * xc + j];
+      const REAL transCoeffLocal = FN(trans_explicit)(s, velCur); /* :290-294 */
       const REAL brinkmanDrag = alphaLocal * vol;
       REAL aP0 = sumA + (Fe - Fw + Fn - Fs) + transCoeffLocal + sinkDiag + brinkmanDrag;
       aP0 = FN(max_)(aP0, (REAL)1e-10);
       const REAL dDenom = FN(max_)(aP0, (REAL)1e-12);
-      const REAL velCur = x_old[i * xc + j];
       REAL Sp;
       if (isU) { d[i * N + j] = hy / dDenom; Sp = (P_(i, j) - P_(i, j + 1)) * hy; }
       else     { d[i * (N + 1) + j] = hx / dDenom; Sp = (P_(i, j) - P_(i + 1, j)) * hx; }
@@ -483,16 +604,21 @@ int FN(step)(const int* ip, const double* dp, int stop_after, REAL* u, REAL* v, 
   return 0;
 }
 
-/* Outer loop (SIMPLE.cpp:299-318 without ramp, logging or dP window): at most
+/* Outer loop (SIMPLE.cpp:299-327 without the inlet ramp, logging or dP window): at most
  * max_outer steps, stopping once max(residU, residV, residMassDof) <= eps when
  * stop_on_conv.  hist is max_outer x 8 (the step diagnostics); returns steps run. */
 int FN(solve)(const int* ip, const double* dp, int max_outer, double eps, int stop_on_conv, REAL* u, REAL* v,
               REAL* p, REAL* pStar, REAL* uStar, REAL* vStar, REAL* dE, REAL* dN, const REAL* alpha,
               const REAL* gamma, double* hist) {
+  /* the controllers' state starts as the constructor leaves it (SIMPLE.cpp:78-82, SIMPLE.h:280-292) */
+  double dpl[28], st[4] = {dp[27], 0.0, 1.0, 0.0};
+  for (int k = 0; k < 28; ++k) dpl[k] = dp[k];
   int it = 0;
   for (; it < max_outer; ++it) {
     double* h = hist + 8 * it;
-    if (FN(step)(ip, dp, 3, u, v, p, pStar, uStar, vStar, dE, dN, alpha, gamma, h) != 0) return -1;
+    dpl[27] = st[0];
+    if (FN(step)(ip, dpl, 3, u, v, p, pStar, uStar, vStar, dE, dN, alpha, gamma, h) != 0) return -1;
+    FN(pseudo_update)(ip, dpl, st, ip[13] ? h[4] : h[2], it); /* SIMPLE.cpp:323-326 */
     double conv = h[0];
     if (conv < h[1]) conv = h[1];
     if (conv < h[3]) conv = h[3];
