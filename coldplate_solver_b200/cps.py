@@ -85,6 +85,39 @@ class CpsCaseParams(ctypes.Structure):
                 ("Ht", ctypes.c_double), ("has_Ht", ctypes.c_int)]
 
 
+class CpsPseudo(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_int) for k in ("enable", "use_local", "enable_ser", "enable_line_search",
+                                             "enable_cfl_ramp", "ser_use_max_resid", "ser_min_iter",
+                                             "ls_max_tries")] + \
+               [(k, ctypes.c_double) for k in ("target_velocity", "time_step_multiplier", "min_pseudo_speed",
+                                                "pseudo_cfl", "cfl_initial", "cfl_max", "cfl_ramp_start_res",
+                                                "cfl_ramp_exponent", "cfl_ramp_smooth", "ser_cfl_min", "ser_cfl_max",
+                                                "ser_smooth", "ser_max_increase", "ser_max_decrease",
+                                                "ls_alpha_min", "ls_alpha_reduce", "ls_resid_increase_tol", "time_step")]
+
+
+class CpsPseudoState(ctypes.Structure):
+    _fields_ = [("pseudo_cfl", ctypes.c_double), ("ser_resid_prev", ctypes.c_double), ("ls_alpha", ctypes.c_double),
+                ("ls_backtracks", ctypes.c_int), ("pad", ctypes.c_int)]
+
+
+def pseudo_from_design(design: Design) -> CpsPseudo:
+    """The cps_pseudo block of a design's pseudo-transient settings
+    (reference member names, SIMPLE.h:255-313)."""
+    d = design
+    return CpsPseudo(enable=int(d.enablePseudoTimeStepping), use_local=int(d.useLocalPseudoTime),
+                     enable_ser=int(d.enableSER), enable_line_search=int(d.enableLineSearch),
+                     enable_cfl_ramp=int(d.enableCflRamp), ser_use_max_resid=int(d.serUseMaxResid),
+                     ser_min_iter=d.serMinIter, ls_max_tries=d.lsMaxTries, target_velocity=d.inletVelocity,
+                     time_step_multiplier=d.timeStepMultiplier, min_pseudo_speed=d.minPseudoSpeed,
+                     pseudo_cfl=d.pseudoCFL, cfl_initial=d.pseudoCFLInitial, cfl_max=d.pseudoCFLMax,
+                     cfl_ramp_start_res=d.cflRampStartRes, cfl_ramp_exponent=d.cflRampExponent,
+                     cfl_ramp_smooth=d.cflRampSmooth, ser_cfl_min=d.serCFLMin, ser_cfl_max=d.serCFLMax,
+                     ser_smooth=d.serSmooth, ser_max_increase=d.serMaxIncrease, ser_max_decrease=d.serMaxDecrease,
+                     ls_alpha_min=d.lsAlphaMin, ls_alpha_reduce=d.lsAlphaReduce,
+                     ls_resid_increase_tol=d.lsResidIncreaseTol)
+
+
 class CpsBatchResult(ctypes.Structure):
     _fields_ = [("n_done", ctypes.c_int), ("converged", ctypes.c_int), ("status", ctypes.c_int),
                 ("last", CpsStepOut)]
@@ -118,6 +151,10 @@ SIGNATURES = {
     "cps_solve_monitored": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                            ctypes.POINTER(CpsStepOut), _D, ctypes.POINTER(ctypes.c_int),
                                            ctypes.POINTER(ctypes.c_int)]),
+    "cps_pseudo_defaults": (ctypes.c_int, [ctypes.POINTER(CpsPseudo), ctypes.c_double]),
+    "cps_set_pseudo": (ctypes.c_int, [_P, ctypes.POINTER(CpsPseudo)]),
+    "cps_get_pseudo_state": (ctypes.c_int, [_P, ctypes.POINTER(CpsPseudoState)]),
+    "cps_set_pseudo_state": (ctypes.c_int, [_P, ctypes.POINTER(CpsPseudoState)]),
     "cps_read_case_params": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(CpsCaseParams)]),
     "cps_read_geometry": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _D, _D,
                                          ctypes.POINTER(ctypes.c_int)]),
@@ -208,6 +245,8 @@ class Solver:
             raise CpsError(st, self.lib.cps_last_error(None).decode())
         self.ctx = ctx
         self.inletVelocity = design.inletVelocity
+        if design.enablePseudoTimeStepping:
+            self.set_pseudo(design)
 
     def _check(self, st: int) -> None:
         if st != CPS_OK:
@@ -285,6 +324,26 @@ class Solver:
             h = hist[k]
             out[k] = (h.residU, h.residV, h.residMass, h.residMassDof, h.err, h.pIters, h.uSweeps, h.vSweeps)
         return out
+
+    def set_pseudo(self, design: Optional[Design] = None) -> None:
+        """cps_set_pseudo with the pseudo-transient settings of ``design``
+        (default: this solver's); ``enablePseudoTimeStepping = False``
+        switches the term off.  Resets the CFL controllers' state."""
+        p = pseudo_from_design(self.design if design is None else design)
+        self._check(self.lib.cps_set_pseudo(self.ctx, ctypes.byref(p)))
+
+    def pseudo_state(self) -> Dict[str, float]:
+        """The CFL controllers' state: pseudo_cfl, ser_resid_prev, ls_alpha,
+        ls_backtracks."""
+        st = CpsPseudoState()
+        self._check(self.lib.cps_get_pseudo_state(self.ctx, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in CpsPseudoState._fields_ if k != "pad"}
+
+    def set_pseudo_state(self, pseudo_cfl: float, ser_resid_prev: float = 0.0, ls_alpha: float = 1.0,
+                         ls_backtracks: int = 0) -> None:
+        st = CpsPseudoState(pseudo_cfl=pseudo_cfl, ser_resid_prev=ser_resid_prev, ls_alpha=ls_alpha,
+                            ls_backtracks=ls_backtracks)
+        self._check(self.lib.cps_set_pseudo_state(self.ctx, ctypes.byref(st)))
 
     def set_dp_monitor(self, gate: bool = True, window: int = 500, percent: float = 1.0, slope_gate: bool = False,
                        slope_window: int = 1000, slope_max_delta: float = 10.0, ramp_steps: int = 1000,

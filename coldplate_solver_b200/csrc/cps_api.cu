@@ -68,6 +68,8 @@ struct cps_ctx {
   double* dplog = nullptr;   // device, kHistChunk x 4 pressure drops of the last launch
   double* hdplog = nullptr;  // pinned copy
   double* ddphist = nullptr; // device, the pressure-drop gate's windows (cudaMalloc'd by cps_set_dp_monitor)
+  double* dpseudo = nullptr; // device, the CFL controllers' state (4 doubles)
+  double pseudo_start = 0.0; // the controllers' starting CFL number
   int iter = 0;              // outer-loop iteration index of the next iteration (monitor and gate)
   int grid = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -83,13 +85,16 @@ template <typename T, bool Monitor>
 __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_grid_kernel(cps::DesignView d, cps::RunControl rc,
                                                                 cps::GridBarrier* bar, double* red) {
   __shared__ double smem[(Monitor ? cps::kPlaneSums : cps::kRedWidth) * 8];
+  __shared__ cps::PseudoRun s_pr;
   extern __shared__ __align__(16) char tile_smem[];
   cps::GridGroup g{bar, red, rc.status, blockIdx.x, gridDim.x, 0u, 0ull};
+  cps::load_pseudo(d, s_pr);
+  __syncthreads();
   for (int it = 0; it < rc.n_outer; ++it) {
     double out[8];
     const int r = cps::outer_iteration<T, cps::GridGroup, Monitor>(
         d, g, smem, tile_smem, out, it + 1 == rc.n_outer, rc.stop_on_conv != 0, rc.eps, rc.iter0 + it,
-        rc.dplog ? rc.dplog + (size_t)4 * it : nullptr, rc.dp_converged);
+        rc.dplog ? rc.dplog + (size_t)4 * it : nullptr, rc.dp_converged, &s_pr);
     if (r < 0) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       for (int k = 0; k < 8; ++k) rc.hist[(size_t)it * 8 + k] = out[k];
@@ -101,13 +106,14 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_grid_kernel
 
 // Batched solves: each cluster takes the next design from the queue and runs
 // its outer iterations to convergence or to the item's budget.
-template <typename T>
+template <typename T, bool Pseudo>
 __global__ void __launch_bounds__(cps::kThreads) cps_cluster_kernel(const cps::BatchItem* __restrict__ items,
                                                                    const int* __restrict__ order, int n_items,
                                                                    int* queue, cps::BatchResult* results) {
   __shared__ double smem[cps::kRedWidth * 8];
   __shared__ double redbuf[2 * cps::kRedWidth];
   __shared__ __align__(16) cps::BatchItem s_item;
+  __shared__ cps::PseudoRun s_pr;
   __shared__ int s_next;
   extern __shared__ __align__(16) char tile_smem[];
   cps::cg::cluster_group cl = cps::cg::this_cluster();
@@ -125,13 +131,16 @@ __global__ void __launch_bounds__(cps::kThreads) cps_cluster_kernel(const cps::B
     }
     __syncthreads();
     const cps::BatchItem& item = s_item;
+    cps::load_pseudo(item.view, s_pr);
+    __syncthreads();
     cps::BatchResult* res = results + id;
     g.status = &res->status;
     double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int done = 0;
     for (int it = 0; it < item.n_outer; ++it) {
-      const int r = cps::outer_iteration<T>(item.view, g, smem, tile_smem, out, it + 1 == item.n_outer, item.stop_on_conv != 0,
-                                            item.eps);
+      const int r = cps::outer_iteration<T, cps::ClusterGroup, false, Pseudo>(
+          item.view, g, smem, tile_smem, out, it + 1 == item.n_outer, item.stop_on_conv != 0, item.eps, item.iter0 + it,
+          nullptr, nullptr, &s_pr);
       done = it + 1;
       if (g.rank == 0 && threadIdx.x == 0 && item.hist && it < item.hist_cap)
         for (int k = 0; k < 8; ++k) item.hist[(size_t)it * 8 + k] = out[k];
@@ -153,7 +162,7 @@ __global__ void __launch_bounds__(cps::kThreads) cps_cluster_kernel(const cps::B
 // time and runs each with the bounded software barrier of its own counter.
 // The group count sets how many designs are in flight (and so the in-flight
 // working set against the 126 MB L2); K sets how many CTAs share one design.
-template <typename T>
+template <typename T, bool Pseudo>
 __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_group_kernel(const cps::BatchItem* __restrict__ items,
                                                                     const int* __restrict__ order, int n_items,
                                                                     int* queue, cps::BatchResult* results,
@@ -161,6 +170,7 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_group_kerne
                                                                     int* slots, int group_ctas) {
   __shared__ double smem[cps::kRedWidth * 8];
   __shared__ __align__(16) cps::BatchItem s_item;
+  __shared__ cps::PseudoRun s_pr;
   extern __shared__ __align__(16) char tile_smem[];
   const unsigned grp = blockIdx.x / group_ctas;
   int* slot = slots + 2 * grp;  // [0] next queue index, [1] group status before a design is assigned
@@ -181,13 +191,16 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_group_kerne
     }
     __syncthreads();
     const cps::BatchItem& item = s_item;
+    cps::load_pseudo(item.view, s_pr);
+    __syncthreads();
     cps::BatchResult* res = results + id;
     g.status = &res->status;
     double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int done = 0;
     for (int it = 0; it < item.n_outer; ++it) {
-      const int r = cps::outer_iteration<T>(item.view, g, smem, tile_smem, out, it + 1 == item.n_outer, item.stop_on_conv != 0,
-                                            item.eps);
+      const int r = cps::outer_iteration<T, cps::GridGroup, false, Pseudo>(
+          item.view, g, smem, tile_smem, out, it + 1 == item.n_outer, item.stop_on_conv != 0, item.eps, item.iter0 + it,
+          nullptr, nullptr, &s_pr);
       if (r < 0) return;  // a bounded wait expired; the design's status says so
       done = it + 1;
       if (g.rank == 0 && threadIdx.x == 0 && item.hist && it < item.hist_cap)
@@ -208,7 +221,7 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_group_kerne
 // designs.  CTAs [first[g], first[g+1]) form group g and run design which[g]
 // to convergence or to its budget with the bounded software barrier of their
 // own counter; their reduction ring starts at first[g] ring rows.
-template <typename T>
+template <typename T, bool Pseudo>
 __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_wave_kernel(const cps::BatchItem* __restrict__ items,
                                                                    const int* __restrict__ first,
                                                                    const int* __restrict__ which, int groups,
@@ -216,6 +229,7 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_wave_kernel
                                                                    cps::GridBarrier* bars, double* rings) {
   __shared__ double smem[cps::kRedWidth * 8];
   __shared__ __align__(16) cps::BatchItem s_item;
+  __shared__ cps::PseudoRun s_pr;
   extern __shared__ __align__(16) char tile_smem[];
   int lo = 0, hi = groups;  // first[lo] <= blockIdx.x < first[lo + 1]
   while (hi - lo > 1) {
@@ -230,14 +244,17 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_wave_kernel
   }
   __syncthreads();
   const cps::BatchItem& item = s_item;
+  cps::load_pseudo(item.view, s_pr);
+  __syncthreads();
   cps::BatchResult* res = results + id;
   cps::GridGroup g{bars + grp, rings + (size_t)first[grp] * cps::kRedSlots * cps::kRedWidth, &res->status,
                    blockIdx.x - (unsigned)first[grp], (unsigned)K, 0u, 0ull};
   double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int done = 0;
   for (int it = 0; it < item.n_outer; ++it) {
-    const int r = cps::outer_iteration<T>(item.view, g, smem, tile_smem, out, it + 1 == item.n_outer,
-                                          item.stop_on_conv != 0, item.eps);
+    const int r = cps::outer_iteration<T, cps::GridGroup, false, Pseudo>(
+        item.view, g, smem, tile_smem, out, it + 1 == item.n_outer, item.stop_on_conv != 0, item.eps, item.iter0 + it,
+        nullptr, nullptr, &s_pr);
     if (r < 0) return;  // a bounded wait expired; the design's status says so
     done = it + 1;
     if (g.rank == 0 && threadIdx.x == 0 && item.hist && it < item.hist_cap)
@@ -291,7 +308,16 @@ size_t footprint_bytes(int M, int N, int precision, size_t* plane_elems_out, int
   bytes += (size_t)(cps::kRedSlots * cps::kRedWidth + cps::kPlaneSums) * kMaxGridCtas * 8;  // reduction ring
   bytes += (size_t)kHistChunk * 8 * 8 + 64;                               // history + plane metrics
   bytes += (size_t)kHistChunk * 4 * 8;                                    // pressure-drop log
+  bytes += 64;                                                            // CFL controllers' state
   return round_up(bytes, 256);
+}
+
+// The CFL controllers' state on the device (pseudoCFL, serResidPrev,
+// lsCurrentAlpha, lsBacktrackCount), written in stream order.
+bool write_pseudo_state(cps_ctx* c, double cfl, double prev, double alpha, int count) {
+  const double h[4] = {cfl, prev, alpha, (double)count};
+  return cuda_ok(c, cudaMemcpyAsync(c->dpseudo, h, sizeof(h), cudaMemcpyHostToDevice, c->stream), "h2d") &&
+         cuda_ok(c, cudaStreamSynchronize(c->stream), "h2d");
 }
 
 cps_status validate(const cps_desc* d) {
@@ -553,6 +579,7 @@ cps_status cps_create(const cps_desc* d, cps_ctx** out) {
   c->dhist = c->red + (size_t)(cps::kRedSlots * cps::kRedWidth + cps::kPlaneSums) * kMaxGridCtas;
   c->dplane = c->dhist + (size_t)kHistChunk * 8;
   c->dplog = c->dplane + 8;
+  c->dpseudo = c->dplog + (size_t)4 * kHistChunk;
 
   cps::DesignView& v = c->view;
   v.M = d->M; v.N = d->N; v.P = c->P;
@@ -644,7 +671,118 @@ cps_status cps_reset_fields(cps_ctx* c) {
   if (!cuda_ok(c, cudaMemsetAsync(c->slab, 0, c->plane_elems * sizeof(double) * (kDN + 1), c->stream), "memset"))
     return CPS_ERR_CUDA;
   c->iter = 0;
+  if (c->view.pseudo && !write_pseudo_state(c, c->pseudo_start, 0.0, 1.0, 0)) return CPS_ERR_CUDA;
   return CPS_OK;
+}
+
+cps_status cps_pseudo_defaults(cps_pseudo* p, double target_velocity) {
+  if (!p) return fail(nullptr, CPS_ERR_ARG, "p is NULL");
+  cps_pseudo q;
+  std::memset(&q, 0, sizeof(q));
+  // SIMPLE.h:255-313
+  q.enable = 0;
+  q.use_local = 1;
+  q.enable_ser = 1;
+  q.enable_line_search = 1;
+  q.enable_cfl_ramp = 1;
+  q.ser_use_max_resid = 0;
+  q.ser_min_iter = 10;
+  q.ls_max_tries = 4;
+  q.target_velocity = target_velocity;
+  q.time_step_multiplier = 0.01;
+  q.min_pseudo_speed = 0.05;
+  q.pseudo_cfl = 0.1;
+  q.cfl_initial = 0.1;
+  q.cfl_max = 30.0;
+  q.cfl_ramp_start_res = 1e-4;
+  q.cfl_ramp_exponent = 0.8;
+  q.cfl_ramp_smooth = 0.1;
+  q.ser_cfl_min = 0.1;
+  q.ser_cfl_max = 5.0;
+  q.ser_smooth = 0.5;
+  q.ser_max_increase = 1.1;
+  q.ser_max_decrease = 0.7;
+  q.ls_alpha_min = 0.1;
+  q.ls_alpha_reduce = 0.3;
+  q.ls_resid_increase_tol = 1.01;
+  *p = q;
+  return CPS_OK;
+}
+
+cps_status cps_set_pseudo(cps_ctx* c, const cps_pseudo* p) {
+  if (!c) return fail(nullptr, CPS_ERR_ARG, "ctx is NULL");
+  cps::DesignView& v = c->view;
+  if (!p || !p->enable) {
+    v.pseudo = 0;
+    return CPS_OK;
+  }
+  const double reals[] = {p->time_step, p->target_velocity, p->time_step_multiplier, p->min_pseudo_speed, p->pseudo_cfl,
+                          p->cfl_initial, p->cfl_max, p->cfl_ramp_start_res, p->cfl_ramp_exponent,
+                          p->cfl_ramp_smooth, p->ser_cfl_min, p->ser_cfl_max, p->ser_smooth, p->ser_max_increase,
+                          p->ser_max_decrease, p->ls_alpha_min, p->ls_alpha_reduce, p->ls_resid_increase_tol};
+  for (double x : reals)
+    if (!std::isfinite(x)) return fail(c, CPS_ERR_ARG, "pseudo-transient parameters must be finite");
+  if (!(p->time_step_multiplier > 0.0 || p->time_step > 0.0) || p->ser_min_iter < 0 || p->ls_max_tries < 0)
+    return fail(c, CPS_ERR_ARG,
+                "pseudo-transient: time_step or time_step_multiplier > 0, ser_min_iter >= 0, ls_max_tries >= 0");
+  if (!cuda_ok(c, cudaSetDevice(c->device), "cudaSetDevice")) return CPS_ERR_CUDA;
+  v.pseudoLocal = p->use_local ? 1 : 0;
+  v.serOn = p->enable_ser ? 1 : 0;
+  v.lsOn = p->enable_line_search ? 1 : 0;
+  v.rampOn = p->enable_cfl_ramp ? 1 : 0;
+  v.serUseMax = p->ser_use_max_resid ? 1 : 0;
+  v.serMinIter = p->ser_min_iter;
+  v.lsMaxTries = p->ls_max_tries;
+  // SIMPLE.cpp:68-70, in the reference's operation order
+  const double domainLength = c->N * v.hx;
+  const double velRef = std::max(p->target_velocity, 1e-6);
+  v.timeStep = p->time_step > 0.0 ? p->time_step : p->time_step_multiplier * domainLength / velRef;
+  v.minPseudoSpeed = p->min_pseudo_speed;
+  v.hChar = std::min(v.hx, v.hy);  // momentum_solver.cpp:190, iterations.cpp:189
+  v.cflInitial = p->cfl_initial;
+  v.cflMax = p->cfl_max;
+  v.rampStartRes = p->cfl_ramp_start_res;
+  v.rampExponent = p->cfl_ramp_exponent;
+  v.rampSmooth = p->cfl_ramp_smooth;
+  v.serCFLMin = p->ser_cfl_min;
+  v.serCFLMax = p->ser_cfl_max;
+  v.serSmooth = p->ser_smooth;
+  v.serMaxIncrease = p->ser_max_increase;
+  v.serMaxDecrease = p->ser_max_decrease;
+  v.lsAlphaMin = p->ls_alpha_min;
+  v.lsAlphaReduce = p->ls_alpha_reduce;
+  v.lsTol = p->ls_resid_increase_tol;
+  v.pseudoState = c->dpseudo;
+  // the constructor starts the ramp at pseudoCFLInitial (SIMPLE.cpp:78-82)
+  c->pseudo_start = p->enable_cfl_ramp ? p->cfl_initial : p->pseudo_cfl;
+  if (!write_pseudo_state(c, c->pseudo_start, 0.0, 1.0, 0)) return CPS_ERR_CUDA;
+  v.pseudo = 1;
+  return CPS_OK;
+}
+
+cps_status cps_get_pseudo_state(cps_ctx* c, cps_pseudo_state* state) {
+  if (!c || !state) return fail(c, CPS_ERR_ARG, "ctx and state are required");
+  if (!cuda_ok(c, cudaSetDevice(c->device), "cudaSetDevice")) return CPS_ERR_CUDA;
+  double h[4];
+  if (!cuda_ok(c, cudaMemcpyAsync(h, c->dpseudo, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "d2h") ||
+      !cuda_ok(c, cudaStreamSynchronize(c->stream), "d2h"))
+    return CPS_ERR_CUDA;
+  state->pseudo_cfl = h[0];
+  state->ser_resid_prev = h[1];
+  state->ls_alpha = h[2];
+  state->ls_backtracks = (int)h[3];
+  state->pad = 0;
+  return CPS_OK;
+}
+
+cps_status cps_set_pseudo_state(cps_ctx* c, const cps_pseudo_state* state) {
+  if (!c || !state) return fail(c, CPS_ERR_ARG, "ctx and state are required");
+  if (!std::isfinite(state->pseudo_cfl) || !std::isfinite(state->ser_resid_prev) || !std::isfinite(state->ls_alpha))
+    return fail(c, CPS_ERR_ARG, "pseudo state must be finite");
+  if (!cuda_ok(c, cudaSetDevice(c->device), "cudaSetDevice")) return CPS_ERR_CUDA;
+  return write_pseudo_state(c, state->pseudo_cfl, state->ser_resid_prev, state->ls_alpha, state->ls_backtracks)
+             ? CPS_OK
+             : CPS_ERR_CUDA;
 }
 
 cps_status cps_get_stream(cps_ctx* c, void** stream) {
@@ -759,6 +897,10 @@ cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVeloc
   std::string err;
   BatchWorkspace* ws = batch_workspace(c0->device, (size_t)n, err);
   if (!ws) return fail(c0, CPS_ERR_OOM, err);
+  // The batch kernels carry the pseudo-transient term and the CFL controllers
+  // only when a design of the batch has them on (a separate instantiation:
+  // compiled in, they slow every batched outer iteration by a quarter).
+  bool pseudo = false;
   for (int k = 0; k < n; ++k) {
     cps_ctx* c = ctxs[k];
     set_step_inputs(c, inletVelocity ? inletVelocity[k] : c->view.Uin);
@@ -771,6 +913,8 @@ cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVeloc
     it.eps = opts->eps;
     it.hist = c->dhist;
     it.hist_cap = kHistChunk;
+    it.iter0 = c->iter;
+    pseudo = pseudo || c->view.pseudo != 0;
   }
   std::vector<int> ord(n);
   std::iota(ord.begin(), ord.end(), 0);
@@ -789,8 +933,9 @@ cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVeloc
   if (opts->tiles_per_cta > 0) {
     // Groups sized to their designs, packed into waves (first fit, largest
     // first); one cooperative launch per wave, all CTAs of a wave co-resident.
-    const void* wk = c0->precision == CPS_MIXED ? (const void*)cps_wave_kernel<float>
-                                                : (const void*)cps_wave_kernel<double>;
+    const void* wk = c0->precision == CPS_MIXED
+                         ? (pseudo ? (const void*)cps_wave_kernel<float, true> : (const void*)cps_wave_kernel<float, false>)
+                         : (pseudo ? (const void*)cps_wave_kernel<double, true> : (const void*)cps_wave_kernel<double, false>);
     int per_sm = 0, sms = 0;
     const size_t tsm = tile_smem_for(c0->precision);
     if (!allow_smem(c0, wk, tsm) ||
@@ -849,8 +994,9 @@ cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVeloc
     }
   } else if (opts->group_ctas > 0) {
     // Groups of CTAs in one cooperative launch (all CTAs co-resident).
-    const void* gk = c0->precision == CPS_MIXED ? (const void*)cps_group_kernel<float>
-                                                : (const void*)cps_group_kernel<double>;
+    const void* gk = c0->precision == CPS_MIXED
+                         ? (pseudo ? (const void*)cps_group_kernel<float, true> : (const void*)cps_group_kernel<float, false>)
+                         : (pseudo ? (const void*)cps_group_kernel<double, true> : (const void*)cps_group_kernel<double, false>);
     int per_sm = 0, sms = 0;
     const size_t tsm = tile_smem_for(c0->precision);
     if (!allow_smem(c0, gk, tsm) ||
@@ -878,7 +1024,9 @@ cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVeloc
       return CPS_ERR_CUDA;
   } else {
   using KernFn = void (*)(const cps::BatchItem*, const int*, int, int*, cps::BatchResult*);
-  KernFn kern = c0->precision == CPS_MIXED ? (KernFn)cps_cluster_kernel<float> : (KernFn)cps_cluster_kernel<double>;
+  KernFn kern = c0->precision == CPS_MIXED
+                    ? (pseudo ? (KernFn)cps_cluster_kernel<float, true> : (KernFn)cps_cluster_kernel<float, false>)
+                    : (pseudo ? (KernFn)cps_cluster_kernel<double, true> : (KernFn)cps_cluster_kernel<double, false>);
   if (cl > 8 &&
       !cuda_ok(c0, cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1), "attr"))
     return CPS_ERR_CUDA;
@@ -927,6 +1075,7 @@ cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVeloc
                                                           : CPS_ERR_DIVERGED;
     to_step_out(r.last, &results[k].last);
     ctxs[k]->outer_done += r.n_done;
+    ctxs[k]->iter += r.n_done;
     if (r.status != cps::kStatusOk) {
       status = (cps_status)results[k].status;
       ctxs[k]->err = r.status == cps::kStatusTimeout ? "device group barrier timed out"

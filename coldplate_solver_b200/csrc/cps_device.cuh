@@ -122,6 +122,26 @@ struct DesignView {
   double dpSlopeMaxDelta; // dpSlopeMaxDelta
   double xPlane[4];       // core inlet, core outlet, x = 0, x = N hx
   double* dpHist;         // dpWindow circular slots, then dpSlopeWindow slots (slot = iter mod window)
+  // Pseudo-transient term of the momentum equations and the outer loop's CFL
+  // controllers (SIMPLE.h:255-313); pseudo = 0 leaves both out.
+  int pseudo;             // enablePseudoTimeStepping
+  int pseudoLocal;        // useLocalPseudoTime
+  int serOn, lsOn, rampOn; // enableSER, enableLineSearch, enableCflRamp
+  int serUseMax;          // serUseMaxResid: SER watches the step's error instead of residMass
+  int serMinIter, lsMaxTries;
+  double timeStep;        // timeStepMultiplier * N hx / max(targetVel, 1e-6) (SIMPLE.cpp:68-70)
+  double minPseudoSpeed, hChar;  // hChar = min(hx, hy)
+  double cflInitial, cflMax, rampStartRes, rampExponent, rampSmooth;
+  double serCFLMin, serCFLMax, serSmooth, serMaxIncrease, serMaxDecrease;
+  double lsAlphaMin, lsAlphaReduce, lsTol;
+  double* pseudoState;    // pseudoCFL, serResidPrev, lsCurrentAlpha, lsBacktrackCount (across launches)
+};
+
+// The CFL controllers' state while a design runs; every CTA keeps a copy in
+// shared memory and updates it identically from the grid-reduced residuals.
+struct PseudoRun {
+  double cfl, prev, alpha;
+  int count, pad;
 };
 
 template <typename T> __device__ __forceinline__ const Inner<T>& inner(const DesignView& d);
@@ -149,7 +169,7 @@ struct BatchItem {
   double eps;
   double* hist;       // hist_cap x 8 (the first hist_cap iterations of the visit), may be null
   int hist_cap;
-  int pad;
+  int iter0;          // the outer loop's iteration index of the visit's first iteration
 };
 struct BatchResult {
   int n_done;         // outer iterations run in this visit
@@ -170,6 +190,105 @@ struct GridBarrier {
 __device__ __forceinline__ double maxd(double a, double b) { return (a < b) ? b : a; }
 __device__ __forceinline__ double mind(double a, double b) { return (b < a) ? b : a; }
 __device__ __forceinline__ double clampd(double v, double lo, double hi) { return (v < lo) ? lo : (hi < v) ? hi : v; }
+
+// ---------------------------------------------------------------------------
+// Pseudo-transient term and CFL controllers
+// ---------------------------------------------------------------------------
+// rho vol / dt of the implicit assembly at a point whose current velocity is
+// vel (momentum_solver.cpp:231-241).
+__device__ __forceinline__ double trans_implicit(const DesignView& d, double cfl, double vel) {
+  double dtLocal = maxd(d.timeStep, 1e-20);
+  if (d.pseudoLocal) {
+    const double speed = maxd(fabs(vel), d.minPseudoSpeed);
+    dtLocal = mind(dtLocal, cfl * d.hChar / speed);
+    dtLocal = maxd(dtLocal, 1e-20);
+  }
+  return d.rho * d.vol / dtLocal;
+}
+
+// The same coefficient of the explicit update, from computeLocalDt
+// (iterations.cpp:207-217, 290-294).
+__device__ __forceinline__ double trans_explicit(const DesignView& d, double cfl, double vel) {
+  double dtLocal = d.timeStep;
+  if (d.pseudoLocal) {
+    const double speed = maxd(fabs(vel), d.minPseudoSpeed);
+    dtLocal = mind(d.timeStep, cfl * d.hChar / speed);
+  }
+  return d.rho * d.vol / dtLocal;
+}
+
+// The outer loop's controllers after the step with index `iteration`
+// (SIMPLE.cpp:321-327): updateCflSER (time_control.cpp:82-118),
+// applyLineSearch (:127-166), updateCflRamp (:43-63), in that order; resid is
+// the monitoring residual.  The ramp's power is CUDA's pow, which may differ
+// from the host's in the last bit.
+__device__ __forceinline__ void pseudo_update(const DesignView& d, PseudoRun& s, double resid, int iteration) {
+  double cfl = s.cfl, prev = s.prev, alpha = s.alpha;
+  int count = s.count;
+  if (d.serOn && iteration >= d.serMinIter) {
+    const double cur = maxd(resid, 1e-15);
+    if (prev <= 0.0) {
+      prev = cur;
+    } else {
+      double ratio = prev / cur;
+      ratio = maxd(ratio, d.serMaxDecrease);
+      ratio = mind(ratio, d.serMaxIncrease);
+      double target = cfl * ratio;
+      target = maxd(target, d.serCFLMin);
+      target = mind(target, d.serCFLMax);
+      cfl = (1.0 - d.serSmooth) * cfl + d.serSmooth * target;
+      if (!isfinite(cfl) || cfl <= 0.0) cfl = d.serCFLMin;
+      prev = cur;
+    }
+  }
+  if (d.lsOn && d.serOn) {
+    if (prev <= 0.0) {
+      alpha = 1.0;
+      count = 0;
+    } else if (resid / prev > d.lsTol) {
+      ++count;
+      if (count <= d.lsMaxTries) {
+        alpha = maxd(alpha * d.lsAlphaReduce, d.lsAlphaMin);
+        cfl = maxd(cfl * d.lsAlphaReduce, d.serCFLMin);
+      }
+    } else {
+      if (alpha < 1.0) alpha = mind(alpha * 1.1, 1.0);
+      count = 0;
+    }
+  }
+  if (d.rampOn && !d.serOn) {
+    const double cur = maxd(resid, 1e-12);
+    if (cur > d.rampStartRes) {
+      cfl = d.cflInitial;
+    } else {
+      const double rawFactor = pow(d.rampStartRes / cur, d.rampExponent);
+      const double target = mind(d.cflInitial * rawFactor, d.cflMax);
+      cfl = (1.0 - d.rampSmooth) * cfl + d.rampSmooth * target;
+      if (!isfinite(cfl) || cfl <= 0.0) cfl = d.cflInitial;
+    }
+  }
+  s.cfl = cfl;
+  s.prev = prev;
+  s.alpha = alpha;
+  s.count = count;
+}
+
+// Thread 0 loads a design's controller state at the start of its run; the
+// caller synchronises the CTA before the state is read.
+__device__ __forceinline__ void load_pseudo(const DesignView& d, PseudoRun& s) {
+  if (threadIdx.x != 0) return;
+  if (d.pseudo && d.pseudoState) {
+    s.cfl = __ldcg(d.pseudoState);
+    s.prev = __ldcg(d.pseudoState + 1);
+    s.alpha = __ldcg(d.pseudoState + 2);
+    s.count = (int)__ldcg(d.pseudoState + 3);
+  } else {
+    s.cfl = 0.0;
+    s.prev = 0.0;
+    s.alpha = 1.0;
+    s.count = 0;
+  }
+}
 
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
   unsigned long long v;
@@ -587,8 +706,9 @@ __device__ __forceinline__ double sou_correction(const DesignView& d, const X& x
 // squared residual of sweep 1 (0 when no sweep is run).
 //   FP64:  b = Sp, x1 = x0 + (b - A x0)/aP.
 //   mixed: b = r0 = Sp - A x0 (FP64 defect), delta1 = r0/aP (delta0 = 0).
-template <bool IsU, typename T>
-__device__ __forceinline__ double assemble_point(const DesignView& d, const LayoutA& L, int i, int j, bool sweep) {
+template <bool IsU, typename T, bool Pseudo>
+__device__ __forceinline__ double assemble_point(const DesignView& d, const LayoutA& L, int i, int j, bool sweep,
+                                                 double cfl) {
   constexpr bool kMixed = sizeof(T) == 4;
   const Inner<T>& w = inner<T>(d);
   const int M = d.M, N = d.N, P = d.P;
@@ -613,13 +733,13 @@ __device__ __forceinline__ double assemble_point(const DesignView& d, const Layo
   const double aE = d.De + maxd(0.0, -Fe), aW = d.De + maxd(0.0, Fw);
   const double aN = d.Dn + maxd(0.0, -Fn), aS = d.Dn + maxd(0.0, Fs);
   const double sumA = aE + aW + aN + aS;
-  const double transCoeff = 0.0;  // pseudo-transient off
+  const auto& X = IsU ? u : v;
+  const double velCur = X(i, j);
+  const double transCoeff = (Pseudo && d.pseudo) ? trans_implicit(d, cfl, velCur) : 0.0;
   const double brinkmanDrag = alphaLocal * d.vol;
   double aP0 = sumA + (Fe - Fw + Fn - Fs) + transCoeff + d.sinkDiag + brinkmanDrag;
   aP0 = maxd(aP0, 1e-10);
   const double aP = aP0 / d.uvAlpha;
-  const auto& X = IsU ? u : v;
-  const double velCur = X(i, j);
   double Sp = IsU ? (L.p(i, j) - L.p(i, j + 1)) * d.hy : (L.p(i, j) - L.p(i + 1, j)) * d.hx;
   Sp += transCoeff * velCur;
   Sp += d.relax * aP0 * velCur;
@@ -667,13 +787,13 @@ __device__ __forceinline__ double assemble_point(const DesignView& d, const Layo
 }
 
 // The explicit momentum update at one unknown (momentumSolverType = 0,
-// iterations.cpp:254-412, pseudo-transient off so the transient coefficient
+// iterations.cpp:254-412; with the pseudo-transient term off its coefficient
 // is rho vol / inf = 0): the full coefficients, one point update from the
 // current velocities, clamped to +-maxVel; d = h / max(aP0, 1e-12).  Its
 // result goes where phase C reads the final Jacobi iterate (FP64: the value;
 // mixed: its difference to the current velocity).
-template <bool IsU, typename T>
-__device__ __forceinline__ void explicit_point(const DesignView& d, const LayoutA& L, int i, int j) {
+template <bool IsU, typename T, bool Pseudo>
+__device__ __forceinline__ void explicit_point(const DesignView& d, const LayoutA& L, int i, int j, double cfl) {
   constexpr bool kMixed = sizeof(T) == 4;
   const Inner<T>& w = inner<T>(d);
   const int P = d.P;
@@ -701,13 +821,13 @@ __device__ __forceinline__ void explicit_point(const DesignView& d, const Layout
   const auto& X = IsU ? u : v;
   const double Sdc = (d.conv == 1) ? sou_correction<IsU>(d, X, i, j, Fe, Fw, Fn, Fs) : 0.0;
   const double sumA = aE + aW + aN + aS;
-  const double transCoeffLocal = 0.0;
+  const double velCur = X(i, j);
+  const double transCoeffLocal = (Pseudo && d.pseudo) ? trans_explicit(d, cfl, velCur) : 0.0;
   const double brinkmanDrag = alphaLocal * d.vol;
   double aP0 = sumA + (Fe - Fw + Fn - Fs) + transCoeffLocal + d.sinkDiag + brinkmanDrag;
   aP0 = maxd(aP0, 1e-10);
   const double dDenom = maxd(aP0, 1e-12);
   const size_t o = (size_t)i * P + j;
-  const double velCur = X(i, j);
   double Sp;
   if (IsU) {
     d.dE[o] = d.hy / dDenom;
@@ -1506,22 +1626,25 @@ constexpr size_t tile_smem_bytes() {
 
 // ---------------------------------------------------------------------------
 // One outer iteration for one design on group g; out[8] receives the step
-// diagnostics.  tbuf: tile_smem_bytes<T>() of shared memory.  With Monitor
-// (compiled in for the single-design kernel only) and d.dpMonitor, iter is the
-// outer loop's iteration index, dplog (may be null)
-// receives its four pressure drops and *dpConverged is set when the
-// pressure-drop gate ends the loop.  Returns 0 to continue with another outer
+// diagnostics.  tbuf: tile_smem_bytes<T>() of shared memory.  iter is the
+// outer loop's iteration index of this step.  With Monitor (compiled in for
+// the single-design kernel only) and d.dpMonitor, dplog (may be null) receives
+// its four pressure drops and *dpConverged is set when the pressure-drop gate
+// ends the loop.  pr (may be null) holds the CTA's copy of the CFL
+// controllers' state when d.pseudo; Pseudo = false compiles the
+// pseudo-transient term and the controllers out.  Returns 0 to continue with another outer
 // iteration, 1 when this one is the last (iteration budget, convergence, the
 // pressure-drop gate, or a non-finite residual), -1 when the group must stop
 // because a device-side wait failed.
 // ---------------------------------------------------------------------------
-template <typename T, class Group, bool Monitor = false>
+template <typename T, class Group, bool Monitor = false, bool Pseudo = true>
 __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char* tbuf, double (&out)[8],
                                bool lastIter, bool stopOnConv, double eps, int iter = 0, double* dplog = nullptr,
-                               int* dpConverged = nullptr) {
+                               int* dpConverged = nullptr, PseudoRun* pr = nullptr) {
   const Inner<T>& w = inner<T>(d);
   const int M = d.M, N = d.N, P = d.P;
   // ---- A: assembly + sweep 1 (or the explicit update) ----
+  const double cfl = (Pseudo && d.pseudo && pr) ? pr->cfl : 0.0;
   const bool expl = d.momExplicit != 0;
   const bool anySweep = !expl && d.maxMomIter > 0;
   double red2[2] = {0.0, 0.0};
@@ -1536,12 +1659,12 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
       [&](const LayoutA& L, int i, int j, bool inside) {
         if (!inside) return;
         if (expl) {
-          if (j <= N - 2) explicit_point<true, T>(d, L, i, j);
-          if (i <= M - 2) explicit_point<false, T>(d, L, i, j);
+          if (j <= N - 2) explicit_point<true, T, Pseudo>(d, L, i, j, cfl);
+          if (i <= M - 2) explicit_point<false, T, Pseudo>(d, L, i, j, cfl);
           return;
         }
-        if (j <= N - 2) red2[0] += assemble_point<true, T>(d, L, i, j, anySweep);
-        if (i <= M - 2) red2[1] += assemble_point<false, T>(d, L, i, j, anySweep);
+        if (j <= N - 2) red2[0] += assemble_point<true, T, Pseudo>(d, L, i, j, anySweep, cfl);
+        if (i <= M - 2) red2[1] += assemble_point<false, T, Pseudo>(d, L, i, j, anySweep, cfl);
       });
   if (!g.template sync_reduce<2, 0u>(red2, smem)) return -1;
   int kU = anySweep ? 1 : 0, kV = kU;
@@ -1587,6 +1710,18 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
   const bool finite = isfinite(e) && isfinite(out[3]) && rc[4] == 0.0;
   if (!finite && g.rank == 0 && threadIdx.x == 0 && g.status) atomicCAS(g.status, kStatusOk, kStatusDiverged);
   const bool stop = lastIter || !finite || (stopOnConv && conv <= eps);
+  // The CFL controllers (SIMPLE.cpp:321-327).  Every CTA's thread 0 updates its
+  // copy from the same reduced residuals; the barriers before the next phase A
+  // publish it to the CTA.
+  if (Pseudo && d.pseudo && pr && threadIdx.x == 0) {
+    pseudo_update(d, *pr, d.serUseMax ? out[4] : out[2], iter);
+    if (g.rank == 0 && d.pseudoState) {
+      d.pseudoState[0] = pr->cfl;
+      d.pseudoState[1] = pr->prev;
+      d.pseudoState[2] = pr->alpha;
+      d.pseudoState[3] = (double)pr->count;
+    }
+  }
   // ---- P: Jacobi-preconditioned CG ----
   if (d.pcgSingleReduction) {
     const int its = pcg_single_reduction<T>(d, g, smem, rc[5], rc[6]);

@@ -78,12 +78,32 @@ void ensure_device(SIMPLE& s) {
   g_dev.N = s.N;
   const std::vector<double> u = to_double(s.u), v = to_double(s.v), p = to_double(s.p);
   check(cps_upload_fields(ctx, u.data(), v.data(), p.data(), CPS_COL_MAJOR), "cps_upload_fields");
+  if (s.enablePseudoTimeStepping) {
+    // The pseudo-transient term with the global time step the constructor set
+    // (SIMPLE.cpp:68-70); the CFL controllers stay the reference's own, on the
+    // host (SIMPLE.cpp:321-327), and hand their CFL number to every step.
+    cps_pseudo ps;
+    cps_pseudo_defaults(&ps, static_cast<double>(s.targetVel));
+    ps.enable = 1;
+    ps.use_local = s.useLocalPseudoTime ? 1 : 0;
+    ps.enable_ser = 0;
+    ps.enable_line_search = 0;
+    ps.enable_cfl_ramp = 0;
+    ps.min_pseudo_speed = s.minPseudoSpeed;
+    ps.pseudo_cfl = s.pseudoCFL;
+    ps.time_step = s.timeStep;
+    check(cps_set_pseudo(ctx, &ps), "cps_set_pseudo");
+  }
 }
 
 }  // namespace
 
 real b200StepDropIn(SIMPLE& s, int& pressureIterations) {
   ensure_device(s);
+  if (s.enablePseudoTimeStepping) {
+    cps_pseudo_state st = {static_cast<double>(s.pseudoCFL), 0.0, 1.0, 0, 0};
+    check(cps_set_pseudo_state(g_dev.ctx, &st), "cps_set_pseudo_state");
+  }
   cps_step_in in = {static_cast<double>(s.inletVelocity)};
   cps_step_out out = {};
   check(cps_step(g_dev.ctx, &in, &out), "cps_step");

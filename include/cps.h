@@ -190,6 +190,73 @@ cps_status cps_set_dp_monitor(cps_ctx* ctx, const cps_dp_monitor* m);
 cps_status cps_solve_monitored(cps_ctx* ctx, double inletVelocity, int max_outer, double eps, cps_step_out* history,
                                double* dp_history, int* n_done, int* dp_converged);
 
+/* Pseudo-transient term of the momentum equations and the outer loop's CFL
+ * controllers (SIMPLE.h:255-313; momentum_solver.cpp:231-241 and
+ * iterations.cpp:189-217 for the term, time_control.cpp:43-166 with
+ * SIMPLE.cpp:321-327 for the controllers).  With enable set, every momentum
+ * unknown gets rho hx hy / dt on its diagonal and times its current velocity
+ * in its source, dt = min(time_step, pseudo_cfl min(hx, hy) / max(|vel|,
+ * min_pseudo_speed)) with use_local (else time_step), and after every outer
+ * iteration SER (Switched Evolution Relaxation), its line search and the
+ * residual ramp update pseudo_cfl from residMass (or, with
+ * ser_use_max_resid, the step's error).  time_step =
+ * time_step_multiplier * N hx / max(target_velocity, 1e-6) (SIMPLE.cpp:68-70)
+ * unless given. */
+typedef struct {
+  int    enable;                /* enablePseudoTimeStepping (SIMPLE.h:262) */
+  int    use_local;             /* useLocalPseudoTime */
+  int    enable_ser;            /* enableSER */
+  int    enable_line_search;    /* enableLineSearch */
+  int    enable_cfl_ramp;       /* enableCflRamp (ignored while SER is on) */
+  int    ser_use_max_resid;     /* serUseMaxResid */
+  int    ser_min_iter;          /* serMinIter */
+  int    ls_max_tries;          /* lsMaxTries */
+  double target_velocity;       /* targetVel [m/s] */
+  double time_step_multiplier;  /* timeStepMultiplier */
+  double min_pseudo_speed;      /* minPseudoSpeed [m/s] */
+  double pseudo_cfl;            /* pseudoCFL: the starting CFL number when the ramp is off */
+  double cfl_initial;           /* pseudoCFLInitial: the starting CFL number when the ramp is on */
+  double cfl_max;               /* pseudoCFLMax */
+  double cfl_ramp_start_res;    /* cflRampStartRes */
+  double cfl_ramp_exponent;     /* cflRampExponent */
+  double cfl_ramp_smooth;       /* cflRampSmooth */
+  double ser_cfl_min;           /* serCFLMin */
+  double ser_cfl_max;           /* serCFLMax */
+  double ser_smooth;            /* serSmooth */
+  double ser_max_increase;      /* serMaxIncrease */
+  double ser_max_decrease;      /* serMaxDecrease */
+  double ls_alpha_min;          /* lsAlphaMin */
+  double ls_alpha_reduce;       /* lsAlphaReduce */
+  double ls_resid_increase_tol; /* lsResidIncreaseTol */
+  double time_step;             /* > 0: the global pseudo time step timeStep [s] itself, in place of the formula */
+} cps_pseudo;
+
+/* The controllers' state carried from one outer iteration to the next. */
+typedef struct {
+  double pseudo_cfl;      /* pseudoCFL: the CFL number of the next step */
+  double ser_resid_prev;  /* serResidPrev */
+  double ls_alpha;        /* lsCurrentAlpha */
+  int    ls_backtracks;   /* lsBacktrackCount */
+  int    pad;
+} cps_pseudo_state;
+
+/* The reference's defaults (SIMPLE.h:255-313), enable = 0. */
+cps_status cps_pseudo_defaults(cps_pseudo* p, double target_velocity);
+
+/* Switch the term and controllers on (p->enable) or off (p == NULL or
+ * !p->enable) for every later step, solve and batch of ctx; resets the
+ * controllers' state to its start (pseudo_cfl = cfl_initial with the ramp on,
+ * else pseudo_cfl; ser_resid_prev 0; ls_alpha 1; ls_backtracks 0).  The
+ * outer-loop iteration index that serMinIter counts restarts at 0 with
+ * cps_reset_fields. */
+cps_status cps_set_pseudo(cps_ctx* ctx, const cps_pseudo* p);
+
+/* Read or overwrite the controllers' state (a caller that runs the
+ * controllers itself, such as the reference's own outer loop, sets the CFL
+ * number before each cps_step). */
+cps_status cps_get_pseudo_state(cps_ctx* ctx, cps_pseudo_state* state);
+cps_status cps_set_pseudo_state(cps_ctx* ctx, const cps_pseudo_state* state);
+
 /* Options of a batched solve. */
 typedef struct {
   int cluster_ctas;   /* CTAs of the thread-block cluster that runs one design (1..16; 0 = 8) */

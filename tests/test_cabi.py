@@ -47,6 +47,8 @@ int main(void) {
          sizeof(cps_dp_monitor), offsetof(cps_dp_monitor, ramp_steps), offsetof(cps_dp_monitor, x_core_out));
   printf("%zu %zu %zu\n", sizeof(cps_case_params), offsetof(cps_case_params, N_in_buffer),
          offsetof(cps_case_params, has_Ht));
+  printf("%zu %zu %zu %zu %zu\n", sizeof(cps_pseudo), offsetof(cps_pseudo, target_velocity),
+         offsetof(cps_pseudo, ls_resid_increase_tol), sizeof(cps_pseudo_state), offsetof(cps_pseudo_state, ls_backtracks));
   return 0;
 }'''
     with tempfile.TemporaryDirectory() as t:
@@ -58,7 +60,10 @@ int main(void) {
           cps.CpsDesc.grid_ctas.offset, ctypes.sizeof(cps.CpsStepOut), cps.CpsStepOut.vSweeps.offset,
           ctypes.sizeof(cps.CpsPlane), ctypes.sizeof(cps.CpsBatchOpts), cps.CpsBatchOpts.tiles_per_cta.offset,
           ctypes.sizeof(cps.CpsDpMonitor), cps.CpsDpMonitor.ramp_steps.offset, cps.CpsDpMonitor.x_core_out.offset,
-          ctypes.sizeof(cps.CpsCaseParams), cps.CpsCaseParams.N_in_buffer.offset, cps.CpsCaseParams.has_Ht.offset]
+          ctypes.sizeof(cps.CpsCaseParams), cps.CpsCaseParams.N_in_buffer.offset, cps.CpsCaseParams.has_Ht.offset,
+          ctypes.sizeof(cps.CpsPseudo), cps.CpsPseudo.target_velocity.offset,
+          cps.CpsPseudo.ls_resid_increase_tol.offset, ctypes.sizeof(cps.CpsPseudoState),
+          cps.CpsPseudoState.ls_backtracks.offset]
     assert vals == py
 
 

@@ -38,3 +38,24 @@ def test_reference_driver_with_b200_branch(case):
     for k in FIELDS:
         assert rel(a[k], b[k]) <= 1e-10, (k, rel(a[k], b[k]))
     np.testing.assert_allclose(a["planes"], b["planes"], rtol=1e-10, atol=1e-300)
+
+
+@pytest.mark.parametrize("mom", [1, 0])
+def test_reference_driver_with_pseudo_transient(mom):
+    """The pseudo-transient term through the drop-in: the reference's own CFL
+    controllers run on the host after every step and hand the CFL number to
+    the next B200 step."""
+    from oracle import reference
+    if not (reference.available("dropin") and reference.available("f64")):
+        pytest.skip("reference binaries not built in this checkout")
+    d = geometry.channel_network(M=40, N=72, h=20e-6, wmin=4, wmax=8, seed=5).replace(
+        enablePseudoTimeStepping=True, serMinIter=3, momentumSolverType=mom, uvAlpha=0.5 if mom == 0 else 0.7)
+    n = 15
+    a = reference.run(d, n, precision="dropin")
+    b = reference.run(d, n, precision="f64")
+    assert np.array_equal(a["pIters"], b["pIters"])
+    for k in ("residU", "residV", "residMass", "err"):
+        np.testing.assert_allclose(a[k], b[k], rtol=1e-8, atol=1e-300)
+    np.testing.assert_allclose(a["pseudoCFL"], b["pseudoCFL"], rtol=1e-9)
+    for k in FIELDS:
+        assert rel(a[k], b[k]) <= 1e-10, (k, rel(a[k], b[k]))
