@@ -151,6 +151,7 @@ SIGNATURES = {
     "cps_solve_monitored": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                            ctypes.POINTER(CpsStepOut), _D, ctypes.POINTER(ctypes.c_int),
                                            ctypes.POINTER(ctypes.c_int)]),
+    "cps_set_inlet_ramp": (ctypes.c_int, [_P, ctypes.c_int]),
     "cps_pseudo_defaults": (ctypes.c_int, [ctypes.POINTER(CpsPseudo), ctypes.c_double]),
     "cps_set_pseudo": (ctypes.c_int, [_P, ctypes.POINTER(CpsPseudo)]),
     "cps_get_pseudo_state": (ctypes.c_int, [_P, ctypes.POINTER(CpsPseudoState)]),
@@ -247,6 +248,8 @@ class Solver:
         self.inletVelocity = design.inletVelocity
         if design.enablePseudoTimeStepping:
             self.set_pseudo(design)
+        if design.enableInletRamp and design.rampSteps > 0:
+            self.set_inlet_ramp(design.rampSteps)
 
     def _check(self, st: int) -> None:
         if st != CPS_OK:
@@ -331,6 +334,11 @@ class Solver:
         switches the term off.  Resets the CFL controllers' state."""
         p = pseudo_from_design(self.design if design is None else design)
         self._check(self.lib.cps_set_pseudo(self.ctx, ctypes.byref(p)))
+
+    def set_inlet_ramp(self, ramp_steps: int) -> None:
+        """cps_set_inlet_ramp: solve() and solve_monitored() ramp the inlet
+        velocity over the first ``ramp_steps`` outer iterations (0: off)."""
+        self._check(self.lib.cps_set_inlet_ramp(self.ctx, int(ramp_steps)))
 
     def pseudo_state(self) -> Dict[str, float]:
         """The CFL controllers' state: pseudo_cfl, ser_resid_prev, ls_alpha,

@@ -70,6 +70,7 @@ struct cps_ctx {
   double* ddphist = nullptr; // device, the pressure-drop gate's windows (cudaMalloc'd by cps_set_dp_monitor)
   double* dpseudo = nullptr; // device, the CFL controllers' state (4 doubles)
   double pseudo_start = 0.0; // the controllers' starting CFL number
+  int ramp_steps = 0;        // inlet velocity ramp of cps_solve (0: off)
   int iter = 0;              // outer-loop iteration index of the next iteration (monitor and gate)
   int grid = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -408,12 +409,22 @@ void to_step_out(const double* h, cps_step_out* o) {
 }
 
 cps_status run(cps_ctx* c, int n_outer, int stop_on_conv, double eps, cps_step_out* hist, int* n_done,
-               double* dp_history = nullptr, int* dp_converged = nullptr) {
+               double* dp_history = nullptr, int* dp_converged = nullptr, bool ramp = false) {
   int done_total = 0;
   const bool monitor = c->view.dpMonitor != 0;
+  const double target = c->view.Uin;
   if (dp_converged) *dp_converged = 0;
   while (done_total < n_outer) {
-    const int chunk = std::min(kHistChunk, n_outer - done_total);
+    int chunk = std::min(kHistChunk, n_outer - done_total);
+    if (ramp && c->ramp_steps > 0) {
+      // SIMPLE.cpp:303-307: one launch per ramp iteration, each with its own inlet velocity
+      if (c->iter < c->ramp_steps) {
+        chunk = 1;
+        set_step_inputs(c, ((double)(c->iter + 1) / c->ramp_steps) * target);
+      } else {
+        set_step_inputs(c, target);
+      }
+    }
     cps::RunControl rc{chunk, stop_on_conv, eps, c->dhist, c->dndone, c->dstatus, c->iter,
                        monitor ? c->dplog : nullptr, c->dstatus + 2};
     if (!cuda_ok(c, cudaMemsetAsync(c->dndone, 0, 2 * sizeof(int), c->stream), "memset") ||
@@ -457,6 +468,7 @@ cps_status run(cps_ctx* c, int n_outer, int stop_on_conv, double eps, cps_step_o
     }
     if (nd < chunk) break;  // converged
   }
+  if (ramp && c->ramp_steps > 0) set_step_inputs(c, target);
   return CPS_OK;
 }
 
@@ -828,7 +840,14 @@ cps_status cps_solve(cps_ctx* c, double inletVelocity, int max_outer, double eps
   if (max_outer == 0) return CPS_OK;
   if (!cuda_ok(c, cudaSetDevice(c->device), "cudaSetDevice")) return CPS_ERR_CUDA;
   set_step_inputs(c, inletVelocity);
-  return run(c, max_outer, eps > 0.0 ? 1 : 0, eps, history, n_done);
+  return run(c, max_outer, eps > 0.0 ? 1 : 0, eps, history, n_done, nullptr, nullptr, true);
+}
+
+cps_status cps_set_inlet_ramp(cps_ctx* c, int ramp_steps) {
+  if (!c) return fail(nullptr, CPS_ERR_ARG, "ctx is NULL");
+  if (ramp_steps < 0) return fail(c, CPS_ERR_ARG, "ramp_steps < 0");
+  c->ramp_steps = ramp_steps;
+  return CPS_OK;
 }
 
 cps_status cps_set_dp_monitor(cps_ctx* c, const cps_dp_monitor* m) {
@@ -877,7 +896,7 @@ cps_status cps_solve_monitored(cps_ctx* c, double inletVelocity, int max_outer, 
   if (max_outer == 0) return CPS_OK;
   if (!cuda_ok(c, cudaSetDevice(c->device), "cudaSetDevice")) return CPS_ERR_CUDA;
   set_step_inputs(c, inletVelocity);
-  return run(c, max_outer, eps > 0.0 ? 1 : 0, eps, history, n_done, dp_history, dp_converged);
+  return run(c, max_outer, eps > 0.0 ? 1 : 0, eps, history, n_done, dp_history, dp_converged, true);
 }
 
 cps_status cps_batch_solve(cps_ctx* const* ctxs, int n, const double* inletVelocity, const cps_batch_opts* opts,

@@ -97,6 +97,10 @@ class Design:
     cflRampStartRes: float = 1e-4
     cflRampExponent: float = 0.8
     cflRampSmooth: float = 0.1
+    # Inlet velocity ramp of the outer loop (SIMPLE.h:345-346, SIMPLE.cpp:303-307): for the first
+    # rampSteps iterations the inlet velocity is (iter + 1) / rampSteps of inletVelocity.
+    enableInletRamp: bool = False
+    rampSteps: int = 1000
 
     def __post_init__(self) -> None:
         self.gamma = np.ascontiguousarray(self.gamma, dtype=np.float64)
@@ -133,7 +137,8 @@ class Design:
                          int(self.enableConvectionScaling), self.maxPressureIter, self.maxMomentumIter,
                          self.momentumSolverType, int(self.enablePseudoTimeStepping), int(self.useLocalPseudoTime),
                          int(self.enableSER), int(self.enableLineSearch), int(self.enableCflRamp),
-                         int(self.serUseMaxResid), self.serMinIter, self.lsMaxTries], dtype=np.int32)
+                         int(self.serUseMaxResid), self.serMinIter, self.lsMaxTries, int(self.enableInletRamp),
+                         self.rampSteps], dtype=np.int32)
 
     def real_params(self, pseudo_cfl: Optional[float] = None) -> np.ndarray:
         """dp[27] is the CFL number the step uses (default: the first step's)."""

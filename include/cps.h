@@ -75,7 +75,7 @@ typedef struct {
                                      (Chronopoulos-Gear recurrences: one reduction per iteration) */
   int momentum_explicit;          /* 0: implicit Jacobi momentum (momentumSolverType = 1, SIMPLE.h:172);
                                      1: the explicit point update (momentumSolverType = 0,
-                                     iterations.cpp:176-441, pseudo-transient off) */
+                                     iterations.cpp:176-441) */
 } cps_desc;
 
 /* PCG recurrences (same Krylov iterates in exact arithmetic). */
@@ -141,7 +141,9 @@ cps_status cps_download_fields(cps_ctx* ctx, double* u, double* v, double* p, do
 cps_status cps_upload_geometry(cps_ctx* ctx, const double* alpha, const double* gamma, int layout);
 
 /* Zero u, v, p and every derived field on the device: the state cps_create
- * leaves (SIMPLE.cpp:184-197), without a host copy. */
+ * leaves (SIMPLE.cpp:184-197), without a host copy.  Also restarts the
+ * outer-loop iteration index (inlet ramp, serMinIter, pressure-drop window)
+ * and the CFL controllers' state, as a fresh solve of the reference does. */
 cps_status cps_reset_fields(cps_ctx* ctx);
 
 /* The cudaStream_t (as void*) every call of this context issues its work on,
@@ -256,6 +258,15 @@ cps_status cps_set_pseudo(cps_ctx* ctx, const cps_pseudo* p);
  * number before each cps_step). */
 cps_status cps_get_pseudo_state(cps_ctx* ctx, cps_pseudo_state* state);
 cps_status cps_set_pseudo_state(cps_ctx* ctx, const cps_pseudo_state* state);
+
+/* The outer loop's inlet velocity ramp (enableInletRamp && rampSteps > 0,
+ * SIMPLE.cpp:303-307): in cps_solve and cps_solve_monitored, outer iteration
+ * iter < ramp_steps runs with inlet velocity ((iter + 1) / ramp_steps) times
+ * the call's inletVelocity (iter: the context's outer-loop index, restarted by
+ * cps_reset_fields).  Those iterations run one launch each.  ramp_steps = 0
+ * switches it off.  cps_step and cps_batch_solve take their inlet velocities
+ * from the caller as given. */
+cps_status cps_set_inlet_ramp(cps_ctx* ctx, int ramp_steps);
 
 /* Options of a batched solve. */
 typedef struct {

