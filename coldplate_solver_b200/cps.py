@@ -118,6 +118,22 @@ def pseudo_from_design(design: Design) -> CpsPseudo:
                      ls_resid_increase_tol=d.lsResidIncreaseTol)
 
 
+class CpsThermalDesc(ctypes.Structure):
+    _fields_ = [("Nx", ctypes.c_int), ("Ny", ctypes.c_int), ("nz_solid", ctypes.c_int), ("nz_fluid", ctypes.c_int),
+                ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("H_b", ctypes.c_double), ("H_t", ctypes.c_double),
+                ("k_s", ctypes.c_double), ("k_f", ctypes.c_double), ("rho", ctypes.c_double), ("Cp", ctypes.c_double),
+                ("T_inlet", ctypes.c_double), ("rtol", ctypes.c_double), ("maxiter", ctypes.c_int),
+                ("k_interp_mode", ctypes.c_int), ("qk", ctypes.c_double), ("gamma", ctypes.c_void_p),
+                ("u", ctypes.c_void_p), ("v", ctypes.c_void_p), ("q0", ctypes.c_void_p), ("q", ctypes.c_double),
+                ("device", ctypes.c_int), ("mg_sweeps", ctypes.c_int), ("mg_omega", ctypes.c_double),
+                ("mg_overcorrect", ctypes.c_double)]
+
+
+class CpsThermalResult(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("converged", ctypes.c_int), ("rel_residual", ctypes.c_double),
+                ("true_rel_residual", ctypes.c_double)]
+
+
 class CpsBatchResult(ctypes.Structure):
     _fields_ = [("n_done", ctypes.c_int), ("converged", ctypes.c_int), ("status", ctypes.c_int),
                 ("last", CpsStepOut)]
@@ -164,6 +180,16 @@ SIGNATURES = {
     "cps_save_all": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                     ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D, _D, ctypes.c_int]),
     "cps_io_last_error": (ctypes.c_char_p, []),
+    "cps_thermal_defaults": (ctypes.c_int, [ctypes.POINTER(CpsThermalDesc)]),
+    "cps_thermal_create": (ctypes.c_int, [ctypes.POINTER(CpsThermalDesc), ctypes.POINTER(_P)]),
+    "cps_thermal_update": (ctypes.c_int, [_P, _D, _D, _D, _D]),
+    "cps_thermal_solve": (ctypes.c_int, [_P, ctypes.POINTER(CpsThermalResult)]),
+    "cps_thermal_download": (ctypes.c_int, [_P, _D]),
+    "cps_thermal_system": (ctypes.c_int, [_P, _D, _D]),
+    "cps_thermal_timing": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int),
+                                          ctypes.c_int]),
+    "cps_thermal_destroy": (None, [_P]),
+    "cps_thermal_last_error": (ctypes.c_char_p, [_P]),
     "cps_last_error": (ctypes.c_char_p, [_P]),
     "cps_version": (ctypes.c_char_p, []),
 }

@@ -1,0 +1,232 @@
+"""The 3-D conjugate-heat-transfer step downstream of the flow solve, on the
+GPU (include/cps_thermal.h): the system of ThermalSolver3D::solve
+(ThermalSolver/thermal_solver.cpp:420-560) assembled on the device and solved
+by multigrid-preconditioned BiCGStab.
+
+A ``ThermalCase`` carries the reference's Params (thermal_solver.cpp:147-193)
+and the 2-D inputs its main() loads (:706-760): gamma (1 = fluid), the
+cell-centred velocities of the thermal crop and the base heat flux.
+``ThermalCase.from_export`` reads the files the reference reads;
+``ThermalCase.from_flow`` builds the same inputs from a flow result in memory
+(the crop saveAll writes as u_thermal.txt / v_thermal.txt, output.cpp:146-171).
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import os
+from typing import Dict, Optional
+
+import numpy as np
+
+from . import cps
+
+
+@dataclasses.dataclass
+class ThermalCase:
+    gamma: np.ndarray           # (Ny, Nx), 1 = fluid
+    u: np.ndarray               # (Ny, Nx) cell-centred x velocity [m/s]
+    v: np.ndarray               # (Ny, Nx) cell-centred y velocity [m/s]
+    dx: float
+    dy: float
+    q: float = 0.0              # uniform base heat flux [W/m^2] (thermal_params.txt)
+    q0: Optional[np.ndarray] = None  # (Ny, Nx) base heat flux, overrides q
+    nz_solid: int = 2
+    nz_fluid: int = 7
+    H_b: float = 0.0005
+    H_t: float = 0.004
+    k_s: float = 400.0
+    k_f: float = 0.6
+    rho: float = 998.0
+    Cp: float = 4180.0
+    T_inlet: float = 30.0
+    rtol: float = 1e-6
+    maxiter: int = 1000
+    k_interp_mode: int = 1
+    qk: float = 1.0
+
+    def __post_init__(self) -> None:
+        self.gamma = np.ascontiguousarray(self.gamma, dtype=np.float64)
+        self.u = np.ascontiguousarray(self.u, dtype=np.float64)
+        self.v = np.ascontiguousarray(self.v, dtype=np.float64)
+        if self.q0 is not None:
+            self.q0 = np.ascontiguousarray(self.q0, dtype=np.float64)
+        if self.u.shape != self.gamma.shape or self.v.shape != self.gamma.shape:
+            raise ValueError("gamma, u and v must have the same (Ny, Nx) shape")
+
+    @property
+    def Ny(self) -> int:
+        return self.gamma.shape[0]
+
+    @property
+    def Nx(self) -> int:
+        return self.gamma.shape[1]
+
+    @property
+    def Nz(self) -> int:
+        return self.nz_solid + self.nz_fluid
+
+    def heat_flux(self) -> np.ndarray:
+        return self.q0 if self.q0 is not None else np.full(self.gamma.shape, float(self.q))
+
+    @staticmethod
+    def from_export(directory: str, qk: float = 1.0, k_interp_mode: int = 1) -> "ThermalCase":
+        """The inputs the reference's main() reads (thermal_solver.cpp:706-760):
+        thermal_params.txt (M N dx dy qf Ht), geometry_thermal.txt (0 = fluid,
+        1 = solid, inverted here to gamma), u_thermal.txt, v_thermal.txt
+        (missing velocity files leave zero velocity)."""
+        with open(os.path.join(directory, "thermal_params.txt")) as f:
+            tok = f.read().split()
+        _M, _N, dx, dy, qf, Ht = int(tok[0]), int(tok[1]), float(tok[2]), float(tok[3]), float(tok[4]), float(tok[5])
+
+        def read_2d(path):
+            rows = []
+            if not os.path.exists(path):
+                return None
+            with open(path) as f:
+                for line in f:
+                    if not line.strip() or line.startswith("#"):
+                        continue
+                    rows.append([float(x) for x in line.split()])
+            return rows
+
+        geo = read_2d(os.path.join(directory, "geometry_thermal.txt"))
+        if not geo:
+            raise FileNotFoundError("could not load geometry_thermal.txt")
+        Ny, Nx = len(geo), len(geo[0])
+        gamma = np.array([[1.0 - x for x in row[:Nx]] for row in geo])
+        u = np.zeros((Ny, Nx))
+        v = np.zeros((Ny, Nx))
+        uu = read_2d(os.path.join(directory, "u_thermal.txt"))
+        vv = read_2d(os.path.join(directory, "v_thermal.txt"))
+        if uu:
+            for j in range(min(Ny, len(uu))):
+                for i in range(min(Nx, len(uu[j]))):
+                    u[j, i] = uu[j][i]
+                    v[j, i] = vv[j][i]
+        return ThermalCase(gamma=gamma, u=u, v=v, dx=dx, dy=dy, q=qf, H_t=Ht, qk=qk, k_interp_mode=k_interp_mode)
+
+    @staticmethod
+    def from_flow(design, fields: Dict[str, np.ndarray], q: float, N_in_buffer: int = 0, N_out_buffer: int = 0,
+                  **params) -> "ThermalCase":
+        """The thermal inputs of a flow result: the cell-centred velocities
+        of saveAll's thermal crop (output.cpp:87-103, 146-171) and the crop of
+        the design's gamma; H_t = the design's channel height when it has one."""
+        U, V = fields["u"], fields["v"]
+        uC = 0.5 * (U[:-1, :] + U[1:, :])
+        vC = 0.5 * (V[:, :-1] + V[:, 1:])
+        lo, hi = N_in_buffer, design.N - N_out_buffer
+        if "H_t" not in params and design.Ht_channel > 0:
+            params["H_t"] = design.Ht_channel
+        return ThermalCase(gamma=design.gamma[:, lo:hi], u=uC[:, lo:hi], v=vC[:, lo:hi], dx=design.hx, dy=design.hy,
+                           q=q, **params)
+
+
+class ThermalSolver:
+    """One thermal case resident on the GPU (a cps_thermal handle)."""
+
+    def __init__(self, case: ThermalCase, device: int = 0, mg_sweeps: int = 0, mg_omega: float = 0.0,
+                 mg_overcorrect: float = 0.0):
+        self.lib = cps.load_library()
+        self.case = case
+        d = cps.CpsThermalDesc()
+        self.lib.cps_thermal_defaults(ctypes.byref(d))
+        for k in ("nz_solid", "nz_fluid", "dx", "dy", "H_b", "H_t", "k_s", "k_f", "rho", "Cp", "T_inlet", "rtol",
+                  "maxiter", "k_interp_mode", "qk", "q"):
+            setattr(d, k, getattr(case, k))
+        d.Nx, d.Ny, d.device = case.Nx, case.Ny, device
+        d.mg_sweeps, d.mg_omega, d.mg_overcorrect = mg_sweeps, mg_omega, mg_overcorrect
+        d.gamma, d.u, d.v = case.gamma.ctypes.data, case.u.ctypes.data, case.v.ctypes.data
+        d.q0 = case.q0.ctypes.data if case.q0 is not None else None
+        h = cps._P()
+        st = self.lib.cps_thermal_create(ctypes.byref(d), ctypes.byref(h))
+        if st != cps.CPS_OK:
+            raise cps.CpsError(st, self.lib.cps_thermal_last_error(None).decode())
+        self.h = h
+
+    def _check(self, st: int) -> None:
+        if st != cps.CPS_OK:
+            raise cps.CpsError(st, self.lib.cps_thermal_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.cps_thermal_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def solve(self) -> Dict[str, float]:
+        r = cps.CpsThermalResult()
+        self._check(self.lib.cps_thermal_solve(self.h, ctypes.byref(r)))
+        return {"iterations": r.iterations, "converged": bool(r.converged), "rel_residual": r.rel_residual,
+                "true_rel_residual": r.true_rel_residual}
+
+    def update(self, gamma=None, u=None, v=None, q0=None) -> None:
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (gamma, u, v, q0)]
+        for a in arrs:
+            if a is not None and a.shape != self.case.gamma.shape:
+                raise ValueError("inputs must be (Ny, Nx)")
+        self._check(self.lib.cps_thermal_update(self.h, *[cps._dptr(a) for a in arrs]))
+
+    def temperature(self) -> np.ndarray:
+        c = self.case
+        T = np.zeros((c.Nz, c.Ny, c.Nx))
+        self._check(self.lib.cps_thermal_download(self.h, cps._dptr(T)))
+        return T
+
+    def system(self):
+        """(planes dict W/E/S/N/B/T/diag, b), each (Nz, Ny, Nx)."""
+        c = self.case
+        n = c.Nz * c.Ny * c.Nx
+        planes = np.zeros(7 * n)
+        b = np.zeros(n)
+        self._check(self.lib.cps_thermal_system(self.h, cps._dptr(planes), cps._dptr(b)))
+        names = ("cW", "cE", "cS", "cN", "cB", "cT", "diag")
+        return ({k: planes[p * n:(p + 1) * n].reshape(c.Nz, c.Ny, c.Nx) for p, k in enumerate(names)},
+                b.reshape(c.Nz, c.Ny, c.Nx))
+
+    def timing(self, reset: bool = False):
+        ms, lv = ctypes.c_double(), ctypes.c_int()
+        self._check(self.lib.cps_thermal_timing(self.h, ctypes.byref(ms), ctypes.byref(lv), int(reset)))
+        return ms.value, lv.value
+
+
+def energy_balance(case: ThermalCase, T: np.ndarray) -> Dict[str, float]:
+    """The temperature ranges and energy balance the reference prints after
+    its solve (thermal_solver.cpp:567-619)."""
+    nzs, Nz = case.nz_solid, case.Nz
+    fluid = np.zeros(T.shape, dtype=bool)
+    fluid[nzs:] = case.gamma > 0.01
+    fin = np.ones(T.shape, dtype=bool)
+    fin[:nzs] = False
+    fin &= ~fluid
+    out = {"T_base_min": float(T[:nzs].min()), "T_base_max": float(T[:nzs].max()),
+           "T_fluid_min": float(T[fluid].min()) if fluid.any() else 1e30,
+           "T_fluid_max": float(T[fluid].max()) if fluid.any() else -1e30,
+           "T_fin_min": float(T[fin].min()) if fin.any() else 1e30,
+           "T_fin_max": float(T[fin].max()) if fin.any() else -1e30}
+    Q_in = float(np.sum(case.heat_flux() * case.dx * case.dy))
+    mdot = mdotT = 0.0
+    dz_f = case.H_t / case.nz_fluid
+    for k in range(nzs, Nz):
+        z = (k - nzs + 0.5) * dz_f / case.H_t
+        po = 4.0 * z * (1 - z)
+        uu = case.u[:, -1] * po
+        m = (case.gamma[:, -1] > 0.01) & (uu > 0)
+        mflow = case.rho * uu[m] * (case.dy * dz_f)
+        mdot += float(mflow.sum())
+        mdotT += float((mflow * T[k, m, -1]).sum())
+    T_out = mdotT / mdot if mdot > 0 else case.T_inlet
+    Q_out = mdot * case.Cp * (T_out - case.T_inlet)
+    out.update(Q_in=Q_in, T_out=T_out, Q_out=Q_out, imbalance=100 * (Q_in - Q_out) / (Q_in + 1e-30))
+    return out

@@ -1,0 +1,125 @@
+"""The 3-D conjugate-heat-transfer solve on the GPU (cps_thermal_*) against
+the thermal oracle (oracle/thermal.py; parity unpinned against the reference
+itself, whose solve needs the absent AMGCL): the device-assembled system
+equals the oracle's restatement of the reference's assembly bit for bit, and
+the device solution satisfies the reference's stop rule on that system and
+agrees with its exact (direct) solution."""
+import numpy as np
+import pytest
+
+from coldplate_solver_b200 import cps, geometry
+from coldplate_solver_b200 import thermal as pt
+from oracle import restatement as rs
+from oracle import thermal as th
+
+pytestmark = pytest.mark.gpu
+
+
+def random_case(Nx, Ny, seed, mode=1, qk=3.0, q0=True):
+    rng = np.random.default_rng(seed)
+    gamma = (rng.random((Ny, Nx)) > 0.4).astype(float)
+    gamma[rng.random((Ny, Nx)) > 0.85] = 0.37
+    gamma[:, 0] = 1.0
+    u = np.abs(rng.normal(0.2, 0.15, (Ny, Nx))) * gamma
+    v = rng.normal(0.0, 0.05, (Ny, Nx)) * gamma
+    q = rng.uniform(5e5, 1.5e6, (Ny, Nx)) if q0 else None
+    return pt.ThermalCase(gamma=gamma, u=u, v=v, dx=20e-6, dy=20e-6, q=8e5, q0=q, H_t=4e-4, k_interp_mode=mode,
+                          qk=qk)
+
+
+def oracle_params(c: pt.ThermalCase) -> th.ThermalParams:
+    return th.ThermalParams(Nx=c.Nx, Ny=c.Ny, dx=c.dx, dy=c.dy, nz_solid=c.nz_solid, nz_fluid=c.nz_fluid,
+                            H_b=c.H_b, H_t=c.H_t, k_s=c.k_s, k_f=c.k_f, rho=c.rho, Cp=c.Cp, T_inlet=c.T_inlet,
+                            rtol=c.rtol, maxiter=c.maxiter, k_interp_mode=c.k_interp_mode, qk=c.qk)
+
+
+def flow_case(M=64, N=131, outer=300, q=1e6):
+    d = geometry.channel_network(M=M, N=N, h=20e-6, wmin=4, wmax=8, seed=7)
+    with cps.Solver(d) as s:
+        s.solve(outer, eps=0.0)
+        f = s.download()
+    return pt.ThermalCase.from_flow(d, f, q=q)
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("shape", [(13, 9), (37, 23)])
+def test_device_system_equals_the_oracle_assembly(shape, mode):
+    c = random_case(*shape, seed=shape[0] + mode, mode=mode, q0=mode != 0)
+    with pt.ThermalSolver(c) as s:
+        planes, b = s.system()
+    po, bo = th.assemble(oracle_params(c), c.gamma, c.u, c.v, c.heat_flux())
+    for k in th.PLANES:
+        assert np.array_equal(planes[k], po[k]), k
+    assert np.array_equal(b, bo)
+
+
+@pytest.mark.parametrize("shape", [(13, 9), (37, 23), (64, 40)])
+def test_solution_matches_the_direct_solve(shape):
+    c = random_case(*shape, seed=5)
+    c.rtol = 1e-10
+    c.maxiter = 2000
+    p = oracle_params(c)
+    with pt.ThermalSolver(c) as s:
+        r = s.solve()
+        T = s.temperature()
+    assert r["converged"] and r["true_rel_residual"] <= 1e-9, r
+    Td = th.solve_direct(p, c.gamma, c.u, c.v, c.heat_flux())
+    err = np.linalg.norm(T - Td) / np.linalg.norm(Td - c.T_inlet)
+    assert err <= 1e-5, err
+
+
+def test_flow_driven_case_meets_the_reference_stop_rule():
+    """Velocities from a flow solve of a channel network: the default stop rule
+    (relative residual 1e-6 from T = T_inlet), checked on the oracle's
+    system, in a modest number of preconditioned iterations; two solves agree
+    bit for bit; the energy balance equals the oracle's statement of it."""
+    c = flow_case()
+    p = oracle_params(c)
+    with pt.ThermalSolver(c) as s:
+        r = s.solve()
+        T = s.temperature()
+        r2 = s.solve()
+        T2 = s.temperature()
+        ms, levels = s.timing()
+    assert r["converged"] and r["iterations"] < 300, r
+    assert np.array_equal(T, T2) and r == r2
+    planes, b = th.assemble(p, c.gamma, c.u, c.v, c.heat_flux())
+    assert th.relative_residual(p, planes, b, T) <= 1.0001e-6
+    Td = th.solve_direct(p, c.gamma, c.u, c.v, c.heat_flux())
+    assert np.linalg.norm(T - Td) / np.linalg.norm(Td - c.T_inlet) <= 1e-3
+    e_dev = pt.energy_balance(c, T)
+    e_ora = th.energy_balance(p, c.gamma, c.u, c.heat_flux(), T)
+    for k in ("T_base_max", "T_fluid_max", "T_fin_max", "Q_in", "Q_out", "T_out"):
+        assert abs(e_dev[k] - e_ora[k]) <= 1e-9 * max(1.0, abs(e_ora[k])), k
+    assert levels == 9 and ms > 0
+
+
+def test_update_equals_a_fresh_solver():
+    a = random_case(37, 23, seed=1)
+    b = random_case(37, 23, seed=2)
+    with pt.ThermalSolver(a) as s:
+        s.solve()
+        s.update(gamma=b.gamma, u=b.u, v=b.v, q0=b.q0)
+        s.solve()
+        T1 = s.temperature()
+        pl1, b1 = s.system()
+    with pt.ThermalSolver(b) as s:
+        s.solve()
+        T2 = s.temperature()
+        pl2, b2 = s.system()
+    assert np.array_equal(T1, T2) and np.array_equal(b1, b2)
+
+
+def test_arguments_are_validated():
+    import ctypes
+    lib = cps.load_library()
+    d = cps.CpsThermalDesc()
+    lib.cps_thermal_defaults(ctypes.byref(d))
+    h = cps._P()
+    assert lib.cps_thermal_create(ctypes.byref(d), ctypes.byref(h)) == cps.CPS_ERR_ARG  # Nx = 0
+    d.Nx, d.Ny, d.dx, d.dy = 4, 4, 1e-5, 1e-5
+    assert lib.cps_thermal_create(ctypes.byref(d), ctypes.byref(h)) == cps.CPS_ERR_ARG  # no inputs
+    g = np.ones((4, 4))
+    d.gamma = d.u = d.v = g.ctypes.data
+    d.k_interp_mode = 3
+    assert lib.cps_thermal_create(ctypes.byref(d), ctypes.byref(h)) == cps.CPS_ERR_ARG
