@@ -385,12 +385,147 @@ def run_b200(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# thermal workload: the 3-D conjugate-heat-transfer solve downstream of the flow
+# ---------------------------------------------------------------------------
+THERMAL_METRIC = "converged thermal solves/s (relative residual 1e-6)"
+
+
+def thermal_bytes_per_iteration(n_levels_cells) -> float:
+    """Minimal single-pass FP64 streams of one BiCGStab iteration of the
+    thermal solve: two V-cycles (per level and cell, 2 + 2 damped-Jacobi
+    sweeps, restriction and prolongation: 44 elements), the two matrix-vector
+    products with their dots (10 elements each), s (3), the T/r update (8)
+    and p (4) on the finest level."""
+    n0 = n_levels_cells[0]
+    return 8.0 * (2 * 44 * sum(n_levels_cells[:-1]) + (10 + 3 + 10 + 8 + 4) * n0)
+
+
+def thermal_case(nx: int = 1000, setup_outer: int = 3000):
+    """The thermal inputs of the nx x nx/2 density-field design: the flow
+    after ``setup_outer`` outer iterations (untimed set-up), uniform base flux
+    1e6 W/m^2, reference Params otherwise (H_t = the design's channel height)."""
+    from coldplate_solver_b200 import cps, geometry as g, thermal as pt
+    d = g.density_field(Nx=nx)
+    with cps.Solver(d) as s:
+        s.solve(setup_outer, eps=0.0)
+        f = s.download()
+    c = pt.ThermalCase.from_flow(d, f, q=1e6)
+    cfg = {"workload": f"thermal_density_{c.Nx}x{c.Ny}x{c.Nz}", "grid": f"{c.Nx}x{c.Ny}x{c.Nz}", "dx_um": 10,
+           "flow": f"density_field_{d.N}x{d.M} after {setup_outer} outer iterations", "q_w_m2": 1e6,
+           "rtol": c.rtol, "k_interp": "RAMP qk=1"}
+    return c, cfg
+
+
+def run_thermal(args) -> None:
+    rank, local, world = dist_init(args.gpus)
+    import torch
+
+    from coldplate_solver_b200 import thermal as pt
+    device = local
+    torch.cuda.set_device(device)
+    case, cfg = thermal_case(args.thermal_nx)
+    ts = pt.ThermalSolver(case, device=device)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+    for _ in range(args.warmup):
+        r = ts.solve()
+    iters_per_solve = r["iterations"]
+    levels_cells = []
+    nx, ny = case.Nx, case.Ny
+    while True:
+        levels_cells.append(nx * ny * case.Nz)
+        if nx == 1 and ny == 1:
+            break
+        nx, ny = (nx + 1) // 2, (ny + 1) // 2
+    barrier(world)
+    torch.cuda.synchronize(device)
+    ts.timing(reset=True)
+    step_ms, iters = [], []
+    with ClockSampler(device) as clocks:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize(device)
+            before, _ = ts.timing()
+            r = ts.solve()
+            after, _ = ts.timing()
+            step_ms.append(after - before)
+            iters.append(r["iterations"])
+    torch.cuda.synchronize(device)
+    barrier(world)
+    kernel_ms, n_levels = ts.timing(reset=True)
+    total_s = max_over_ranks(sum(step_ms) / 1e3, world, local)
+    value = world * args.steps / total_s
+    alg_bytes = sum(iters) * thermal_bytes_per_iteration(levels_cells)
+    # end to end through the C ABI: host inputs in, host temperature out
+    pin = {k: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+           for k, a in (("gamma", case.gamma), ("u", case.u), ("v", case.v), ("q0", case.heat_flux()))}
+    T_host = torch.zeros(case.Nz * case.Ny * case.Nx, dtype=torch.float64).pin_memory().numpy()
+    h2d = sum(a.nbytes for a in pin.values())
+    d2h = T_host.nbytes + 8 * 4
+    e2e_steps = max(1, min(args.steps, 5))
+    barrier(world)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ts.update(pin["gamma"], pin["u"], pin["v"], pin["q0"])
+        ts.solve()
+        T_host[:] = ts.temperature().ravel()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, local)
+    barrier(world)
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        from oracle import thermal as th
+        p = th.ThermalParams(Nx=case.Nx, Ny=case.Ny, dx=case.dx, dy=case.dy, H_t=case.H_t, rtol=case.rtol)
+        _, it_cpu, sec, done = th.mg_bicgstab_cpu(p, case.gamma, case.u, case.v, case.heat_flux(),
+                                                   time_cap=args.cpu_time_cap)
+        per_solve = sec if done else sec * max(1, iters_per_solve) / max(1, it_cpu)
+        cpu = {"value": 1.0 / per_solve, "unit": "solves/s", "cores": 1, "kind": "port",
+               "sample": (f"scipy port of this solve's algorithm (assembly, aggregation multigrid, BiCGStab), "
+                          f"{it_cpu} iterations in {sec:.1f} s" + ("" if done else
+                          f", extrapolated to the GPU's {iters_per_solve} iterations")),
+               "note": "the reference's own thermal solve needs AMGCL, absent from the reference tree"}
+    ts.close()
+    if rank != 0:
+        return
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = alg_bytes / (kernel_ms / 1e3) / 1e9 if kernel_ms > 0 else None
+    line = {
+        "metric": THERMAL_METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+        "impl": "b200",
+        "config": dict(cfg, l2="flushed between steps (512 MiB write)", iterations_per_solve=iters_per_solve,
+                       multigrid_levels=n_levels, parallelism=f"replicas x{world}"),
+        "e2e": {"value": world * e2e_steps / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s",
+                     "kernel": "cpt::solve_kernel", "kernel_ms_per_launch": kernel_ms / args.steps,
+                     "algorithmic_bytes_per_launch": alg_bytes / args.steps},
+        "gpu_launches": args.steps,
+        "clocks": clocks.summary(),
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args) -> None:
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from oracle import reference
+    if args.workload == "thermal":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's thermal solve includes AMGCL, whose "
+                          "headers are absent from the reference tree (ThermalSolver/amgcl is empty)"}), flush=True)
+        return
     if args.workload == "served":
         print(json.dumps({"impl": "reference", "unavailable": "a served stream is a GPU serving loop; the "
                           "reference's CPU rate on the same designs is the mix arm's (--workload mix)"}))
@@ -604,7 +739,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="network", choices=["straight", "network", "density", "mix", "served"])
+    ap.add_argument("--workload", default="network", choices=["straight", "network", "density", "mix", "served", "thermal"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--cpu-sample-iters", type=int, default=200,
                     help="CPU baseline without the reference binary: oracle-port iterations per sampled state")
@@ -620,6 +755,8 @@ def main() -> None:
     ap.add_argument("--visit", type=int, default=4096, help="mix/served: outer iterations per design per launch")
     ap.add_argument("--placement", default="default",
                     help='mix/served: JSON placement, e.g. \'{"group_ctas": 148}\' or \'{"tiles_per_cta": 8}\'')
+    ap.add_argument("--thermal-nx", type=int, default=1000,
+                    help="thermal: cells in x of the density-field design (y = x/2); 500 for small profiling captures")
     ap.add_argument("--max-outer", type=int, default=MAX_OUTER,
                     help="cap on outer iterations per solve (small profiling captures; the line then says converged=false)")
     args = ap.parse_args()
@@ -629,6 +766,8 @@ def main() -> None:
         run_reference(args)
     elif args.workload in ("mix", "served"):
         run_many(args)
+    elif args.workload == "thermal":
+        run_thermal(args)
     else:
         run_b200(args)
 

@@ -1,6 +1,7 @@
 """CPU restatement of the reference's 3-D conjugate-heat-transfer solve
 (ThermalSolver/thermal_solver.cpp) — TEST INFRASTRUCTURE ONLY: the oracle the
-CUDA thermal path is checked against; no product code calls it.
+CUDA thermal path is checked against; no product code calls it (tests use
+it, and bench.py's CPU-baseline leg times mg_bicgstab_cpu).
 
 Parity unpinned: the reference's thermal solver cannot be built here (it
 includes AMGCL, whose headers are absent from the reference tree:
@@ -396,3 +397,81 @@ def energy_balance(p: ThermalParams, gamma, u, q0, T) -> Dict[str, float]:
     Q_out = s["mdot"] * p.Cp * (s["T_out"] - p.T_inlet)
     s.update(Q_in=Q_in, Q_out=Q_out, imbalance=100 * (Q_in - Q_out) / (Q_in + 1e-30))
     return s
+
+
+def mg_bicgstab_cpu(p: ThermalParams, gamma, u, v, q0, sweeps: int = 2, omega: float = 0.8, alpha: float = 1.7,
+                    time_cap: float = 1e30):
+    """CPU port (scipy, single process) of the GPU solve's algorithm: the
+    assembly above, the 2 x 2 aggregation hierarchy with exact Galerkin
+    coarse operators, BiCGStab right-preconditioned by the same V-cycle, from
+    T = T_inlet to ||b - A T|| <= rtol ||b||.  Used only as the CPU baseline of
+    the thermal benchmark (the reference's own solve needs the absent AMGCL).
+    Returns (T, iterations, seconds, finished)."""
+    import time
+
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+    t0 = time.perf_counter()
+    planes, b3 = assemble(p, gamma, u, v, q0)
+    A = to_csr(p, planes)
+    b = b3.ravel()
+    levels = []
+    nx, ny, Nz = p.Nx, p.Ny, p.Nz
+    Al = A
+    while True:
+        levels.append({"A": Al, "dinv": 1.0 / Al.diagonal()})
+        if nx == 1 and ny == 1:
+            break
+        cx, cy = (nx + 1) // 2, (ny + 1) // 2
+        k, j, i = np.meshgrid(np.arange(Nz), np.arange(ny), np.arange(nx), indexing="ij")
+        P = sp.csr_matrix((np.ones(k.size), ((k * ny * nx + j * nx + i).ravel(), (k * cy * cx + (j // 2) * cx + i // 2).ravel())),
+                          shape=(nx * ny * Nz, cx * cy * Nz))
+        levels[-1]["P"] = P
+        Al = (P.T @ Al @ P).tocsr()
+        nx, ny = cx, cy
+    levels[-1]["lu"] = spl.splu(levels[-1]["A"].tocsc())
+
+    def vcycle(l, rhs):
+        L = levels[l]
+        if "lu" in L:
+            return L["lu"].solve(rhs)
+        A_, dinv = L["A"], L["dinv"]
+        x = omega * dinv * rhs
+        for _ in range(sweeps - 1):
+            x = x + omega * dinv * (rhs - A_ @ x)
+        e = vcycle(l + 1, L["P"].T @ (rhs - A_ @ x))
+        x = x + alpha * (L["P"] @ e)
+        for _ in range(sweeps):
+            x = x + omega * dinv * (rhs - A_ @ x)
+        return x
+
+    T = np.full(p.n, p.T_inlet)
+    r = b - A @ T
+    rhat = r.copy()
+    pv = np.zeros_like(r)
+    vv = np.zeros_like(r)
+    bnorm = np.linalg.norm(b) or 1.0
+    rho = al = om = 1.0
+    rho_new = float(r @ r)
+    it = 0
+    while np.linalg.norm(r) > p.rtol * bnorm and it < p.maxiter:
+        if time.perf_counter() - t0 > time_cap:
+            return T.reshape(Nz, p.Ny, p.Nx), it, time.perf_counter() - t0, False
+        beta = (rho_new / rho) * (al / om)
+        pv = r + beta * (pv - om * vv)
+        ph = vcycle(0, pv)
+        vv = A @ ph
+        al = rho_new / float(rhat @ vv)
+        s = r - al * vv
+        if np.linalg.norm(s) <= p.rtol * bnorm:
+            T = T + al * ph
+            it += 1
+            break
+        sh = vcycle(0, s)
+        t = A @ sh
+        om = float(t @ s) / float(t @ t)
+        T = T + al * ph + om * sh
+        r = s - om * t
+        rho, rho_new = rho_new, float(rhat @ r)
+        it += 1
+    return T.reshape(Nz, p.Ny, p.Nx), it, time.perf_counter() - t0, True

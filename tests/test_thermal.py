@@ -48,3 +48,16 @@ def test_direct_solution_satisfies_the_system_and_balances_energy():
     e = th.energy_balance(p, gamma, u, q0, T)
     assert abs(e["imbalance"]) < 1.0, e
     assert e["T_base_max"] > e["T_out"] > p.T_inlet
+
+
+def test_cpu_port_reaches_the_stop_rule():
+    """The CPU port timed as the thermal benchmark's CPU baseline solves the
+    same system to the same stop rule."""
+    p, gamma, u, v, q0 = case(Nx=40, Ny=24, seed=3)
+    u = np.abs(u)
+    T, it, sec, done = th.mg_bicgstab_cpu(p, gamma, u, v, q0)
+    planes, b = th.assemble(p, gamma, u, v, q0)
+    assert done and it < 200
+    assert th.relative_residual(p, planes, b, T) <= p.rtol * 1.0001
+    Td = th.solve_direct(p, gamma, u, v, q0)
+    assert np.linalg.norm(T - Td) / np.linalg.norm(Td - p.T_inlet) < 1e-3
