@@ -232,28 +232,66 @@ struct Loop {
   __device__ Loop() : start(blockIdx.x * blockDim.x + threadIdx.x), stride(gridDim.x * blockDim.x) {}
 };
 
-// One V-cycle on rhs0 (level 0) into a0/a1; returns the buffer holding M^-1 rhs0.
-__device__ double* vcycle(const View& tv, cps::GridGroup& g, const double* rhs0, double* a0, double* a1, bool& ok) {
-  const Loop lp;
+// Levels with at most this many cells run inside CTA 0 alone (block-stride
+// loops, CTA barriers): below it a grid barrier costs more than the work.
+constexpr int kLocalCells = 2048;
+
+// Where a phase runs: the whole grid (grid-stride loops, grid barrier) or,
+// with Local, CTA 0 alone (block-stride loops, __syncthreads).
+template <bool Local>
+struct Exec {
+  int start, stride;
+  cps::GridGroup* g;
+  __device__ explicit Exec(cps::GridGroup* gg) : g(gg) {
+    start = Local ? (int)threadIdx.x : (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    stride = Local ? (int)blockDim.x : (int)(gridDim.x * blockDim.x);
+  }
+  __device__ bool sync() {
+    if (Local) {
+      __syncthreads();
+      return true;
+    }
+    return g->sync();
+  }
+};
+
+// The first level at or below which every level is small enough for CTA 0.
+__device__ __forceinline__ int local_from(const View& tv) {
+  int l = tv.nlev - 1;
+  while (l > 0 && tv.lv[l - 1].n <= kLocalCells) --l;
+  return l;
+}
+
+// One V-cycle over levels [l0, nlev) on rhs0 (level l0), iterate buffers
+// a0/a1 of level l0.  Every non-coarsest level's result ends in its second
+// buffer (2 sweeps - 1 swaps in all), the coarsest's in its first; so the
+// caller knows where the result is without being told.  The grid instance
+// hands the small levels to CTA 0 and waits at one grid barrier.
+template <bool Local>
+__device__ double* vcycle_from(const View& tv, cps::GridGroup& g, int l0, const double* rhs0, double* a0, double* a1,
+                               bool& ok) {
+  Exec<Local> ex(&g);
   double* cur[kMaxLevels];
   double* oth[kMaxLevels];
   const double w = tv.omega;
   const double* rhs = rhs0;
   const int last = tv.nlev - 1;
-  for (int l = 0; l < last; ++l) {
+  const int split = Local ? last + 1 : local_from(tv);  // grid instance: levels >= split go to CTA 0
+  int l = l0;
+  for (; l < last && (Local || l < split); ++l) {
     const Level& L = tv.lv[l];
-    double* xa = l == 0 ? a0 : L.x0;
-    double* xb = l == 0 ? a1 : L.x1;
-    for (int P = lp.start; P < L.n; P += lp.stride) xa[P] = w * rhs[P] / L.c[kD][P];
-    if (!g.sync()) { ok = false; return a0; }
+    double* xa = l == l0 ? a0 : L.x0;
+    double* xb = l == l0 ? a1 : L.x1;
+    for (int P = ex.start; P < L.n; P += ex.stride) xa[P] = w * rhs[P] / L.c[kD][P];
+    if (!ex.sync()) { ok = false; return a0; }
     for (int sw = 1; sw < tv.sweeps; ++sw) {
-      for (int P = lp.start; P < L.n; P += lp.stride) xb[P] = xa[P] + w * (rhs[P] - apply(L, xa, P)) / L.c[kD][P];
+      for (int P = ex.start; P < L.n; P += ex.stride) xb[P] = xa[P] + w * (rhs[P] - apply(L, xa, P)) / L.c[kD][P];
       double* tmp = xa; xa = xb; xb = tmp;
-      if (!g.sync()) { ok = false; return a0; }
+      if (!ex.sync()) { ok = false; return a0; }
     }
     const Level& C = tv.lv[l + 1];
     const int fplane = L.nx * L.ny, cplane = C.nx * C.ny;
-    for (int Q = lp.start; Q < C.n; Q += lp.stride) {
+    for (int Q = ex.start; Q < C.n; Q += ex.stride) {
       const int I = Q % C.nx, J = (Q / C.nx) % C.ny, k = Q / cplane;
       double acc = 0.0;
       for (int bb = 0; bb < 2; ++bb)
@@ -265,16 +303,24 @@ __device__ double* vcycle(const View& tv, cps::GridGroup& g, const double* rhs0,
         }
       C.b[Q] = acc;
     }
-    if (!g.sync()) { ok = false; return a0; }
+    if (!ex.sync()) { ok = false; return a0; }
     cur[l] = xa;
     oth[l] = xb;
     rhs = C.b;
   }
-  {
+  // l is now the first level this instance does not descend from
+  if (!Local && l < last) {
+    // levels [l, last] inside CTA 0; the rest of the grid waits at the barrier
+    double* x0 = l == l0 ? a0 : tv.lv[l].x0;
+    double* x1 = l == l0 ? a1 : tv.lv[l].x1;
+    if (g.rank == 0) vcycle_from<true>(tv, g, l, rhs, x0, x1, ok);
+    if (!g.sync()) { ok = false; return a0; }
+    cur[l] = x1;
+  } else {
     // coarsest: one column of nz cells, tridiagonal in z (Thomas algorithm)
     const Level& Z = tv.lv[last];
-    double* xz = last == 0 ? a0 : Z.x0;
-    if (g.rank == 0 && threadIdx.x == 0) {
+    double* xz = last == l0 ? a0 : Z.x0;
+    if ((Local || g.rank == 0) && threadIdx.x == 0) {
       double cp[kMaxNz], dp[kMaxNz];
       const int nz = Z.nz;
       for (int k = 0; k < nz; ++k) {
@@ -286,30 +332,35 @@ __device__ double* vcycle(const View& tv, cps::GridGroup& g, const double* rhs0,
       xz[nz - 1] = dp[nz - 1];
       for (int k = nz - 2; k >= 0; --k) xz[k] = dp[k] - cp[k] * xz[k + 1];
     }
-    if (!g.sync()) { ok = false; return a0; }
+    if (!ex.sync()) { ok = false; return a0; }
     cur[last] = xz;
+    l = last;
   }
-  for (int l = last - 1; l >= 0; --l) {
-    const Level& L = tv.lv[l];
-    const Level& C = tv.lv[l + 1];
-    const double* rhsl = l == 0 ? rhs0 : L.b;
-    double* xa = cur[l];
-    double* xb = oth[l];
-    const double* e = cur[l + 1];
+  for (int m = l - 1; m >= l0; --m) {
+    const Level& L = tv.lv[m];
+    const Level& C = tv.lv[m + 1];
+    const double* rhsl = m == l0 ? rhs0 : L.b;
+    double* xa = cur[m];
+    double* xb = oth[m];
+    const double* e = cur[m + 1];
     const int fplane = L.nx * L.ny, cplane = C.nx * C.ny;
-    for (int P = lp.start; P < L.n; P += lp.stride) {
+    for (int P = ex.start; P < L.n; P += ex.stride) {
       const int i = P % L.nx, j = (P / L.nx) % L.ny, k = P / fplane;
       xa[P] += tv.alpha * e[k * cplane + (j >> 1) * C.nx + (i >> 1)];
     }
-    if (!g.sync()) { ok = false; return a0; }
+    if (!ex.sync()) { ok = false; return a0; }
     for (int sw = 0; sw < tv.sweeps; ++sw) {
-      for (int P = lp.start; P < L.n; P += lp.stride) xb[P] = xa[P] + w * (rhsl[P] - apply(L, xa, P)) / L.c[kD][P];
+      for (int P = ex.start; P < L.n; P += ex.stride) xb[P] = xa[P] + w * (rhsl[P] - apply(L, xa, P)) / L.c[kD][P];
       double* tmp = xa; xa = xb; xb = tmp;
-      if (!g.sync()) { ok = false; return a0; }
+      if (!ex.sync()) { ok = false; return a0; }
     }
-    cur[l] = xa;
+    cur[m] = xa;
   }
-  return cur[0];
+  return cur[l0];
+}
+
+__device__ double* vcycle(const View& tv, cps::GridGroup& g, const double* rhs0, double* a0, double* a1, bool& ok) {
+  return vcycle_from<false>(tv, g, 0, rhs0, a0, a1, ok);
 }
 
 // BiCGStab, right-preconditioned by the V-cycle, from T = T_inlet.
