@@ -364,7 +364,14 @@ __device__ double* vcycle(const View& tv, cps::GridGroup& g, const double* rhs0,
 }
 
 // BiCGStab, right-preconditioned by the V-cycle, from T = T_inlet.
-__global__ void __launch_bounds__(cps::kThreads, 2) solve_kernel(View tv, double T_in, cps::GridBarrier* bar,
+// Three CTAs per SM (80 registers, no spills): the fine-level phases are
+// bound by memory latency, and 24 warps per SM keep more loads in flight than
+// 16 (B200, 1000 x 500 x 9 cells: 98 -> 84 ms per solve; four per SM spill
+// and gain nothing more).
+#ifndef CPT_MIN_BLOCKS
+#define CPT_MIN_BLOCKS 3
+#endif
+__global__ void __launch_bounds__(cps::kThreads, CPT_MIN_BLOCKS) solve_kernel(View tv, double T_in, cps::GridBarrier* bar,
                                                                  double* red, int* status) {
   __shared__ double smem[cps::kRedWidth * 8];
   cps::GridGroup g{bar, red, status, blockIdx.x, gridDim.x, 0u, 0ull};
