@@ -389,6 +389,10 @@ def run_b200(args) -> None:
 # thermal workload: the 3-D conjugate-heat-transfer solve downstream of the flow
 # ---------------------------------------------------------------------------
 THERMAL_METRIC = "converged thermal solves/s (relative residual 1e-6)"
+# DRAM bytes (read + write) per launch of the thermal solve on the full
+# 1000 x 500 x 9 workload (63 BiCGStab iterations), from a one-pass ncu launch
+# list; profiles/cpt_solve_kernel_thermal_density_fp64.txt has the command.
+THERMAL_TRAFFIC = 3.058e11
 
 
 def thermal_bytes_per_iteration(n_levels_cells) -> float:
@@ -504,7 +508,10 @@ def run_thermal(args) -> None:
         "e2e": {"value": world * e2e_steps / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "frac": (achieved / peak) if achieved else None,
+                     "traffic": THERMAL_TRAFFIC if args.thermal_nx == 1000 else None,
+                     "traffic_source": "ncu launch list of the full workload (dram bytes per launch, 63 iterations)"
+                     if args.thermal_nx == 1000 else None,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s",
                      "kernel": "cpt::solve_kernel", "kernel_ms_per_launch": kernel_ms / args.steps,
                      "algorithmic_bytes_per_launch": alg_bytes / args.steps},
