@@ -15,7 +15,8 @@ import sys
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 REPO_DIR = os.path.dirname(PKG_DIR)
 LIB_PATH = os.path.join(PKG_DIR, "libcps.so")
-SOURCES = [os.path.join(PKG_DIR, "csrc", f) for f in ("cps_api.cu", "cps_noalloc.cu", "cps_thermal.cu", "cps_io.cpp")]
+SOURCES = [os.path.join(PKG_DIR, "csrc", f) for f in ("cps_api.cu", "cps_noalloc.cu", "cps_thermal.cu", "cps_io.cpp",
+                                                              "cps_thermal_io.cpp")]
 HEADERS = [os.path.join(PKG_DIR, "csrc", f) for f in os.listdir(os.path.join(PKG_DIR, "csrc")) if f.endswith(".cuh")]
 HEADERS.append(os.path.join(REPO_DIR, "include", "cps.h"))
 HEADERS.append(os.path.join(REPO_DIR, "include", "cps_thermal.h"))

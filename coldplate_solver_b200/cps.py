@@ -134,6 +134,14 @@ class CpsThermalResult(ctypes.Structure):
                 ("true_rel_residual", ctypes.c_double)]
 
 
+class CpsThermalMetrics(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in (
+        "T_avg_base", "T_avg_fluid", "T_avg_solid", "T_avg_global", "T_std_base", "T_std_fluid", "T_std_global",
+        "T_range_base", "T_range_fluid", "T_range_global", "T_uniformity_base", "T_uniformity_global",
+        "grad_max", "grad_avg", "grad_max_base", "grad_avg_base")] + \
+        [(k, ctypes.c_int) for k in ("grad_max_i", "grad_max_j", "grad_max_k", "pad")]
+
+
 class CpsBatchResult(ctypes.Structure):
     _fields_ = [("n_done", ctypes.c_int), ("converged", ctypes.c_int), ("status", ctypes.c_int),
                 ("last", CpsStepOut)]
@@ -188,6 +196,9 @@ SIGNATURES = {
     "cps_thermal_system": (ctypes.c_int, [_P, _D, _D]),
     "cps_thermal_timing": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int),
                                           ctypes.c_int]),
+    "cps_thermal_compute_metrics": (ctypes.c_int, [ctypes.POINTER(CpsThermalDesc), _D, _D,
+                                                   ctypes.POINTER(CpsThermalMetrics)]),
+    "cps_thermal_save": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(CpsThermalDesc), _D, _D, _D, _D]),
     "cps_thermal_destroy": (None, [_P]),
     "cps_thermal_last_error": (ctypes.c_char_p, [_P]),
     "cps_last_error": (ctypes.c_char_p, [_P]),

@@ -104,7 +104,9 @@ class ThermalCase:
                 for i in range(min(Nx, len(uu[j]))):
                     u[j, i] = uu[j][i]
                     v[j, i] = vv[j][i]
-        return ThermalCase(gamma=gamma, u=u, v=v, dx=dx, dy=dy, q=qf, H_t=Ht, qk=qk, k_interp_mode=k_interp_mode)
+        # Params::dx() = Lx / Nx with Lx = cols * dx (thermal_solver.cpp:188, 723)
+        return ThermalCase(gamma=gamma, u=u, v=v, dx=(Nx * dx) / Nx, dy=(Ny * dy) / Ny, q=qf, H_t=Ht, qk=qk,
+                           k_interp_mode=k_interp_mode)
 
     @staticmethod
     def from_flow(design, fields: Dict[str, np.ndarray], q: float, N_in_buffer: int = 0, N_out_buffer: int = 0,
@@ -120,6 +122,44 @@ class ThermalCase:
             params["H_t"] = design.Ht_channel
         return ThermalCase(gamma=design.gamma[:, lo:hi], u=uC[:, lo:hi], v=vC[:, lo:hi], dx=design.hx, dy=design.hy,
                            q=q, **params)
+
+
+def _desc(case: ThermalCase) -> "cps.CpsThermalDesc":
+    lib = cps.load_library()
+    d = cps.CpsThermalDesc()
+    lib.cps_thermal_defaults(ctypes.byref(d))
+    for k in ("nz_solid", "nz_fluid", "dx", "dy", "H_b", "H_t", "k_s", "k_f", "rho", "Cp", "T_inlet", "rtol",
+              "maxiter", "k_interp_mode", "qk", "q"):
+        setattr(d, k, getattr(case, k))
+    d.Nx, d.Ny = case.Nx, case.Ny
+    return d
+
+
+def metrics(case: ThermalCase, T: np.ndarray) -> Dict[str, float]:
+    """compute_thermal_metrics (thermal_output.cpp:135-320) of a temperature
+    field (Nz, Ny, Nx): volume-weighted averages, deviations, ranges,
+    uniformity and gradient statistics (cps_thermal_compute_metrics)."""
+    lib = cps.load_library()
+    T = np.ascontiguousarray(T, dtype=np.float64)
+    m = cps.CpsThermalMetrics()
+    d = _desc(case)
+    st = lib.cps_thermal_compute_metrics(ctypes.byref(d), cps._dptr(T), cps._dptr(case.gamma), ctypes.byref(m))
+    if st != cps.CPS_OK:
+        raise cps.CpsError(st, "cps_thermal_compute_metrics: bad arguments")
+    return {k: getattr(m, k) for k, _ in cps.CpsThermalMetrics._fields_ if k != "pad"}
+
+
+def save(directory: str, case: ThermalCase, T: np.ndarray) -> None:
+    """The files the reference's thermal main writes (thermal_results_3d.vtk,
+    thermal_metrics.txt, k_thermal.txt, thermal_gradient_3d.vtk;
+    cps_thermal_save)."""
+    lib = cps.load_library()
+    T = np.ascontiguousarray(T, dtype=np.float64)
+    d = _desc(case)
+    st = lib.cps_thermal_save(directory.encode(), ctypes.byref(d), cps._dptr(T), cps._dptr(case.gamma),
+                              cps._dptr(case.u), cps._dptr(case.v))
+    if st != cps.CPS_OK:
+        raise cps.CpsError(st, f"cps_thermal_save: could not write to {directory}")
 
 
 class ThermalSolver:

@@ -86,6 +86,33 @@ cps_status cps_thermal_system(cps_thermal* t, double* planes, double* b);
  * launching stream; *levels = multigrid levels. */
 cps_status cps_thermal_timing(cps_thermal* t, double* kernel_ms, int* levels, int reset);
 
+/* The statistics ThermalMetrics holds (thermal_output.cpp:14-42, computed as
+ * compute_thermal_metrics does, :135-320: volume-weighted over the base plate
+ * k < nz_solid, the fluid gamma > 0.01 and the solid fins above the base). */
+typedef struct {
+  double T_avg_base, T_avg_fluid, T_avg_solid, T_avg_global;
+  double T_std_base, T_std_fluid, T_std_global;
+  double T_range_base, T_range_fluid, T_range_global;
+  double T_uniformity_base, T_uniformity_global;
+  double grad_max, grad_avg, grad_max_base, grad_avg_base;
+  int grad_max_i, grad_max_j, grad_max_k, pad;
+} cps_thermal_metrics;
+
+/* Host code, no GPU.  d supplies the grid (Nx, Ny, nz_solid, nz_fluid, dx,
+ * dy, H_b, H_t); T is Nz x Ny x Nx, gamma Ny x Nx (1 = fluid). */
+cps_status cps_thermal_compute_metrics(const cps_thermal_desc* d, const double* T, const double* gamma,
+                                       cps_thermal_metrics* out);
+
+/* The files the reference's thermal main writes after its solve
+ * (thermal_solver.cpp:750-763) into directory dir, with the reference's
+ * number formats: thermal_results_3d.vtk (ThermalSolver3D::save_vtk, :622-662;
+ * needs u and v, Ny x Nx, and d's conductivity settings), thermal_metrics.txt
+ * (save_thermal_metrics, thermal_output.cpp:326-371), k_thermal.txt
+ * (save_k_field, :530-568) and thermal_gradient_3d.vtk
+ * (compute_gradient_field + save_gradient_vtk, :411-524). */
+cps_status cps_thermal_save(const char* dir, const cps_thermal_desc* d, const double* T, const double* gamma,
+                            const double* u, const double* v);
+
 void cps_thermal_destroy(cps_thermal* t);
 const char* cps_thermal_last_error(const cps_thermal* t);
 

@@ -183,3 +183,38 @@ def build_alpha(gamma: np.ndarray, kmin: float = 1e-14, q: float = 1.0, precisio
             raise RuntimeError(proc.stderr.decode()[-2000:])
         out = casefile.read_records(opath)
     return out["alpha"].reshape(M, N), out["gamma"].reshape(M, N)
+
+
+def run_thermal_outputs(T: np.ndarray, gamma: np.ndarray, dx: float, dy: float, nz_solid: int = 2,
+                        nz_fluid: int = 7, H_b: float = 0.0005, H_t: float = 0.004, k_s: float = 400.0,
+                        k_f: float = 0.6, qk: float = 1.0, timeout: float = 600) -> Dict[str, object]:
+    """The reference's thermal output module (ThermalSolver/thermal_output.cpp,
+    harness oracle/thermal_out_harness.cpp) on a temperature field T
+    (Nz, Ny, Nx) and gamma (Ny, Nx): returns its metrics (with its
+    Params::dx(), dy()) and the bytes of the files it writes."""
+    path = os.path.join(REF_DIR, "thermal_out")
+    if not os.access(path, os.X_OK):
+        raise FileNotFoundError(f"{path} not built (make -C oracle ref)")
+    Ny, Nx = gamma.shape
+    with tempfile.TemporaryDirectory(prefix="cps_thout_") as tmp:
+        cpath, opath = os.path.join(tmp, "case.bin"), os.path.join(tmp, "out.bin")
+        outdir = os.path.join(tmp, "out")
+        os.mkdir(outdir)
+        casefile.write_records(cpath, {"ints": np.array([Nx, Ny, nz_solid, nz_fluid], dtype=np.int32),
+                                       "reals": [dx, dy, H_b, H_t, k_s, k_f, qk],
+                                       "T": np.ascontiguousarray(T, dtype=np.float64).ravel(),
+                                       "gamma": np.ascontiguousarray(gamma, dtype=np.float64).ravel()})
+        proc = subprocess.run([path, cpath, opath, outdir], cwd=tmp, stdout=subprocess.DEVNULL,
+                              stderr=subprocess.PIPE, timeout=timeout)
+        if proc.returncode != 0:
+            raise RuntimeError(f"thermal_out failed: {proc.stderr.decode()[-2000:]}")
+        vals = casefile.read_records(opath)["metrics"]
+        files = {}
+        for name in os.listdir(outdir):
+            with open(os.path.join(outdir, name), "rb") as f:
+                files[name] = f.read()
+    keys = ("T_avg_base", "T_avg_fluid", "T_avg_solid", "T_avg_global", "T_std_base", "T_std_fluid", "T_std_global",
+            "T_range_base", "T_range_fluid", "T_range_global", "T_uniformity_base", "T_uniformity_global",
+            "grad_max", "grad_avg", "grad_max_base", "grad_avg_base", "grad_max_i", "grad_max_j", "grad_max_k",
+            "dx", "dy")
+    return {"metrics": dict(zip(keys, vals.tolist())), "files": files}

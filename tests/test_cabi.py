@@ -48,8 +48,9 @@ int main(void) {
          sizeof(cps_dp_monitor), offsetof(cps_dp_monitor, ramp_steps), offsetof(cps_dp_monitor, x_core_out));
   printf("%zu %zu %zu\n", sizeof(cps_case_params), offsetof(cps_case_params, N_in_buffer),
          offsetof(cps_case_params, has_Ht));
-  printf("%zu %zu %zu %zu\n", sizeof(cps_thermal_desc), offsetof(cps_thermal_desc, gamma),
-         offsetof(cps_thermal_desc, mg_overcorrect), sizeof(cps_thermal_result));
+  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(cps_thermal_desc), offsetof(cps_thermal_desc, gamma),
+         offsetof(cps_thermal_desc, mg_overcorrect), sizeof(cps_thermal_result), sizeof(cps_thermal_metrics),
+         offsetof(cps_thermal_metrics, grad_max_k));
   printf("%zu %zu %zu %zu %zu\n", sizeof(cps_pseudo), offsetof(cps_pseudo, target_velocity),
          offsetof(cps_pseudo, ls_resid_increase_tol), sizeof(cps_pseudo_state), offsetof(cps_pseudo_state, ls_backtracks));
   return 0;
@@ -65,7 +66,8 @@ int main(void) {
           ctypes.sizeof(cps.CpsDpMonitor), cps.CpsDpMonitor.ramp_steps.offset, cps.CpsDpMonitor.x_core_out.offset,
           ctypes.sizeof(cps.CpsCaseParams), cps.CpsCaseParams.N_in_buffer.offset, cps.CpsCaseParams.has_Ht.offset,
           ctypes.sizeof(cps.CpsThermalDesc), cps.CpsThermalDesc.gamma.offset, cps.CpsThermalDesc.mg_overcorrect.offset,
-          ctypes.sizeof(cps.CpsThermalResult),
+          ctypes.sizeof(cps.CpsThermalResult), ctypes.sizeof(cps.CpsThermalMetrics),
+          cps.CpsThermalMetrics.grad_max_k.offset,
           ctypes.sizeof(cps.CpsPseudo), cps.CpsPseudo.target_velocity.offset,
           cps.CpsPseudo.ls_resid_increase_tol.offset, ctypes.sizeof(cps.CpsPseudoState),
           cps.CpsPseudoState.ls_backtracks.offset]

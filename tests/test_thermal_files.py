@@ -1,0 +1,67 @@
+"""The thermal step's outputs (cps_thermal_compute_metrics, cps_thermal_save;
+host code) against the reference's own thermal output module
+(ThermalSolver/thermal_output.cpp compiled under oracle/thermal_out_harness.cpp):
+the metrics equal bit for bit and thermal_metrics.txt, k_thermal.txt and
+thermal_gradient_3d.vtk are byte-identical.  thermal_results_3d.vtk is
+written by a member of the reference's solver class, which cannot be built
+(it needs AMGCL): its layout is checked here, not its bytes."""
+import os
+
+import numpy as np
+import pytest
+
+from coldplate_solver_b200 import thermal as pt
+from oracle import reference
+
+
+def field(Nx=23, Ny=11, seed=0):
+    rng = np.random.default_rng(seed)
+    gamma = (rng.random((Ny, Nx)) > 0.5).astype(float)
+    gamma[rng.random((Ny, Nx)) > 0.8] = 0.42
+    T = 30.0 + 20.0 * rng.random((9, Ny, Nx))
+    u = rng.normal(0.1, 0.05, (Ny, Nx)) * gamma
+    v = rng.normal(0.0, 0.02, (Ny, Nx)) * gamma
+    return gamma, T, u, v
+
+
+@pytest.mark.skipif(not os.access(os.path.join(reference.REF_DIR, "thermal_out"), os.X_OK),
+                    reason="oracle/_ref/thermal_out not built")
+@pytest.mark.parametrize("seed,qk,dx", [(0, 1.0, 1e-5), (1, 10.0, 2.3e-5)])
+def test_outputs_equal_the_reference_module(tmp_path, seed, qk, dx):
+    gamma, T, u, v = field(seed=seed)
+    ref = reference.run_thermal_outputs(T, gamma, dx, dx, H_t=5e-4, qk=qk)
+    m = ref["metrics"]
+    # the reference's Params::dx() = (Nx dx) / Nx is what the library is given
+    case = pt.ThermalCase(gamma=gamma, u=u, v=v, dx=m["dx"], dy=m["dy"], H_t=5e-4, qk=qk)
+    got = pt.metrics(case, T)
+    for k, val in got.items():
+        assert val == m[k], (k, val, m[k])
+    pt.save(str(tmp_path), case, T)
+    for name in ("thermal_metrics.txt", "k_thermal.txt", "thermal_gradient_3d.vtk"):
+        assert (tmp_path / name).read_bytes() == ref["files"][name], name
+    lines = (tmp_path / "thermal_results_3d.vtk").read_text().splitlines()
+    Ny, Nx = gamma.shape
+    n = 9 * Ny * Nx
+    assert lines[:4] == ["# vtk DataFile Version 3.0", "Thermal3D", "ASCII", "DATASET RECTILINEAR_GRID"]
+    assert lines[4] == f"DIMENSIONS {Nx + 1} {Ny + 1} 10"
+    assert f"CELL_DATA {n}" in lines
+    for tag in ("SCALARS Temperature double 1", "SCALARS Region int 1", "SCALARS Density double 1",
+                "SCALARS ThermalConductivity double 1", "VECTORS Velocity double"):
+        assert tag in lines, tag
+    start = lines.index("SCALARS Temperature double 1") + 2
+    np.testing.assert_allclose([float(x) for x in lines[start:start + n]], T.ravel(), rtol=1e-5)
+
+
+def test_from_export_reads_the_reference_inputs(tmp_path):
+    gamma, T, u, v = field(Nx=7, Ny=5, seed=2)
+    (tmp_path / "thermal_params.txt").write_text("5 7 2.5e-05 2.5e-05 750000 0.0004\n")
+    (tmp_path / "geometry_thermal.txt").write_text(
+        "\n".join(" ".join(repr(float(1.0 - g)) for g in row) for row in gamma) + "\n")
+    (tmp_path / "u_thermal.txt").write_text("\n".join("\t".join(repr(float(x)) for x in row) for row in u) + "\n")
+    (tmp_path / "v_thermal.txt").write_text("\n".join("\t".join(repr(float(x)) for x in row) for row in v) + "\n")
+    c = pt.ThermalCase.from_export(str(tmp_path), qk=3.0)
+    assert (c.Nx, c.Ny) == (7, 5) and c.q == 750000 and c.H_t == 0.0004 and c.qk == 3.0
+    assert c.dx == (7 * 2.5e-05) / 7 and c.dy == (5 * 2.5e-05) / 5
+    np.testing.assert_array_equal(c.gamma, 1.0 - (1.0 - gamma))
+    np.testing.assert_array_equal(c.u, u)
+    np.testing.assert_array_equal(c.v, v)
