@@ -666,8 +666,12 @@ cps_status cps_thermal_create(const cps_thermal_desc* d, cps_thermal** out) {
   in.v = t->dv;
   in.q0 = t->dq;
   if (!d->q0) {
-    std::vector<double> q(n2, d->q);  // main: s.q0.assign(Ny*Nx, qf) (thermal_solver.cpp:760)
-    if (!tcuda(t, cudaMemcpy(t->dq, q.data(), n2 * sizeof(double), cudaMemcpyHostToDevice), "h2d"))
+    // main: s.q0.assign(Ny*Nx, qf) (thermal_solver.cpp:760).  On the handle's
+    // stream, after the slab's memset: that stream does not order against the
+    // legacy default stream.
+    std::vector<double> q(n2, d->q);
+    if (!tcuda(t, cudaMemcpyAsync(t->dq, q.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, t->stream), "h2d") ||
+        !tcuda(t, cudaStreamSynchronize(t->stream), "h2d"))
       return bail(CPS_ERR_CUDA);
   }
   const cps_status st = assemble(t, d->gamma, d->u, d->v, d->q0);
