@@ -344,12 +344,28 @@ __device__ double* vcycle_from(const View& tv, cps::GridGroup& g, int l0, const 
     double* xb = oth[m];
     const double* e = cur[m + 1];
     const int fplane = L.nx * L.ny, cplane = C.nx * C.ny;
+    const double alpha = tv.alpha;
+    // First post-smoothing sweep with the coarse correction folded in: every
+    // value it reads is x + alpha e(parent), computed as the separate
+    // prolongation pass would have stored it (the same operations, so the same
+    // bits), which saves that pass and its barrier.
     for (int P = ex.start; P < L.n; P += ex.stride) {
       const int i = P % L.nx, j = (P / L.nx) % L.ny, k = P / fplane;
-      xa[P] += tv.alpha * e[k * cplane + (j >> 1) * C.nx + (i >> 1)];
+      auto xc = [&](int q, int ii, int jj, int kk) { return xa[q] + alpha * e[kk * cplane + (jj >> 1) * C.nx + (ii >> 1)]; };
+      double s = 0.0;  // A x in apply()'s order
+      if (k > 0) s += L.c[kB][P] * xc(P - fplane, i, j, k - 1);
+      if (j > 0) s += L.c[kS][P] * xc(P - L.nx, i, j - 1, k);
+      if (i > 0) s += L.c[kW][P] * xc(P - 1, i - 1, j, k);
+      const double xP = xc(P, i, j, k);
+      s += L.c[kD][P] * xP;
+      if (i < L.nx - 1) s += L.c[kE][P] * xc(P + 1, i + 1, j, k);
+      if (j < L.ny - 1) s += L.c[kN][P] * xc(P + L.nx, i, j + 1, k);
+      if (k < L.nz - 1) s += L.c[kT][P] * xc(P + fplane, i, j, k + 1);
+      xb[P] = xP + w * (rhsl[P] - s) / L.c[kD][P];
     }
+    { double* tmp = xa; xa = xb; xb = tmp; }
     if (!ex.sync()) { ok = false; return a0; }
-    for (int sw = 0; sw < tv.sweeps; ++sw) {
+    for (int sw = 1; sw < tv.sweeps; ++sw) {
       for (int P = ex.start; P < L.n; P += ex.stride) xb[P] = xa[P] + w * (rhsl[P] - apply(L, xa, P)) / L.c[kD][P];
       double* tmp = xa; xa = xb; xb = tmp;
       if (!ex.sync()) { ok = false; return a0; }
