@@ -123,3 +123,26 @@ def test_arguments_are_validated():
     d.gamma = d.u = d.v = g.ctypes.data
     d.k_interp_mode = 3
     assert lib.cps_thermal_create(ctypes.byref(d), ctypes.byref(h)) == cps.CPS_ERR_ARG
+
+
+@pytest.mark.parametrize("shape,nz", [((1, 7), (2, 7)), ((9, 1), (2, 7)), ((5, 3), (1, 3)), ((2, 2), (3, 1)),
+                                      ((17, 12), (1, 1))])
+def test_edge_grids_match_the_oracle(shape, nz):
+    """Degenerate and small grids (one column, one row, single layers): the
+    hierarchy still ends in one column, the system equals the oracle's and
+    the solution its direct solve."""
+    c = random_case(*shape, seed=11)
+    c.nz_solid, c.nz_fluid = nz
+    c.rtol = 1e-10
+    p = oracle_params(c)
+    with pt.ThermalSolver(c) as s:
+        planes, b = s.system()
+        r = s.solve()
+        T = s.temperature()
+    po, bo = th.assemble(p, c.gamma, c.u, c.v, c.heat_flux())
+    for k in th.PLANES:
+        assert np.array_equal(planes[k], po[k]), k
+    assert np.array_equal(b, bo)
+    Td = th.solve_direct(p, c.gamma, c.u, c.v, c.heat_flux())
+    assert r["converged"], r
+    assert np.linalg.norm(T - Td) / max(np.linalg.norm(Td - c.T_inlet), 1e-300) <= 1e-5
