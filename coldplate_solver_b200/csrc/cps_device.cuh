@@ -453,11 +453,25 @@ struct GridGroup {
 #pragma unroll
       for (int k = 0; k < K; ++k) acc[k] = 0.0;
       if (ok) {
-        for (unsigned b = lane; b < nblk; b += 32) {
+        // CTAs lane, lane + 32, ... in order, their values loaded kBatch at a
+        // time before any is added (one L2 round trip per batch instead of
+        // one per CTA; the order of the additions is unchanged).
+        constexpr int kBatch = K >= 16 ? 1 : 16 / K;
+        for (unsigned b0 = lane; b0 < nblk; b0 += 32u * kBatch) {
+          double x[K][kBatch];
 #pragma unroll
-          for (int k = 0; k < K; ++k) {
-            const double x = __ldcg(slot + (size_t)k * nblk + b);
-            acc[k] = ((MaxMask >> k) & 1u) ? maxd(acc[k], x) : acc[k] + x;
+          for (int k = 0; k < K; ++k)
+#pragma unroll
+            for (int j = 0; j < kBatch; ++j) {
+              const unsigned b = b0 + 32u * j;
+              x[k][j] = b < nblk ? __ldcg(slot + (size_t)k * nblk + b) : 0.0;
+            }
+#pragma unroll
+          for (int j = 0; j < kBatch; ++j) {
+            if (b0 + 32u * j >= nblk) break;
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+              acc[k] = ((MaxMask >> k) & 1u) ? maxd(acc[k], x[k][j]) : acc[k] + x[k][j];
           }
         }
 #pragma unroll
