@@ -169,12 +169,8 @@ class ThermalSolver:
                  mg_overcorrect: float = 0.0):
         self.lib = cps.load_library()
         self.case = case
-        d = cps.CpsThermalDesc()
-        self.lib.cps_thermal_defaults(ctypes.byref(d))
-        for k in ("nz_solid", "nz_fluid", "dx", "dy", "H_b", "H_t", "k_s", "k_f", "rho", "Cp", "T_inlet", "rtol",
-                  "maxiter", "k_interp_mode", "qk", "q"):
-            setattr(d, k, getattr(case, k))
-        d.Nx, d.Ny, d.device = case.Nx, case.Ny, device
+        d = _desc(case)
+        d.device = device
         d.mg_sweeps, d.mg_omega, d.mg_overcorrect = mg_sweeps, mg_omega, mg_overcorrect
         d.gamma, d.u, d.v = case.gamma.ctypes.data, case.u.ctypes.data, case.v.ctypes.data
         d.q0 = case.q0.ctypes.data if case.q0 is not None else None
