@@ -27,7 +27,7 @@
 //
 // Two arithmetic modes share this code through the storage type T of the
 // inner-solve arrays:
-//   T = double (plain FP64, the drop-in judge).  Every product/sum that feeds
+//   T = double (plain FP64, the path checked against the reference).  Every product/sum that feeds
 //     a stored value is evaluated in the reference's order and the unit is
 //     compiled with --fmad=false, so per-point values equal the FP64
 //     reference's; only the grid-wide sums (Jacobi RMS, PCG dots) are added

@@ -45,7 +45,7 @@ enum { CPS_ROW_MAJOR = 0, CPS_COL_MAJOR = 1 /* Eigen::MatrixX? default */ };
 
 /* Arithmetic of the inner solves. */
 enum {
-  CPS_FP64 = 0,  /* plain FP64, the drop-in judge path */
+  CPS_FP64 = 0,  /* plain FP64, the path checked bit-closely against the reference */
   CPS_MIXED = 1  /* FP32 Jacobi and PCG inside FP64 defect correction */
 };
 

@@ -1,7 +1,7 @@
 """ctypes binding of the oracle's C restatement, oracle/liboracle.so (TEST
 INFRASTRUCTURE ONLY).
 
-``precision="f64"`` is the reference promoted to double (the parity judge),
+``precision="f64"`` is the reference promoted to double (the parity reference),
 ``"f32"`` the reference as shipped.  Fields are row-major numpy arrays in the
 reference's index space: u/uStar/dE (M+1, N), v/vStar/dN (M, N+1), p/pStar
 (M+1, N+1).
