@@ -71,3 +71,28 @@ def test_ramp_restarts_with_reset_fields():
         h2 = s.solve(6, eps=0.0)
         assert s.lib.cps_set_inlet_ramp(s.ctx, -1) == cps.CPS_ERR_ARG
     assert np.array_equal(h1, h2)
+
+
+def test_gate_with_ramp_and_pseudo_transient():
+    """The monitored loop with the inlet ramp and the pseudo-transient term
+    and its controllers all on, against the oracle's loop (which
+    tests/test_inlet_ramp.py pins to the reference's runIterations).  The
+    pseudo-transient iteration amplifies the sum-order differences of every
+    step (measured: at most 1.1e-5 relative in the drops over the ~900
+    iterations to the gate, the first iterations equal to 7 digits), so the
+    drops are compared to 1e-4 and the stop iteration within two."""
+    d = geometry.channel_network(M=24, N=40, h=20e-6, wmin=3, wmax=6, seed=3).replace(
+        enableInletRamp=True, enablePseudoTimeStepping=True, serMinIter=5)
+    xc = (0.25 * d.N * d.hx, 0.75 * d.N * d.hx)
+    W, pct, ramp = 30, 0.2, 15
+    f = rs.new_fields(d)
+    dp_o, conv_o = rs.dp_gate_solve(d, f, 5000, W, pct, ramp, x_core=xc)
+    assert conv_o
+    with cps.Solver(d.replace(rampSteps=ramp)) as s:
+        s.set_dp_monitor(gate=True, window=W, percent=pct, ramp_steps=ramp, x_core_in=xc[0], x_core_out=xc[1])
+        hist, dp_g, conv_g = s.solve_monitored(5000, eps=0.0)
+    assert conv_g
+    assert abs(len(dp_g) - len(dp_o)) <= 2, (len(dp_g), len(dp_o))
+    k = min(len(dp_g), len(dp_o))
+    np.testing.assert_allclose(dp_g[:k], dp_o[:k], rtol=1e-4, atol=1e-9)
+    np.testing.assert_allclose(dp_g[:30], dp_o[:30], rtol=1e-8, atol=1e-9)  # the ramp's iterations
