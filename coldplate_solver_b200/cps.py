@@ -192,6 +192,7 @@ SIGNATURES = {
     "cps_thermal_create": (ctypes.c_int, [ctypes.POINTER(CpsThermalDesc), ctypes.POINTER(_P)]),
     "cps_thermal_update": (ctypes.c_int, [_P, _D, _D, _D, _D]),
     "cps_thermal_solve": (ctypes.c_int, [_P, ctypes.POINTER(CpsThermalResult)]),
+    "cps_thermal_solve_from": (ctypes.c_int, [_P, _D, ctypes.POINTER(CpsThermalResult)]),
     "cps_thermal_download": (ctypes.c_int, [_P, _D]),
     "cps_thermal_system": (ctypes.c_int, [_P, _D, _D]),
     "cps_thermal_timing": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int),

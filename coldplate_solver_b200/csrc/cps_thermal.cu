@@ -387,7 +387,7 @@ __device__ double* vcycle(const View& tv, cps::GridGroup& g, const double* rhs0,
 #ifndef CPT_MIN_BLOCKS
 #define CPT_MIN_BLOCKS 3
 #endif
-__global__ void __launch_bounds__(cps::kThreads, CPT_MIN_BLOCKS) solve_kernel(View tv, double T_in, cps::GridBarrier* bar,
+__global__ void __launch_bounds__(cps::kThreads, CPT_MIN_BLOCKS) solve_kernel(View tv, double T_in, int warm, cps::GridBarrier* bar,
                                                                  double* red, int* status) {
   __shared__ double smem[cps::kRedWidth * 8];
   cps::GridGroup g{bar, red, status, blockIdx.x, gridDim.x, 0u, 0ull};
@@ -396,8 +396,10 @@ __global__ void __launch_bounds__(cps::kThreads, CPT_MIN_BLOCKS) solve_kernel(Vi
   const int n = L.n;
   bool ok = true;
   double q2[2] = {0.0, 0.0};
-  for (int P = lp.start; P < n; P += lp.stride) tv.T[P] = T_in;
-  if (!g.sync()) return;
+  if (!warm) {
+    for (int P = lp.start; P < n; P += lp.stride) tv.T[P] = T_in;
+    if (!g.sync()) return;
+  }
   for (int P = lp.start; P < n; P += lp.stride) {
     const double r = tv.rhs[P] - apply(L, tv.T, P);
     tv.r[P] = r;
@@ -710,13 +712,16 @@ cps_status cps_thermal_update(cps_thermal* t, const double* gamma, const double*
   return assemble(t, gamma, u, v, q0);
 }
 
-cps_status cps_thermal_solve(cps_thermal* t, cps_thermal_result* res) {
-  if (!t) return tfail(nullptr, CPS_ERR_ARG, "handle is NULL");
-  if (!tcuda(t, cudaSetDevice(t->device), "cudaSetDevice")) return CPS_ERR_CUDA;
+}  // extern "C"
+
+namespace {
+
+// One solve launch: from T = T_inlet, or (warm) from the handle's current temperature.
+cps_status solve_launch(cps_thermal* t, int warm, cps_thermal_result* res) {
   cpt::View& tv = t->view;
   if (!tcuda(t, cudaMemsetAsync(tv.out, 0, 32 * sizeof(double), t->stream), "memset")) return CPS_ERR_CUDA;
   double T_in = t->desc.T_inlet;
-  void* args[] = {&tv, &T_in, &t->bar, &t->red, &t->status};
+  void* args[] = {&tv, &T_in, &warm, &t->bar, &t->red, &t->status};
   if (!tcuda(t, cudaEventRecord(t->ev0, t->stream), "event") ||
       !tcuda(t, cudaLaunchCooperativeKernel((const void*)cpt::solve_kernel, dim3(t->grid), dim3(cps::kThreads), args, 0,
                                             t->stream), "cooperative launch") ||
@@ -738,6 +743,27 @@ cps_status cps_thermal_solve(cps_thermal* t, cps_thermal_result* res) {
   if (status == cps::kStatusTimeout) return tfail(t, CPS_ERR_TIMEOUT, "device grid barrier timed out");
   if (status == cps::kStatusDiverged) return tfail(t, CPS_ERR_DIVERGED, "residual is not finite");
   return CPS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+cps_status cps_thermal_solve(cps_thermal* t, cps_thermal_result* res) {
+  if (!t) return tfail(nullptr, CPS_ERR_ARG, "handle is NULL");
+  if (!tcuda(t, cudaSetDevice(t->device), "cudaSetDevice")) return CPS_ERR_CUDA;
+  return solve_launch(t, 0, res);
+}
+
+cps_status cps_thermal_solve_from(cps_thermal* t, const double* T0, cps_thermal_result* res) {
+  if (!t) return tfail(nullptr, CPS_ERR_ARG, "handle is NULL");
+  if (!tcuda(t, cudaSetDevice(t->device), "cudaSetDevice")) return CPS_ERR_CUDA;
+  if (T0) {
+    const size_t n = (size_t)t->view.lv[0].n;
+    if (!tcuda(t, cudaMemcpyAsync(t->view.T, T0, n * sizeof(double), cudaMemcpyHostToDevice, t->stream), "h2d"))
+      return CPS_ERR_CUDA;
+  }
+  return solve_launch(t, 1, res);
 }
 
 cps_status cps_thermal_download(cps_thermal* t, double* T) {

@@ -207,6 +207,17 @@ class ThermalSolver:
         return {"iterations": r.iterations, "converged": bool(r.converged), "rel_residual": r.rel_residual,
                 "true_rel_residual": r.true_rel_residual}
 
+    def solve_from(self, T0: Optional[np.ndarray] = None) -> Dict[str, float]:
+        """The solve from T0 (Nz, Ny, Nx), or from the last result when None
+        (cps_thermal_solve_from: a warm start for design loops)."""
+        r = cps.CpsThermalResult()
+        T = None if T0 is None else np.ascontiguousarray(T0, dtype=np.float64)
+        if T is not None and T.shape != (self.case.Nz, self.case.Ny, self.case.Nx):
+            raise ValueError("T0 must be (Nz, Ny, Nx)")
+        self._check(self.lib.cps_thermal_solve_from(self.h, cps._dptr(T), ctypes.byref(r)))
+        return {"iterations": r.iterations, "converged": bool(r.converged), "rel_residual": r.rel_residual,
+                "true_rel_residual": r.true_rel_residual}
+
     def update(self, gamma=None, u=None, v=None, q0=None) -> None:
         arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (gamma, u, v, q0)]
         for a in arrs:

@@ -73,6 +73,12 @@ cps_status cps_thermal_update(cps_thermal* t, const double* gamma, const double*
 /* Solve from T = T_inlet (thermal_solver.cpp:425); *res may be NULL. */
 cps_status cps_thermal_solve(cps_thermal* t, cps_thermal_result* res);
 
+/* The same solve from a given temperature field (Nz x Ny x Nx; NULL: the
+ * handle's current one, i.e. the last solve's result): a warm start for a
+ * design loop whose successive designs differ little.  No counterpart in the
+ * reference, which starts every solve from T_inlet. */
+cps_status cps_thermal_solve_from(cps_thermal* t, const double* T0, cps_thermal_result* res);
+
 /* Temperature, Nz x Ny x Nx doubles. */
 cps_status cps_thermal_download(cps_thermal* t, double* T);
 

@@ -146,3 +146,24 @@ def test_edge_grids_match_the_oracle(shape, nz):
     Td = th.solve_direct(p, c.gamma, c.u, c.v, c.heat_flux())
     assert r["converged"], r
     assert np.linalg.norm(T - Td) / max(np.linalg.norm(Td - c.T_inlet), 1e-300) <= 1e-5
+
+
+def test_warm_start_from_a_previous_solution():
+    """cps_thermal_solve_from: from the converged field nothing is left to do;
+    after a 5 % change of the heat flux, a start from the previous field
+    needs fewer iterations than the start from T_inlet and reaches the same
+    solution (to the stop rule's accuracy)."""
+    c = flow_case()
+    with pt.ThermalSolver(c) as s:
+        s.solve()
+        T1 = s.temperature()
+        r0 = s.solve_from()
+        assert r0["iterations"] == 0 and r0["converged"] and r0["true_rel_residual"] <= 1e-6
+        s.update(q0=c.heat_flux() * 1.05)
+        cold = s.solve()
+        T_cold = s.temperature()
+        warm = s.solve_from(T1)
+        T_warm = s.temperature()
+    assert cold["converged"] and warm["converged"] and warm["true_rel_residual"] <= 1.0001e-6
+    assert warm["iterations"] < cold["iterations"], (warm, cold)
+    assert np.linalg.norm(T_warm - T_cold) / np.linalg.norm(T_cold - c.T_inlet) <= 1e-3
