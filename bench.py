@@ -2,7 +2,7 @@
 """Benchmark: converged SIMPLE solves per second on one B200 (and N GPUs).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload network|straight|density|mix|served] [--precision fp64|mixed]
+                    [--workload network|straight|density|mix|served|thermal] [--precision fp64|mixed]
 
 A step is one converged solve (outer residual max(residU, residV,
 residMassDof) <= 1e-6) of the workload's design(s), started from the zero
@@ -25,6 +25,14 @@ admission, continuous batching); latency is wall clock from arrival to
 convergence.  Both lines carry the plain FP64 single-design path on the same
 designs, one after another, as the comparison, and the relative dP
 difference of every design against it.
+
+--workload thermal: the 3-D conjugate-heat-transfer step on the
+1000 x 500 x 9 crop of the density-field design's flow (--thermal-nx 500
+for a quarter of it); a step is one thermal solve from T_inlet to a relative
+residual of 1e-6; e2e uploads gamma, u, v and the heat flux and downloads the
+temperature field every step.  Its CPU baseline is a scipy port of the same
+algorithm (the reference's own thermal solve needs AMGCL, which is absent),
+and --impl reference prints an unavailable line.
 
 --impl reference times the reference solver's own CPU implementation
 (oracle/_ref/ref_f64: its sources promoted to FP64, all host threads) on the
