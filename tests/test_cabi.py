@@ -1,11 +1,13 @@
-"""libcps.so loads, exports every entry point include/cps.h declares, and its
-structs have the layout the ctypes binding assumes.  No GPU calls."""
+"""libcps.so loads, exports every entry point include/*.h declares, its structs
+have the layout the ctypes binding assumes, and its host-only functions
+(defaults, thermal metrics and files) behave.  No GPU calls."""
 import ctypes
 import os
 import re
 import subprocess
 import tempfile
 
+import numpy as np
 import pytest
 
 from conftest import REPO
@@ -91,3 +93,41 @@ def test_argument_validation_without_gpu():
     assert lib.cps_create(None, None) == cps.CPS_ERR_ARG
     assert lib.cps_step(None, None, None) == cps.CPS_ERR_ARG
     assert lib.cps_version().startswith(b"cps")
+
+
+def test_host_defaults_match_the_reference_members():
+    """cps_pseudo_defaults and cps_thermal_defaults (host code) give the
+    reference's member defaults, the same the Python dataclasses carry."""
+    from coldplate_solver_b200 import geometry, thermal
+    from oracle import thermal as th
+    lib = cps.load_library()
+    p = cps.CpsPseudo()
+    assert lib.cps_pseudo_defaults(ctypes.byref(p), 0.25) == cps.CPS_OK
+    d = geometry.straight_channel(M=10, N=12, band=(3, 7)).replace(inletVelocity=0.25)
+    ref = cps.pseudo_from_design(d)
+    for name, _ in cps.CpsPseudo._fields_:
+        if name in ("enable", "time_step"):
+            continue
+        assert getattr(p, name) == getattr(ref, name), name
+    assert p.enable == 0 and p.time_step == 0.0
+    t = cps.CpsThermalDesc()
+    assert lib.cps_thermal_defaults(ctypes.byref(t)) == cps.CPS_OK
+    tp = th.ThermalParams(Nx=1, Ny=1, dx=1.0, dy=1.0)
+    tc = thermal.ThermalCase(gamma=np.ones((1, 1)), u=np.zeros((1, 1)), v=np.zeros((1, 1)), dx=1.0, dy=1.0)
+    for name in ("nz_solid", "nz_fluid", "H_b", "H_t", "k_s", "k_f", "rho", "Cp", "T_inlet", "rtol", "maxiter",
+                 "k_interp_mode", "qk"):
+        assert getattr(t, name) == getattr(tp, name) == getattr(tc, name), name
+
+
+def test_thermal_host_functions_validate(tmp_path):
+    lib = cps.load_library()
+    d = cps.CpsThermalDesc()
+    lib.cps_thermal_defaults(ctypes.byref(d))
+    m = cps.CpsThermalMetrics()
+    T = np.zeros(9)
+    g = np.ones(1)
+    assert lib.cps_thermal_compute_metrics(ctypes.byref(d), cps._dptr(T), cps._dptr(g), ctypes.byref(m)) == cps.CPS_ERR_ARG
+    d.Nx, d.Ny, d.dx, d.dy = 1, 1, 1e-5, 1e-5
+    assert lib.cps_thermal_compute_metrics(ctypes.byref(d), cps._dptr(T), cps._dptr(g), ctypes.byref(m)) == cps.CPS_OK
+    assert lib.cps_thermal_save(str(tmp_path / "missing" / "dir").encode(), ctypes.byref(d), cps._dptr(T), cps._dptr(g),
+                                cps._dptr(g), cps._dptr(g)) == cps.CPS_ERR_ARG
