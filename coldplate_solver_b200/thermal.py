@@ -51,8 +51,10 @@ class ThermalCase:
         self.v = np.ascontiguousarray(self.v, dtype=np.float64)
         if self.q0 is not None:
             self.q0 = np.ascontiguousarray(self.q0, dtype=np.float64)
-        if self.u.shape != self.gamma.shape or self.v.shape != self.gamma.shape:
+        if self.gamma.ndim != 2 or self.u.shape != self.gamma.shape or self.v.shape != self.gamma.shape:
             raise ValueError("gamma, u and v must have the same (Ny, Nx) shape")
+        if self.q0 is not None and self.q0.shape != self.gamma.shape:
+            raise ValueError("q0 must have the (Ny, Nx) shape of gamma")
 
     @property
     def Ny(self) -> int:
@@ -141,6 +143,8 @@ def metrics(case: ThermalCase, T: np.ndarray) -> Dict[str, float]:
     uniformity and gradient statistics (cps_thermal_compute_metrics)."""
     lib = cps.load_library()
     T = np.ascontiguousarray(T, dtype=np.float64)
+    if T.shape != (case.Nz, case.Ny, case.Nx):
+        raise ValueError("T must be (Nz, Ny, Nx)")
     m = cps.CpsThermalMetrics()
     d = _desc(case)
     st = lib.cps_thermal_compute_metrics(ctypes.byref(d), cps._dptr(T), cps._dptr(case.gamma), ctypes.byref(m))
@@ -155,6 +159,8 @@ def save(directory: str, case: ThermalCase, T: np.ndarray) -> None:
     cps_thermal_save)."""
     lib = cps.load_library()
     T = np.ascontiguousarray(T, dtype=np.float64)
+    if T.shape != (case.Nz, case.Ny, case.Nx):
+        raise ValueError("T must be (Nz, Ny, Nx)")
     d = _desc(case)
     st = lib.cps_thermal_save(directory.encode(), ctypes.byref(d), cps._dptr(T), cps._dptr(case.gamma),
                               cps._dptr(case.u), cps._dptr(case.v))
