@@ -218,3 +218,38 @@ def run_thermal_outputs(T: np.ndarray, gamma: np.ndarray, dx: float, dy: float, 
             "grad_max", "grad_avg", "grad_max_base", "grad_avg_base", "grad_max_i", "grad_max_j", "grad_max_k",
             "dx", "dy")
     return {"metrics": dict(zip(keys, vals.tolist())), "files": files}
+
+
+def run_thermal_assembly(Nx: int, Ny: int, dx: float, dy: float, gamma: np.ndarray, u: np.ndarray, v: np.ndarray,
+                         q0: np.ndarray, nz_solid: int = 2, nz_fluid: int = 7, H_b: float = 0.0005,
+                         H_t: float = 0.004, k_s: float = 400.0, k_f: float = 0.6, rho: float = 998.0,
+                         Cp: float = 4180.0, T_inlet: float = 30.0, qk: float = 1.0, k_interp_mode: int = 1,
+                         T: Optional[np.ndarray] = None, timeout: float = 600) -> Dict[str, object]:
+    """The matrix (CSR) and right-hand side the reference's own
+    ThermalSolver3D::solve assembles (harness oracle/thermal_asm_harness.cpp),
+    with the reference's Params::dx() = (Nx dx) / Nx.  Given a temperature
+    field T (Nz, Ny, Nx), also the bytes of the thermal_results_3d.vtk the
+    reference's save_vtk writes for it ("vtk")."""
+    path = os.path.join(REF_DIR, "thermal_asm")
+    if not os.access(path, os.X_OK):
+        raise FileNotFoundError(f"{path} not built (make -C oracle ref)")
+    with tempfile.TemporaryDirectory(prefix="cps_thasm_") as tmp:
+        cpath, opath = os.path.join(tmp, "case.bin"), os.path.join(tmp, "out.bin")
+        casefile.write_records(cpath, {
+            "ints": np.array([Nx, Ny, nz_solid, nz_fluid, k_interp_mode], dtype=np.int32),
+            "reals": [dx, dy, H_b, H_t, k_s, k_f, rho, Cp, T_inlet, qk],
+            "gamma": np.ascontiguousarray(gamma, dtype=np.float64).ravel(),
+            "u": np.ascontiguousarray(u, dtype=np.float64).ravel(),
+            "v": np.ascontiguousarray(v, dtype=np.float64).ravel(),
+            "q0": np.ascontiguousarray(q0, dtype=np.float64).ravel(),
+            **({} if T is None else {"T": np.ascontiguousarray(T, dtype=np.float64).ravel()})})
+        env = dict(os.environ, OMP_NUM_THREADS="1")
+        proc = subprocess.run([path, cpath, opath], cwd=tmp, env=env, stdout=subprocess.DEVNULL,
+                              stderr=subprocess.PIPE, timeout=timeout)
+        if proc.returncode != 0:
+            raise RuntimeError(f"thermal_asm failed: {proc.stderr.decode()[-2000:]}")
+        out: Dict[str, object] = dict(casefile.read_records(opath))
+        if T is not None:
+            with open(os.path.join(tmp, "thermal_results_3d.vtk"), "rb") as f:
+                out["vtk"] = f.read()
+        return out

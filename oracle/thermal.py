@@ -3,14 +3,14 @@
 CUDA thermal path is checked against; no product code calls it (tests use
 it, and bench.py's CPU-baseline leg times mg_bicgstab_cpu).
 
-Parity unpinned: the reference's thermal solver cannot be built here (it
-includes AMGCL, whose headers are absent from the reference tree:
-ThermalSolver/amgcl/ is empty and no version is pinned), so this module is
-checked only against itself (two independent restatements of the matrix
-assembly, vectorised and per cell) and against the physics (energy balance);
-the linear solve is a direct sparse LU (scipy), i.e. the exact solution of the
-system the reference's AMG/IDR(s) solve approximates to a relative residual
-of rtol.
+Parity: the assembly is pinned against the reference's own code.  The
+reference's thermal solver includes AMGCL, whose headers are absent from the
+reference tree (ThermalSolver/amgcl/ is empty and no version is pinned), so it
+cannot be built whole; oracle/thermal_asm_harness.cpp compiles it with the
+AMGCL solve cut out, and the matrix and right-hand side it assembles equal
+this module's bit for bit.  The linear solve here is a direct sparse LU
+(scipy), i.e. the exact solution of the system the reference's AMGCL solve
+approximates to a relative residual of rtol; that solve itself stays unpinned.
 
 Index space: T[k, j, i] with P = k*Nx*Ny + j*Nx + i (thermal_solver.cpp:241);
 2-D inputs (gamma, u, v, q0) are (Ny, Nx), gamma = 1 fluid, 0 solid

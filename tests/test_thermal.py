@@ -2,9 +2,12 @@
 3-D CHT assembly (thermal_solver.cpp:420-517) equals the per-cell
 restatement in the reference's own loop structure bit for bit, and the
 direct solution keeps the reference's energy balance."""
+import os
+
 import numpy as np
 import pytest
 
+from oracle import reference
 from oracle import thermal as th
 
 
@@ -61,3 +64,24 @@ def test_cpu_port_reaches_the_stop_rule():
     assert th.relative_residual(p, planes, b, T) <= p.rtol * 1.0001
     Td = th.solve_direct(p, gamma, u, v, q0)
     assert np.linalg.norm(T - Td) / np.linalg.norm(Td - p.T_inlet) < 1e-3
+
+
+@pytest.mark.skipif(not os.access(os.path.join(reference.REF_DIR, "thermal_asm"), os.X_OK),
+                    reason="oracle/_ref/thermal_asm not built")
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("shape", [(13, 9), (31, 17)])
+def test_assembly_equals_the_reference_assembly(shape, mode):
+    """The oracle's assembly against the reference's own ThermalSolver3D::solve
+    assembly (run with its AMGCL solve cut out): every CSR entry and the
+    right-hand side, bit for bit."""
+    Nx, Ny = shape
+    p, gamma, u, v, q0 = case(Nx=Nx, Ny=Ny, seed=Nx + mode, mode=mode)
+    ref = reference.run_thermal_assembly(Nx, Ny, p.dx, p.dy, gamma, u, v, q0, H_t=p.H_t, qk=p.qk,
+                                         k_interp_mode=mode)
+    p.dx, p.dy = float(ref["dxdy"][0]), float(ref["dxdy"][1])  # Params::dx() = (Nx dx) / Nx
+    planes, b = th.assemble(p, gamma, u, v, q0)
+    A = th.to_csr(p, planes)
+    A.sort_indices()
+    assert np.array_equal(A.indptr, ref["row_ptr"]) and np.array_equal(A.indices, ref["col_idx"])
+    assert np.array_equal(A.data, ref["values"])
+    assert np.array_equal(b.ravel(), ref["b"])

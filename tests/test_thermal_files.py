@@ -3,8 +3,9 @@ host code) against the reference's own thermal output module
 (ThermalSolver/thermal_output.cpp compiled under oracle/thermal_out_harness.cpp):
 the metrics equal bit for bit and thermal_metrics.txt, k_thermal.txt and
 thermal_gradient_3d.vtk are byte-identical.  thermal_results_3d.vtk is
-written by a member of the reference's solver class, which cannot be built
-(it needs AMGCL): its layout is checked here, not its bytes."""
+written by a member of the reference's solver class (save_vtk), which is run
+through oracle/thermal_asm_harness.cpp (the class compiled with its AMGCL solve
+cut out): byte-identical too."""
 import os
 
 import numpy as np
@@ -65,3 +66,17 @@ def test_from_export_reads_the_reference_inputs(tmp_path):
     np.testing.assert_array_equal(c.gamma, 1.0 - (1.0 - gamma))
     np.testing.assert_array_equal(c.u, u)
     np.testing.assert_array_equal(c.v, v)
+
+
+@pytest.mark.skipif(not os.access(os.path.join(reference.REF_DIR, "thermal_asm"), os.X_OK),
+                    reason="oracle/_ref/thermal_asm not built")
+@pytest.mark.parametrize("seed,Ht", [(0, 5e-4), (3, 4e-3)])
+def test_results_vtk_equals_the_reference_writer(tmp_path, seed, Ht):
+    gamma, T, u, v = field(seed=seed)
+    Ny, Nx = gamma.shape
+    dx = 1.7e-5
+    ref = reference.run_thermal_assembly(Nx, Ny, dx, dx, gamma, u, v, np.zeros((Ny, Nx)), H_t=Ht, T=T)
+    ddx, ddy = (float(x) for x in ref["dxdy"])
+    case = pt.ThermalCase(gamma=gamma, u=u, v=v, dx=ddx, dy=ddy, H_t=Ht)
+    pt.save(str(tmp_path), case, T)
+    assert (tmp_path / "thermal_results_3d.vtk").read_bytes() == ref["vtk"]
