@@ -8,7 +8,8 @@ reference's thermal solver includes AMGCL, whose headers are absent from the
 reference tree (ThermalSolver/amgcl/ is empty and no version is pinned), so it
 cannot be built whole; oracle/thermal_asm_harness.cpp compiles it with the
 AMGCL solve cut out, and the matrix and right-hand side it assembles equal
-this module's bit for bit.  The linear solve here is a direct sparse LU
+this module's bit for bit (live, and through the committed fixtures
+tests/golden/thermal_asm_*).  The linear solve here is a direct sparse LU
 (scipy), i.e. the exact solution of the system the reference's AMGCL solve
 approximates to a relative residual of rtol; that solve itself stays unpinned.
 
@@ -475,3 +476,24 @@ def mg_bicgstab_cpu(p: ThermalParams, gamma, u, v, q0, sweeps: int = 2, omega: f
         rho, rho_new = rho_new, float(rhat @ r)
         it += 1
     return T.reshape(Nz, p.Ny, p.Nx), it, time.perf_counter() - t0, True
+
+
+def load_assembly_fixture(path: str):
+    """A thermal_asm_* golden fixture (tests/golden/make_golden.py): the
+    ThermalParams, the inputs (gamma, u, v, q0) and the reference's own CSR
+    matrix (scipy, sorted indices) and right-hand side for them."""
+    import scipy.sparse as sp
+    z = np.load(path)
+    Nx, Ny, nzs, nzf, mode = (int(x) for x in z["ints"])
+    dx, dy, H_b, H_t, k_s, k_f, rho, Cp, T_inlet, qk = (float(x) for x in z["reals"])
+    p = ThermalParams(Nx=Nx, Ny=Ny, dx=dx, dy=dy, nz_solid=nzs, nz_fluid=nzf, H_b=H_b, H_t=H_t, k_s=k_s, k_f=k_f,
+                      rho=rho, Cp=Cp, T_inlet=T_inlet, k_interp_mode=mode, qk=qk)
+    A = sp.csr_matrix((z["values"], z["col_idx"], z["row_ptr"]), shape=(p.n, p.n))
+    inputs = {k: np.asarray(z[k]) for k in ("gamma", "u", "v", "q0")}
+    return p, inputs, A, np.asarray(z["b"])
+
+
+def same_csr(A, B) -> bool:
+    """Bit-identical sparsity structure and values (both sorted)."""
+    return (A.shape == B.shape and np.array_equal(A.indptr, B.indptr) and np.array_equal(A.indices, B.indices)
+            and np.array_equal(A.data.view(np.uint64), B.data.view(np.uint64)))

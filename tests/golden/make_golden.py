@@ -5,6 +5,11 @@ as shipped), run with one OpenMP thread so every reduction is sequential.
 Run from the repository root where the reference sources are available:
     make -C oracle ref && python tests/golden/make_golden.py
 The fixtures are committed; tests read them without the reference present.
+
+`python tests/golden/make_golden.py thermal` writes only the thermal_asm_*
+fixtures: the CSR matrix and right-hand side that the reference's own
+ThermalSolver3D::solve assembles (oracle/_ref/thermal_asm, the solver class
+compiled with its AMGCL solve cut out) for seeded inputs, with those inputs.
 """
 from __future__ import annotations
 
@@ -61,5 +66,41 @@ def main() -> None:
     print("wrote alpha_ramp_17x23")
 
 
+THERMAL_PARAMS = ("dx", "dy", "H_b", "H_t", "k_s", "k_f", "rho", "Cp", "T_inlet", "qk")
+
+
+def thermal_cases():
+    # name, Nx, Ny, seed, k_interp_mode, H_t, qk, nz_solid, nz_fluid
+    yield "thermal_asm_13x9_mode0", 13, 9, 1, 0, 4e-4, 1.0, 2, 7
+    yield "thermal_asm_13x9_mode1", 13, 9, 2, 1, 4e-4, 3.0, 2, 7
+    yield "thermal_asm_13x9_mode2", 13, 9, 3, 2, 4e-4, 3.0, 2, 7
+    yield "thermal_asm_21x11_mode1_h3", 21, 11, 4, 1, 3e-3, 10.0, 3, 5
+
+
+def thermal_main() -> None:
+    for name, Nx, Ny, seed, mode, Ht, qk, nzs, nzf in thermal_cases():
+        rng = np.random.default_rng(seed)
+        gamma = (rng.random((Ny, Nx)) > 0.4).astype(float)
+        gamma[rng.random((Ny, Nx)) > 0.85] = 0.37
+        gamma[:, 0] = 1.0
+        u = np.abs(rng.normal(0.2, 0.15, (Ny, Nx))) * gamma
+        v = rng.normal(0.0, 0.05, (Ny, Nx)) * gamma
+        q0 = rng.uniform(5e5, 1.5e6, (Ny, Nx)) if mode != 0 else np.full((Ny, Nx), 8e5)
+        dx = dy = 20e-6
+        ref = reference.run_thermal_assembly(Nx, Ny, dx, dy, gamma, u, v, q0, nz_solid=nzs, nz_fluid=nzf, H_t=Ht,
+                                             qk=qk, k_interp_mode=mode)
+        p = dict(dx=float(ref["dxdy"][0]), dy=float(ref["dxdy"][1]), H_b=0.0005, H_t=Ht, k_s=400.0, k_f=0.6,
+                 rho=998.0, Cp=4180.0, T_inlet=30.0, qk=qk)
+        rec = dict(ints=np.array([Nx, Ny, nzs, nzf, mode], dtype=np.int64),
+                   reals=np.array([p[k] for k in THERMAL_PARAMS]), gamma=gamma, u=u, v=v, q0=q0,
+                   row_ptr=np.asarray(ref["row_ptr"], dtype=np.int64), col_idx=np.asarray(ref["col_idx"], dtype=np.int64),
+                   values=np.asarray(ref["values"]), b=np.asarray(ref["b"]))
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **rec)
+        print("wrote", name)
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["thermal"]:
+        thermal_main()
+    else:
+        main()

@@ -85,3 +85,23 @@ def test_assembly_equals_the_reference_assembly(shape, mode):
     assert np.array_equal(A.indptr, ref["row_ptr"]) and np.array_equal(A.indices, ref["col_idx"])
     assert np.array_equal(A.data, ref["values"])
     assert np.array_equal(b.ravel(), ref["b"])
+
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+ASM_FIXTURES = sorted(f for f in os.listdir(GOLDEN) if f.startswith("thermal_asm_"))
+
+
+def test_assembly_fixtures_exist():
+    assert len(ASM_FIXTURES) >= 4
+
+
+@pytest.mark.parametrize("name", ASM_FIXTURES)
+def test_assembly_equals_the_reference_fixture(name):
+    """The committed output of the reference's own assembly (no reference
+    needed at test time) against the oracle's, bit for bit."""
+    p, x, A_ref, b_ref = th.load_assembly_fixture(os.path.join(GOLDEN, name))
+    planes, b = th.assemble(p, x["gamma"], x["u"], x["v"], x["q0"])
+    A = th.to_csr(p, planes)
+    A.sort_indices()
+    assert th.same_csr(A, A_ref)
+    assert np.array_equal(b.ravel().view(np.uint64), b_ref.view(np.uint64))

@@ -1,9 +1,12 @@
 """The 3-D conjugate-heat-transfer solve on the GPU (cps_thermal_*) against
-the thermal oracle (oracle/thermal.py; parity unpinned against the reference
-itself, whose solve needs the absent AMGCL): the device-assembled system
-equals the oracle's restatement of the reference's assembly bit for bit, and
-the device solution satisfies the reference's stop rule on that system and
-agrees with its exact (direct) solution."""
+the thermal oracle (oracle/thermal.py) and the reference's own assembly: the
+device-assembled system equals the committed CSR matrix and right-hand side
+of the reference's ThermalSolver3D::solve (tests/golden/thermal_asm_*) and the
+oracle's restatement of it bit for bit, and the device solution satisfies the
+reference's stop rule on that system and agrees with its exact (direct)
+solution (the reference's AMGCL solve itself cannot be built)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -51,6 +54,23 @@ def test_device_system_equals_the_oracle_assembly(shape, mode):
     for k in th.PLANES:
         assert np.array_equal(planes[k], po[k]), k
     assert np.array_equal(b, bo)
+
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.mark.parametrize("name", sorted(f for f in os.listdir(GOLDEN) if f.startswith("thermal_asm_")))
+def test_device_system_equals_the_reference_assembly(name):
+    p, x, A_ref, b_ref = th.load_assembly_fixture(os.path.join(GOLDEN, name))
+    c = pt.ThermalCase(gamma=x["gamma"], u=x["u"], v=x["v"], dx=p.dx, dy=p.dy, q0=x["q0"], nz_solid=p.nz_solid,
+                       nz_fluid=p.nz_fluid, H_b=p.H_b, H_t=p.H_t, k_s=p.k_s, k_f=p.k_f, rho=p.rho, Cp=p.Cp,
+                       T_inlet=p.T_inlet, k_interp_mode=p.k_interp_mode, qk=p.qk)
+    with pt.ThermalSolver(c) as s:
+        planes, b = s.system()
+    A = th.to_csr(p, planes)
+    A.sort_indices()
+    assert th.same_csr(A, A_ref)
+    assert np.array_equal(np.asarray(b).ravel().view(np.uint64), b_ref.view(np.uint64))
 
 
 @pytest.mark.parametrize("shape", [(13, 9), (37, 23), (64, 40)])
