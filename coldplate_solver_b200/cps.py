@@ -203,6 +203,7 @@ SIGNATURES = {
     "cps_thermal_destroy": (None, [_P]),
     "cps_thermal_last_error": (ctypes.c_char_p, [_P]),
     "cps_last_error": (ctypes.c_char_p, [_P]),
+    "cps_barrier_selftest": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "cps_version": (ctypes.c_char_p, []),
 }
 

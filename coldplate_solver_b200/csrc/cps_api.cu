@@ -534,11 +534,54 @@ BatchWorkspace* batch_workspace(int device, size_t n, std::string& err) {
 
 }  // namespace
 
+// The persistent kernels' grid barrier, told to expect `expect` CTAs: with more
+// than the launch has, the count it waits for is never reached and the wait
+// ends only by its time limit (cps_barrier_selftest).
+__global__ void __launch_bounds__(cps::kThreads) cps_barrier_selftest_kernel(cps::GridBarrier* bar, int* status,
+                                                                            unsigned expect) {
+  cps::GridGroup g{bar, nullptr, status, blockIdx.x, expect, 0u, 0ull};
+  g.sync();
+}
+
 extern "C" {
 
 const char* cps_version(void) { return "cps 0.2 (sm_100a)"; }
 
 const char* cps_last_error(const cps_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+
+cps_status cps_barrier_selftest(int device, int ctas, double* kernel_ms) {
+  if (ctas < 1 || ctas > 1024) return fail(nullptr, CPS_ERR_ARG, "ctas must be in 1..1024");
+  if (kernel_ms) *kernel_ms = 0.0;
+  if (!cuda_ok(nullptr, cudaSetDevice(device), "cudaSetDevice")) return CPS_ERR_CUDA;
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  char* mem = nullptr;
+  int status = -1;
+  float ms = 0.0f;
+  // counter at [0], status at [64]
+  bool ok = cuda_ok(nullptr, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "stream") &&
+            cuda_ok(nullptr, cudaMalloc(&mem, 128), "device allocation") &&
+            cuda_ok(nullptr, cudaEventCreate(&e0), "event") && cuda_ok(nullptr, cudaEventCreate(&e1), "event") &&
+            cuda_ok(nullptr, cudaMemsetAsync(mem, 0, 128, st), "memset") &&
+            cuda_ok(nullptr, cudaEventRecord(e0, st), "event");
+  if (ok) {
+    cps_barrier_selftest_kernel<<<ctas, cps::kThreads, 0, st>>>(reinterpret_cast<cps::GridBarrier*>(mem),
+                                                                 reinterpret_cast<int*>(mem + 64), (unsigned)ctas + 1u);
+    ok = cuda_ok(nullptr, cudaGetLastError(), "launch") && cuda_ok(nullptr, cudaEventRecord(e1, st), "event") &&
+         cuda_ok(nullptr, cudaMemcpyAsync(&status, mem + 64, sizeof(int), cudaMemcpyDeviceToHost, st), "d2h") &&
+         cuda_ok(nullptr, cudaStreamSynchronize(st), "barrier self-test") &&
+         cuda_ok(nullptr, cudaEventElapsedTime(&ms, e0, e1), "event time");
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (mem) cudaFree(mem);
+  if (st) cudaStreamDestroy(st);
+  if (!ok) return CPS_ERR_CUDA;
+  if (kernel_ms) *kernel_ms = ms;
+  if (status == cps::kStatusTimeout) return fail(nullptr, CPS_ERR_TIMEOUT, "device grid barrier timed out");
+  if (status == cps::kStatusOk) return CPS_OK;
+  return fail(nullptr, CPS_ERR_STATE, "barrier self-test: unexpected device status");
+}
 
 cps_status cps_footprint(const cps_desc* desc, unsigned long long* bytes) {
   cps_status s = validate(desc);

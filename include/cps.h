@@ -376,6 +376,16 @@ cps_status cps_save_all(const char* dir, int M, int N, double hx, double hy, int
 /* Message of the last failed (or warning) file call on this thread. */
 const char* cps_io_last_error(void);
 
+/* Self-test of the persistent kernels' failure detection: launches `ctas`
+ * CTAs (1..1024) on `device` that wait at the grid barrier the persistent
+ * kernels use, told to expect one CTA more than the launch has, so the wait
+ * can end only by its time limit (2 s of %globaltimer), after which the
+ * kernel records a timeout status and every CTA returns.  Returns
+ * CPS_ERR_TIMEOUT, the expected outcome, with the kernel's run time in
+ * *kernel_ms (may be NULL) and the message in cps_last_error(NULL); CPS_OK
+ * would mean the barrier let the CTAs through short of their count. */
+cps_status cps_barrier_selftest(int device, int ctas, double* kernel_ms);
+
 /* Message of the last failed call on ctx (or of the last failed cps_create
  * on this thread when ctx is NULL). */
 const char* cps_last_error(const cps_ctx* ctx);

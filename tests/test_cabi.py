@@ -92,6 +92,9 @@ def test_argument_validation_without_gpu():
     assert lib.cps_footprint(ctypes.byref(bad), ctypes.byref(out)) == cps.CPS_ERR_ARG
     assert lib.cps_create(None, None) == cps.CPS_ERR_ARG
     assert lib.cps_step(None, None, None) == cps.CPS_ERR_ARG
+    assert lib.cps_barrier_selftest(0, 0, None) == cps.CPS_ERR_ARG
+    assert lib.cps_barrier_selftest(0, 1025, None) == cps.CPS_ERR_ARG
+    assert b"1..1024" in lib.cps_last_error(None)
     assert lib.cps_version().startswith(b"cps")
 
 
