@@ -204,6 +204,8 @@ SIGNATURES = {
     "cps_thermal_last_error": (ctypes.c_char_p, [_P]),
     "cps_last_error": (ctypes.c_char_p, [_P]),
     "cps_barrier_selftest": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "cps_save_logs": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(CpsStepOut), _P, _P,
+                                     ctypes.c_double]),
     "cps_version": (ctypes.c_char_p, []),
 }
 

@@ -224,4 +224,25 @@ cps_status cps_save_all(const char* dir, int M, int N, double hx, double hy, int
   return vtk ? CPS_OK : io_fail(CPS_ERR_ARG, "write failed: " + d + "/fluid_results.vtk");
 }
 
+cps_status cps_save_logs(const char* dir, int n, int iter0, const cps_step_out* hist, const double* dp,
+                         const double* cfl, double cfl0) {
+  if (!dir || n < 0 || (n > 0 && !hist)) return io_fail(CPS_ERR_ARG, "dir, n >= 0 and hist are required");
+  const std::string d(dir);
+  // initLogFiles (output.cpp:268-275)
+  std::ofstream resid(d + "/residuals.txt"), dpf(d + "/pressure_drop_history.txt");
+  if (!resid.is_open() || !dpf.is_open()) return io_fail(CPS_ERR_ARG, "could not write to " + d);
+  resid << "Iter MassResid UResid VResid Core_dP_AfterInletBuffer(Pa) "
+        << "Full_dP_FullSystem(Pa) CFL" << std::endl;
+  dpf << "Iter Core_Total(Pa) Full_Total(Pa) Core_Static(Pa) Full_Static(Pa)" << std::endl;
+  // writeIterationLogs (output.cpp:292-313), one row per outer iteration
+  for (int k = 0; k < n; ++k) {
+    const double* q = dp ? dp + (size_t)4 * k : nullptr;
+    const double core = q ? q[0] : 0.0, full = q ? q[1] : 0.0, coreS = q ? q[2] : 0.0, fullS = q ? q[3] : 0.0;
+    resid << iter0 + k << " " << hist[k].residMass << " " << hist[k].residU << " " << hist[k].residV << " " << core
+          << " " << full << " " << (cfl ? cfl[k] : cfl0) << std::endl;
+    dpf << iter0 + k << " " << core << " " << full << " " << coreS << " " << fullS << std::endl;
+  }
+  return (resid && dpf) ? CPS_OK : io_fail(CPS_ERR_ARG, "write failed in " + d);
+}
+
 }  // extern "C"

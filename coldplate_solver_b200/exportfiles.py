@@ -1,8 +1,9 @@
 """The reference's files at the boundary, through libcps's C++ readers and
 writer (include/cps.h): the case a geometry export leaves in ExportFiles
 (fluid_params.txt, geometry_fluid.txt; SIMPLE.cpp:31-47, 517-584), the
-restart matrices u/v/p.txt (SIMPLE.cpp:203-232) and saveAll's output
-(output.cpp:73-266).  Host code only; no GPU is needed."""
+restart matrices u/v/p.txt (SIMPLE.cpp:203-232), saveAll's output
+(output.cpp:73-266) and the outer loop's logs (output.cpp:268-313).  Host
+code only; no GPU is needed."""
 from __future__ import annotations
 
 import ctypes
@@ -72,6 +73,25 @@ def save_all(directory: str, M: int, N: int, hx: float, hy: float, fields: Dict[
     _check(_lib().cps_save_all(directory.encode(), M, N, hx, hy, N_in_buffer, N_out_buffer, cps._dptr(arrs["u"]),
                                cps._dptr(arrs["v"]), cps._dptr(arrs["p"]), cps._dptr(c), cps._dptr(g), cps._dptr(a),
                                cps.CPS_ROW_MAJOR))
+
+
+def save_logs(directory: str, hist: np.ndarray, dp: Optional[np.ndarray] = None, cfl: Optional[np.ndarray] = None,
+              cfl0: float = 0.1, iter0: int = 0) -> None:
+    """runIterations' residuals.txt and pressure_drop_history.txt
+    (output.cpp:268-313) into ``directory``: ``hist`` is a solve's (n, 8)
+    history (residU, residV, residMass, ...), ``dp`` the (n, 4) drops of
+    cps_solve_monitored (core total, full total, core static, full static;
+    None logs 0), ``cfl`` the per-iteration CFL numbers (None: ``cfl0``, the
+    reference's pseudoCFL default, on every row)."""
+    os.makedirs(directory, exist_ok=True)
+    h = np.asarray(hist, dtype=np.float64).reshape(-1, 8)
+    n = h.shape[0]
+    rows = (cps.CpsStepOut * max(1, n))()
+    for k in range(n):
+        rows[k].residU, rows[k].residV, rows[k].residMass = float(h[k, 0]), float(h[k, 1]), float(h[k, 2])
+    d = None if dp is None else np.ascontiguousarray(np.asarray(dp, dtype=np.float64).reshape(n, 4))
+    c = None if cfl is None else np.ascontiguousarray(np.asarray(cfl, dtype=np.float64).reshape(n))
+    _check(_lib().cps_save_logs(directory.encode(), n, iter0, rows, cps._dptr(d), cps._dptr(c), cfl0))
 
 
 def design_from_export(directory: str, **overrides):

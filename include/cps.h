@@ -373,6 +373,19 @@ cps_status cps_save_all(const char* dir, int M, int N, double hx, double hy, int
                         const double* u, const double* v, const double* p, const double* cellType,
                         const double* gamma, const double* alpha, int layout);
 
+/* The outer loop's two logs as runIterations writes them (initLogFiles and
+ * writeIterationLogs, output.cpp:268-313): dir/residuals.txt (iteration,
+ * mass, U and V residuals, core and full total-pressure drop, CFL number)
+ * and dir/pressure_drop_history.txt (iteration, core total, full total,
+ * core static, full static drop), one row per outer iteration numbered from
+ * iter0, numbers as the reference prints them.  hist: n rows of a solve's
+ * history (residMass, residU, residV are logged); dp: n x 4 drops in that
+ * order (cps_solve_monitored's), or NULL to log 0; cfl: n CFL numbers, or
+ * NULL to log cfl0 on every row (pseudoCFL, constant while pseudo-time
+ * stepping is off). */
+cps_status cps_save_logs(const char* dir, int n, int iter0, const cps_step_out* hist, const double* dp,
+                         const double* cfl, double cfl0);
+
 /* Message of the last failed (or warning) file call on this thread. */
 const char* cps_io_last_error(void);
 

@@ -96,7 +96,8 @@ def run_iterations(design, max_iterations: int, window: int, percent: float, ram
     its CFL controllers run after every step.  Returns its
     per-iteration pressure-drop log (``dpIter``; ``dp`` (n, 4): core total,
     full total, core static, full static, as pressure_drop_history.txt prints
-    them, 6 significant digits) and the final fields."""
+    them, 6 significant digits), the final fields and ``logs``: the texts of
+    the residuals.txt and pressure_drop_history.txt it wrote."""
     if not available(precision):
         raise FileNotFoundError(f"{binary(precision)} not built (make -C oracle ref)")
     with tempfile.TemporaryDirectory(prefix="cps_ref_") as tmp:
@@ -112,6 +113,10 @@ def run_iterations(design, max_iterations: int, window: int, percent: float, ram
         if proc.returncode != 0:
             raise RuntimeError(f"reference harness failed: {proc.stderr.decode()[-2000:]}")
         out = casefile.read_records(opath)
+        out["logs"] = {}
+        for name in ("residuals.txt", "pressure_drop_history.txt"):
+            with open(os.path.join(tmp, "ExportFiles", name), "rb") as f:
+                out["logs"][name] = f.read()
     M, N = design.M, design.N
     for k, s in {"u": (M + 1, N), "v": (M, N + 1), "p": (M + 1, N + 1)}.items():
         out[k] = out[k].reshape(s)

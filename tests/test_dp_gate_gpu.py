@@ -11,7 +11,8 @@ import ctypes
 import numpy as np
 import pytest
 
-from coldplate_solver_b200 import cps, geometry
+from coldplate_solver_b200 import cps, exportfiles, geometry
+from oracle import reference
 from oracle import restatement as rs
 
 pytestmark = pytest.mark.gpu
@@ -87,3 +88,27 @@ def test_monitor_arguments_are_checked():
         s.set_dp_monitor(enabled=False)
         with pytest.raises(cps.CpsError):
             s.solve_monitored(5)
+
+
+@pytest.mark.skipif(not reference.available("f64"), reason="oracle/_ref/ref_f64 not built")
+def test_device_logs_match_the_reference_logs(tmp_path):
+    """residuals.txt and pressure_drop_history.txt from the device's monitored
+    solve (cps_save_logs) against the ones the reference's own runIterations
+    writes: the same rows, numbers equal to the six digits both print."""
+    d = geometry.straight_channel(M=20, N=40, band=(5, 15))
+    xc = (0.25 * d.N * d.hx, 0.75 * d.N * d.hx)
+    ref = reference.run_iterations(d, 3000, 20, 0.5, 10, x_core=xc)
+    with cps.Solver(d) as s:
+        s.set_dp_monitor(gate=True, window=20, percent=0.5, ramp_steps=10, x_core_in=xc[0], x_core_out=xc[1])
+        hist, dp, conv = s.solve_monitored(3000, eps=0.0)
+    assert conv
+    exportfiles.save_logs(str(tmp_path), hist, dp=dp)
+    for name, cols in (("residuals.txt", 7), ("pressure_drop_history.txt", 5)):
+        mine = (tmp_path / name).read_text().splitlines()
+        theirs = ref["logs"][name].decode().splitlines()
+        assert mine[0] == theirs[0]
+        assert abs(len(mine) - len(theirs)) <= 1
+        k = min(len(mine), len(theirs))
+        a = np.array([[float(x) for x in ln.split()] for ln in mine[1:k]]).reshape(-1, cols)
+        b = np.array([[float(x) for x in ln.split()] for ln in theirs[1:k]]).reshape(-1, cols)
+        np.testing.assert_allclose(a, b, rtol=2e-5, atol=1e-12)
