@@ -105,3 +105,24 @@ def test_assembly_equals_the_reference_fixture(name):
     A.sort_indices()
     assert th.same_csr(A, A_ref)
     assert np.array_equal(b.ravel().view(np.uint64), b_ref.view(np.uint64))
+
+
+@pytest.mark.skipif(not os.access(os.path.join(reference.REF_DIR, "thermal_asm"), os.X_OK),
+                    reason="oracle/_ref/thermal_asm not built")
+@pytest.mark.parametrize("shape,nz,mode", [((1, 7), (2, 7), 1), ((9, 1), (2, 7), 2), ((5, 3), (1, 3), 0),
+                                           ((2, 2), (3, 1), 1), ((17, 12), (1, 1), 2), ((1, 1), (1, 1), 1)])
+def test_edge_grid_assembly_equals_the_reference(shape, nz, mode):
+    """One column, one row, single layers, a single cell: the oracle's
+    assembly against the reference's own, bit for bit."""
+    Nx, Ny = shape
+    p, gamma, u, v, q0 = case(Nx=Nx, Ny=Ny, seed=7 + Nx, mode=mode)
+    p.nz_solid, p.nz_fluid = nz
+    ref = reference.run_thermal_assembly(Nx, Ny, p.dx, p.dy, gamma, u, v, q0, nz_solid=nz[0], nz_fluid=nz[1],
+                                         H_t=p.H_t, qk=p.qk, k_interp_mode=mode)
+    p.dx, p.dy = float(ref["dxdy"][0]), float(ref["dxdy"][1])
+    planes, b = th.assemble(p, gamma, u, v, q0)
+    A = th.to_csr(p, planes)
+    A.sort_indices()
+    assert np.array_equal(A.indptr, ref["row_ptr"]) and np.array_equal(A.indices, ref["col_idx"])
+    assert np.array_equal(A.data, ref["values"])
+    assert np.array_equal(b.ravel(), ref["b"])
