@@ -6,7 +6,8 @@ Run from the repository root where the reference sources are available:
     make -C oracle ref && python tests/golden/make_golden.py
 The fixtures are committed; tests read them without the reference present.
 
-`python tests/golden/make_golden.py thermal` writes only the thermal_asm_*
+`python tests/golden/make_golden.py NAME ...` writes only the named flow
+fixtures; `python tests/golden/make_golden.py thermal` writes only the thermal_asm_*
 fixtures: the CSR matrix and right-hand side that the reference's own
 ThermalSolver3D::solve assembles (oracle/_ref/thermal_asm, the solver class
 compiled with its AMGCL solve cut out) for seeded inputs, with those inputs.
@@ -42,10 +43,22 @@ def cases():
     d = g.straight_channel(M=9, N=17, band=(2, 7)).replace(maxMomentumIter=3, maxPressureIter=2, pTol=1e-12,
                                                             momentumTol=1e-12)
     yield "capped_9x17", d, 6, None
+    # a channel one cell wide
+    yield "single_row_channel_9x21", g.straight_channel(M=9, N=21, band=(4, 5)), 30, None
+    # the band blocked by a solid column except for a one-cell gap, SOU
+    d = g.straight_channel(M=12, N=24, band=(3, 9))
+    gm = d.gamma.copy()
+    gm[3:8, 12] = 0.0
+    a, gm = g.alpha_ramp_reference(gm)
+    yield "gap_12x24_sou", d.replace(gamma=gm, alpha=a, convectionScheme=1), 25, None
+    # odd sizes, SOU
+    yield "odd_7x13_sou", g.straight_channel(M=7, N=13, band=(2, 5)).replace(convectionScheme=1), 20, None
 
 
-def main() -> None:
+def main(selected=()) -> None:
     for name, d, n, init in cases():
+        if selected and name not in selected:
+            continue
         rec = {k: np.asarray(getattr(d, k)) for k in DESIGN_KEYS}
         rec.update(gamma=d.gamma, alpha=d.alpha, n_outer=np.asarray(n))
         if init is not None:
@@ -57,6 +70,8 @@ def main() -> None:
                 rec[f"{prec}_{k}"] = out[k]
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **rec)
         print("wrote", name)
+    if selected:
+        return
     gm = np.random.default_rng(0).random((17, 23))
     rec = {"gamma_in": gm}
     for prec in ("f64", "f32"):
@@ -103,4 +118,4 @@ if __name__ == "__main__":
     if sys.argv[1:] == ["thermal"]:
         thermal_main()
     else:
-        main()
+        main(tuple(sys.argv[1:]))

@@ -188,6 +188,12 @@ def test_converged_solve_straight_channel():
     assert rel(fluid_p(d, f["p"]), fluid_p(d, fr["p"])) <= REL_FIELD
     dpr = rs.full_dp(d, fr)
     assert abs(dp - dpr) <= REL_DP * abs(dpr), (dp, dpr)
+    # Loose physical sanity: plane Poiseuille flow gives dP = 12 mu U L / H^2
+    # (2.67 Pa here); the solved channel has entrance lengths and Brinkman
+    # walls on top (the reference's own solve gives 3.36 Pa).
+    H, L = 40 * d.hy, d.N * d.hx
+    poiseuille = 12.0 * d.eta * d.inletVelocity * L / H ** 2
+    assert poiseuille <= dp <= 1.35 * poiseuille, (dp, poiseuille)
 
 
 def test_edge_cases_minimal_and_zero_caps():
