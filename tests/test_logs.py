@@ -36,3 +36,22 @@ def test_logs_equal_the_reference_files(tmp_path, pseudo):
         assert np.all(res[:, 6] == 0.1)
         exportfiles.save_logs(str(tmp_path / "c"), hist, dp=dph[:, 1:])
         assert (tmp_path / "c" / "residuals.txt").read_bytes() == ref["logs"]["residuals.txt"]
+
+
+def test_logs_edge_cases(tmp_path):
+    """No rows: the two headers only; no pressure drops: logged as 0; bad arguments are refused."""
+    from coldplate_solver_b200 import cps
+    exportfiles.save_logs(str(tmp_path / "empty"), np.zeros((0, 8)))
+    assert (tmp_path / "empty" / "residuals.txt").read_text() == (
+        "Iter MassResid UResid VResid Core_dP_AfterInletBuffer(Pa) Full_dP_FullSystem(Pa) CFL\n")
+    assert (tmp_path / "empty" / "pressure_drop_history.txt").read_text() == (
+        "Iter Core_Total(Pa) Full_Total(Pa) Core_Static(Pa) Full_Static(Pa)\n")
+    h = np.zeros((2, 8))
+    h[:, 0], h[:, 1], h[:, 2] = [1e-3, 2e-4], [5e-4, 1.5e-5], [0.25, 1.0 / 3.0]
+    exportfiles.save_logs(str(tmp_path / "nodp"), h, iter0=7, cfl0=0.5)
+    assert (tmp_path / "nodp" / "residuals.txt").read_text().splitlines()[1:] == [
+        "7 0.25 0.001 0.0005 0 0 0.5", "8 0.333333 0.0002 1.5e-05 0 0 0.5"]
+    assert (tmp_path / "nodp" / "pressure_drop_history.txt").read_text().splitlines()[1:] == ["7 0 0 0 0", "8 0 0 0 0"]
+    lib = cps.load_library()
+    assert lib.cps_save_logs(None, 0, 0, None, None, None, 0.0) == cps.CPS_ERR_ARG
+    assert lib.cps_save_logs(str(tmp_path).encode(), 3, 0, None, None, None, 0.0) == cps.CPS_ERR_ARG
