@@ -204,18 +204,20 @@ def host_cores() -> int:
         return os.cpu_count() or 1
 
 
-def reference_solve(design, threads: int, est_iters: int, chunks: int, time_cap: float) -> dict:
-    """The reference's own FP64 build (oracle/_ref/ref_f64) solving ``design``
-    from the zero state to the 1e-6 stop, in ``chunks`` calls that carry the
-    state (u, v, p); its own timer around the calculateStep loop is summed.
-    A solve still running after ``time_cap`` seconds is extrapolated to
-    ``est_iters`` outer iterations."""
+def reference_solve(design, threads: int, est_iters: int, chunks: int, time_cap: float,
+                    precision: str = "f64") -> dict:
+    """The reference's own build (oracle/_ref/ref_f64: promoted to FP64, the
+    default; ref_f32: as shipped) solving ``design`` from the zero state to
+    the 1e-6 stop, in ``chunks`` calls that carry the state (u, v, p); its own
+    timer around the calculateStep loop is summed.  A solve still running
+    after ``time_cap`` seconds is extrapolated to ``est_iters`` outer
+    iterations."""
     from oracle import reference
     chunk = max(100, -(-int(1.3 * est_iters) // max(1, chunks)))
     state, total_s, done, n_chunks, converged, per_chunk_ms = None, 0.0, 0, 0, False, []
     t0 = time.perf_counter()
     while not converged and done < MAX_OUTER and time.perf_counter() - t0 < time_cap:
-        out = reference.run(design, chunk, precision="f64", eps=EPS, stop_on_conv=True, threads=threads,
+        out = reference.run(design, chunk, precision=precision, eps=EPS, stop_on_conv=True, threads=threads,
                             init=state, timeout=time_cap + 600)
         total_s += float(out["elapsed"][0])
         per_chunk_ms.append(1e3 * float(out["elapsed"][0]))
@@ -233,6 +235,19 @@ def reference_solve(design, threads: int, est_iters: int, chunks: int, time_cap:
                   f"{est_iters} iterations")
     return {"value": value, "sample": sample, "iters": done, "converged": converged, "chunks": n_chunks,
             "ms_per_chunk": float(np.mean(per_chunk_ms)), "ms_per_outer_iteration": 1e3 * total_s / max(1, done)}
+
+
+def as_shipped_fp32(design, threads: int, est_iters: int, time_cap: float):
+    """The reference as shipped (FP32 throughout, oracle/_ref/ref_f32) on the
+    same workload, reported beside the FP64 figure: the FP64 build is the one
+    this library's FP64 arithmetic is compared with; this one is what the
+    reference's users run today.  None when the binary is absent."""
+    from oracle import reference
+    if not reference.available("f32"):
+        return None
+    r = reference_solve(design, threads, est_iters, 2, time_cap, precision="f32")
+    return {"value": r["value"], "unit": "solves/s", "cores": threads, "outer_iterations": r["iters"],
+            "converged": r["converged"], "ms_per_outer_iteration": r["ms_per_outer_iteration"], "sample": r["sample"]}
 
 
 def cpu_baseline(design, iters_per_solve: int, starts, sample_iters: int, threads: int) -> dict:
@@ -343,7 +358,11 @@ def run_b200(args) -> None:
             # the reference's own solve to its own stop, bounded by --cpu-time-cap
             r = reference_solve(design, host_cores(), cpu_iters, 4, args.cpu_time_cap)
             cpu = {"value": r["value"], "unit": "solves/s", "cores": host_cores(), "kind": "reference",
+                   "precision": "f64 (the reference's sources promoted to double)",
                    "ms_per_outer_iteration": r["ms_per_outer_iteration"], "sample": r["sample"]}
+            shipped = as_shipped_fp32(design, host_cores(), cpu_iters, args.cpu_time_cap)
+            if shipped is not None:
+                cpu["as_shipped_fp32"] = shipped
         else:  # the oracle port on samples along the trajectory when the reference binary is absent
             starts = [None]
             for frac in (0.25, 0.5, 0.75):
@@ -557,6 +576,7 @@ def run_reference(args) -> None:
         reference.run(design, 10, precision="f64", threads=threads)
     r = reference_solve(design, threads, REFERENCE_ITERS.get(args.workload, 20000), args.steps, args.ref_time_cap)
     value, sample, done, chunks = r["value"], r["sample"], r["iters"], r["chunks"]
+    shipped = as_shipped_fp32(design, threads, REFERENCE_ITERS.get(args.workload, 20000), args.ref_time_cap)
     print(json.dumps({
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": chunks,
         "warmup": args.warmup, "ms_per_step": r["ms_per_chunk"], "higher_is_better": True,
@@ -564,7 +584,9 @@ def run_reference(args) -> None:
         "impl": "reference",
         "config": dict(cfg, outer_iterations_per_solve=done, converged=r["converged"],
                        ms_per_outer_iteration=r["ms_per_outer_iteration"]),
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "reference", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "reference", "sample": sample,
+                         "precision": "f64 (the reference's sources promoted to double)",
+                         **({"as_shipped_fp32": shipped} if shipped is not None else {})},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
