@@ -39,7 +39,10 @@ and --impl reference prints an unavailable line.
 same workload: the whole solve to the 1e-6 stop, run in --steps chunks that
 carry the state (u, v, p) from one chunk to the next; a solve that exceeds
 --ref-time-cap seconds is extrapolated with the reference's converged
-iteration count.
+iteration count.  Both arms also report, under cpu_baseline.as_shipped_fp32,
+the reference as shipped (FP32 throughout, oracle/_ref/ref_f32) solving the
+same design the same way; the FP64 build stays the reported value because
+this library computes in FP64.
 """
 from __future__ import annotations
 
