@@ -115,15 +115,18 @@ class ThermalCase:
                   **params) -> "ThermalCase":
         """The thermal inputs of a flow result: the cell-centred velocities
         of saveAll's thermal crop (output.cpp:87-103, 146-171) and the crop of
-        the design's gamma; H_t = the design's channel height when it has one."""
+        the design's gamma; H_t = the design's channel height when it has one.
+        The cell sizes are the thermal program's own, Params::dx() = (Nx dx)/Nx
+        (thermal_solver.cpp:723, 184), as it computes them from dx."""
         U, V = fields["u"], fields["v"]
         uC = 0.5 * (U[:-1, :] + U[1:, :])
         vC = 0.5 * (V[:, :-1] + V[:, 1:])
         lo, hi = N_in_buffer, design.N - N_out_buffer
         if "H_t" not in params and design.Ht_channel > 0:
             params["H_t"] = design.Ht_channel
-        return ThermalCase(gamma=design.gamma[:, lo:hi], u=uC[:, lo:hi], v=vC[:, lo:hi], dx=design.hx, dy=design.hy,
-                           q=q, **params)
+        nx, ny = hi - lo, design.M
+        return ThermalCase(gamma=design.gamma[:, lo:hi], u=uC[:, lo:hi], v=vC[:, lo:hi], dx=(nx * design.hx) / nx,
+                           dy=(ny * design.hy) / ny, q=q, **params)
 
 
 def _desc(case: ThermalCase) -> "cps.CpsThermalDesc":

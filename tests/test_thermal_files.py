@@ -80,3 +80,18 @@ def test_results_vtk_equals_the_reference_writer(tmp_path, seed, Ht):
     case = pt.ThermalCase(gamma=gamma, u=u, v=v, dx=ddx, dy=ddy, H_t=Ht)
     pt.save(str(tmp_path), case, T)
     assert (tmp_path / "thermal_results_3d.vtk").read_bytes() == ref["vtk"]
+
+
+def test_from_flow_crop_and_cell_sizes():
+    """from_flow: the thermal crop between the buffers, saveAll's cell-centred
+    velocities, and the thermal program's cell sizes (Nx dx)/Nx."""
+    from coldplate_solver_b200 import geometry
+    d = geometry.straight_channel(M=12, N=30, h=2.3e-5, band=(3, 9))
+    rng = np.random.default_rng(4)
+    f = {"u": rng.normal(size=(d.M + 1, d.N)), "v": rng.normal(size=(d.M, d.N + 1))}
+    c = pt.ThermalCase.from_flow(d, f, q=1e5, N_in_buffer=3, N_out_buffer=5)
+    assert (c.Nx, c.Ny) == (22, 12)
+    assert c.dx == (22 * d.hx) / 22 and c.dy == (12 * d.hy) / 12
+    np.testing.assert_array_equal(c.u, (0.5 * (f["u"][:-1, :] + f["u"][1:, :]))[:, 3:25])
+    np.testing.assert_array_equal(c.v, (0.5 * (f["v"][:, :-1] + f["v"][:, 1:]))[:, 3:25])
+    np.testing.assert_array_equal(c.gamma, d.gamma[:, 3:25])
