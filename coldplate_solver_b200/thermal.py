@@ -271,17 +271,23 @@ def energy_balance(case: ThermalCase, T: np.ndarray) -> Dict[str, float]:
            "T_fluid_max": float(T[fluid].max()) if fluid.any() else -1e30,
            "T_fin_min": float(T[fin].min()) if fin.any() else 1e30,
            "T_fin_max": float(T[fin].max()) if fin.any() else -1e30}
-    Q_in = float(np.sum(case.heat_flux() * case.dx * case.dy))
-    mdot = mdotT = 0.0
+    # The sums run in the reference's order, one term after another (cumsum),
+    # so that they round as its loops do.
+    terms = (case.heat_flux() * case.dx * case.dy).ravel()
+    Q_in = float(np.cumsum(terms)[-1]) if terms.size else 0.0
     dz_f = case.H_t / case.nz_fluid
+    flows, heats = [], []
     for k in range(nzs, Nz):
         z = (k - nzs + 0.5) * dz_f / case.H_t
         po = 4.0 * z * (1 - z)
         uu = case.u[:, -1] * po
         m = (case.gamma[:, -1] > 0.01) & (uu > 0)
         mflow = case.rho * uu[m] * (case.dy * dz_f)
-        mdot += float(mflow.sum())
-        mdotT += float((mflow * T[k, m, -1]).sum())
+        flows.append(mflow)
+        heats.append(mflow * T[k, m, -1])
+    flows, heats = np.concatenate(flows), np.concatenate(heats)
+    mdot = float(np.cumsum(flows)[-1]) if flows.size else 0.0
+    mdotT = float(np.cumsum(heats)[-1]) if heats.size else 0.0
     T_out = mdotT / mdot if mdot > 0 else case.T_inlet
     Q_out = mdot * case.Cp * (T_out - case.T_inlet)
     out.update(Q_in=Q_in, T_out=T_out, Q_out=Q_out, imbalance=100 * (Q_in - Q_out) / (Q_in + 1e-30))

@@ -233,8 +233,10 @@ def run_thermal_assembly(Nx: int, Ny: int, dx: float, dy: float, gamma: np.ndarr
     """The matrix (CSR) and right-hand side the reference's own
     ThermalSolver3D::solve assembles (harness oracle/thermal_asm_harness.cpp),
     with the reference's Params::dx() = (Nx dx) / Nx.  Given a temperature
-    field T (Nz, Ny, Nx), also the bytes of the thermal_results_3d.vtk the
-    reference's save_vtk writes for it ("vtk")."""
+    field T (Nz, Ny, Nx), the stand-in solve hands it back as the solution,
+    and the result also has the bytes of the thermal_results_3d.vtk the
+    reference's save_vtk writes for it ("vtk") and the text its solve printed
+    ("stdout": the temperature ranges and the energy balance)."""
     path = os.path.join(REF_DIR, "thermal_asm")
     if not os.access(path, os.X_OK):
         raise FileNotFoundError(f"{path} not built (make -C oracle ref)")
@@ -249,11 +251,12 @@ def run_thermal_assembly(Nx: int, Ny: int, dx: float, dy: float, gamma: np.ndarr
             "q0": np.ascontiguousarray(q0, dtype=np.float64).ravel(),
             **({} if T is None else {"T": np.ascontiguousarray(T, dtype=np.float64).ravel()})})
         env = dict(os.environ, OMP_NUM_THREADS="1")
-        proc = subprocess.run([path, cpath, opath], cwd=tmp, env=env, stdout=subprocess.DEVNULL,
+        proc = subprocess.run([path, cpath, opath], cwd=tmp, env=env, stdout=subprocess.PIPE,
                               stderr=subprocess.PIPE, timeout=timeout)
         if proc.returncode != 0:
             raise RuntimeError(f"thermal_asm failed: {proc.stderr.decode()[-2000:]}")
         out: Dict[str, object] = dict(casefile.read_records(opath))
+        out["stdout"] = proc.stdout.decode(errors="replace")
         if T is not None:
             with open(os.path.join(tmp, "thermal_results_3d.vtk"), "rb") as f:
                 out["vtk"] = f.read()

@@ -5,9 +5,13 @@
 // (oracle/_ref/thermal_src/, git-ignored) in which two mechanical edits are
 // made: the AMGCL #include lines are dropped, and the AMGCL set-up and solve
 // (:532-550) are replaced by one call that hands the assembled matrix and
-// right-hand side to this harness (the temperature is left at T_inlet).  Its
-// main() is renamed so that this file's main() drives it the way the
-// reference's main() does (:706-760).
+// right-hand side to this harness and stands in for the solve.  Its main() is
+// renamed so that this file's main() drives it the way the reference's main()
+// does (:706-760).  The temperature is left at T_inlet, or, given a record
+// "T" (Nz*Ny*Nx), set to that field by the stand-in solve, so that solve()
+// prints the reference's temperature ranges and energy balance for it
+// (:567-619); the harness then runs the reference's save_vtk (:622-662),
+// which writes thermal_results_3d.vtk to the working directory.
 //
 //   thermal_asm case.bin out.bin
 #include <cstdint>
@@ -21,7 +25,11 @@
 
 template <class Matrix>
 void harness_capture(const Matrix& A, const std::vector<double>& b);
-inline std::pair<int, double> harness_solve() { return {0, 0.0}; }
+std::vector<double> g_T;  // the field the stand-in solve returns (empty: T stays at T_inlet)
+inline std::pair<int, double> harness_solve(std::vector<double>& T) {
+  if (!g_T.empty()) T = g_T;
+  return {0, 0.0};
+}
 
 #define main reference_main
 #include "thermal_solver.cpp"
@@ -110,13 +118,13 @@ int main(int argc, char** argv) {
     s.u_xy = rec.at("u").d;
     s.v_xy = rec.at("v").d;
     s.q0 = rec.at("q0").d;
-    s.solve();
     auto t = rec.find("T");
     if (t != rec.end()) {
-      if (t->second.d.size() != s.T.size()) throw std::runtime_error("T record has the wrong size");
-      s.T = t->second.d;
-      s.save_vtk("thermal_results_3d.vtk");
+      if (t->second.d.size() != (size_t)p.n_dofs()) throw std::runtime_error("T record has the wrong size");
+      g_T = t->second.d;
     }
+    s.solve();
+    if (t != rec.end()) s.save_vtk("thermal_results_3d.vtk");
     FILE* o = std::fopen(argv[2], "wb");
     if (!o) throw std::runtime_error("cannot write output");
     put(o, "row_ptr", 'i', g_ptr.data(), (int64_t)g_ptr.size());

@@ -95,3 +95,35 @@ def test_from_flow_crop_and_cell_sizes():
     np.testing.assert_array_equal(c.u, (0.5 * (f["u"][:-1, :] + f["u"][1:, :]))[:, 3:25])
     np.testing.assert_array_equal(c.v, (0.5 * (f["v"][:, :-1] + f["v"][:, 1:]))[:, 3:25])
     np.testing.assert_array_equal(c.gamma, d.gamma[:, 3:25])
+
+
+def _printed_balance(text: str) -> dict:
+    import re
+    out = {}
+    for key, name in (("T_base", "T_base"), ("T_fin", "T_fin"), ("T_fluid", "T_fluid")):
+        a, b = re.search(rf"{key}:\s*\[([^,]+), ([^\]]+)\]", text).groups()
+        out[f"{name}_min"], out[f"{name}_max"] = a.strip(), b.strip()
+    for key, name in (("Q_in", "Q_in"), ("T_out", "T_out"), ("Q_out", "Q_out"), ("Imbalance", "imbalance")):
+        out[name] = re.search(rf"{key}\s*=\s*(\S+?)(?:%|\s)", text).group(1)
+    return out
+
+
+@pytest.mark.skipif(not os.access(os.path.join(reference.REF_DIR, "thermal_asm"), os.X_OK),
+                    reason="oracle/_ref/thermal_asm not built")
+@pytest.mark.parametrize("seed,Ht,nz", [(0, 5e-4, (2, 7)), (5, 3e-3, (3, 5)), (9, 8e-4, (1, 1))])
+def test_energy_balance_equals_the_reference_print(seed, Ht, nz):
+    """thermal.energy_balance against the ranges and energy balance the
+    reference's own solve prints (two decimals) for the same field."""
+    gamma, T, u, v = field(seed=seed)
+    Ny, Nx = gamma.shape
+    T = T[:1].repeat(nz[0] + nz[1], axis=0) + np.random.default_rng(seed).random((nz[0] + nz[1], Ny, Nx))
+    q0 = np.random.default_rng(seed + 1).uniform(1e9, 3e9, (Ny, Nx))
+    ref = reference.run_thermal_assembly(Nx, Ny, 2e-5, 2e-5, gamma, u, v, q0, nz_solid=nz[0], nz_fluid=nz[1],
+                                         H_t=Ht, T=T)
+    printed = _printed_balance(ref["stdout"])
+    dxy = [float(x) for x in ref["dxdy"]]
+    case = pt.ThermalCase(gamma=gamma, u=u, v=v, dx=dxy[0], dy=dxy[1], q0=q0, H_t=Ht, nz_solid=nz[0],
+                          nz_fluid=nz[1])
+    mine = pt.energy_balance(case, T)
+    for k, text in printed.items():
+        assert f"{mine[k]:.2f}" == text, (k, mine[k], text)
