@@ -127,3 +127,17 @@ def test_energy_balance_equals_the_reference_print(seed, Ht, nz):
     mine = pt.energy_balance(case, T)
     for k, text in printed.items():
         assert f"{mine[k]:.2f}" == text, (k, mine[k], text)
+
+
+def test_energy_balance_equals_the_oracle_loops():
+    """thermal.energy_balance (vectorised, sums in the reference's order) and
+    the oracle's per-cell loops give the same bits."""
+    from oracle import thermal as th
+    gamma, T, u, v = field(Nx=31, Ny=17, seed=3)
+    q0 = np.random.default_rng(2).uniform(1e5, 1e6, gamma.shape)
+    case = pt.ThermalCase(gamma=gamma, u=u, v=v, dx=2e-5, dy=2e-5, q0=q0, H_t=5e-4)
+    p = th.ThermalParams(Nx=case.Nx, Ny=case.Ny, dx=case.dx, dy=case.dy, H_t=case.H_t)
+    mine, ora = pt.energy_balance(case, T), th.energy_balance(p, gamma, u, q0, T)
+    for k in ("T_base_min", "T_base_max", "T_fluid_min", "T_fluid_max", "T_fin_min", "T_fin_max", "Q_in", "T_out",
+              "Q_out", "imbalance"):
+        assert mine[k] == ora[k], (k, mine[k], ora[k])
