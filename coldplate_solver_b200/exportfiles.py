@@ -75,6 +75,12 @@ def save_all(directory: str, M: int, N: int, hx: float, hy: float, fields: Dict[
                                cps.CPS_ROW_MAJOR))
 
 
+# cps_step_out (include/cps.h) as a NumPy record
+_STEP_OUT = np.dtype([("residU", "f8"), ("residV", "f8"), ("residMass", "f8"), ("residMassDof", "f8"), ("err", "f8"),
+                      ("pIters", "i4"), ("uSweeps", "i4"), ("vSweeps", "i4")], align=True)
+assert _STEP_OUT.itemsize == ctypes.sizeof(cps.CpsStepOut)
+
+
 def save_logs(directory: str, hist: np.ndarray, dp: Optional[np.ndarray] = None, cfl: Optional[np.ndarray] = None,
               cfl0: float = 0.1, iter0: int = 0) -> None:
     """runIterations' residuals.txt and pressure_drop_history.txt
@@ -86,12 +92,12 @@ def save_logs(directory: str, hist: np.ndarray, dp: Optional[np.ndarray] = None,
     os.makedirs(directory, exist_ok=True)
     h = np.asarray(hist, dtype=np.float64).reshape(-1, 8)
     n = h.shape[0]
-    rows = (cps.CpsStepOut * max(1, n))()
-    for k in range(n):
-        rows[k].residU, rows[k].residV, rows[k].residMass = float(h[k, 0]), float(h[k, 1]), float(h[k, 2])
+    rows = np.zeros(max(1, n), dtype=_STEP_OUT)  # cps_step_out[n]; only the three residuals are logged
+    rows["residU"][:n], rows["residV"][:n], rows["residMass"][:n] = h[:, 0], h[:, 1], h[:, 2]
     d = None if dp is None else np.ascontiguousarray(np.asarray(dp, dtype=np.float64).reshape(n, 4))
     c = None if cfl is None else np.ascontiguousarray(np.asarray(cfl, dtype=np.float64).reshape(n))
-    _check(_lib().cps_save_logs(directory.encode(), n, iter0, rows, cps._dptr(d), cps._dptr(c), cfl0))
+    _check(_lib().cps_save_logs(directory.encode(), n, iter0, rows.ctypes.data_as(ctypes.POINTER(cps.CpsStepOut)),
+                                cps._dptr(d), cps._dptr(c), cfl0))
 
 
 def design_from_export(directory: str, **overrides):
