@@ -2,15 +2,27 @@
 """Benchmark: converged SIMPLE solves per second on one B200 (and N GPUs).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload network|straight|density|mix|served|thermal] [--precision fp64|mixed]
+                    [--workload density|network|straight|mix|served|thermal] [--precision fp64|mixed]
 
 A step is one converged solve (outer residual max(residU, residV,
 residMassDof) <= 1e-6) of the workload's design(s), started from the zero
-state.  ``value`` is converged solves/s over all ranks with the inputs
-resident in HBM (device time from CUDA events on the library's stream, L2
-flushed between steps); ``e2e`` is the same metric through the public C ABI
-with host buffers: geometry and initial fields uploaded, the solve run, and
-u, v, p downloaded, every step (wall clock).
+state.  The default workload is the largest single-design configuration: the
+1000 x 500 density-field design (10 um, SOU, 2.5-D, RAMP Brinkman alpha).
+``value`` is converged solves/s over all ranks with the inputs resident in
+HBM (device time from CUDA events on the library's stream, L2 flushed between
+steps); ``e2e`` is the same metric through the public C ABI with host
+buffers: geometry and initial fields uploaded, the solve run, and u, v, p
+downloaded, every step (wall clock).
+
+``error_vs_fp64_oracle``: the solve's u, v, fluid-cell p and full dP against
+the reference's own FP64 fixed point of the same design (committed fixture,
+tests/golden/converged/), at the 1e-6 stop and again after the same solve is
+continued to the 1e-10 residual, beside the reference's own 1e-6 stop state
+against its fixed point.  ``cpu_baseline``: the reference's own build on the
+host cores, on a bounded sample of the solve (timed chunks from five states
+along the trajectory), extrapolated with a per-iteration cost model linear in
+the inner iteration counts.  With --precision mixed the line also carries the
+plain FP64 path on the same design (``vs_plain_fp64_gpu``).
 
 Multi-GPU (torchrun, one rank per GPU): every rank solves its own copy of the
 workload (independent designs, no collective on the data path; weak scaling);
@@ -38,11 +50,12 @@ and --impl reference prints an unavailable line.
 (oracle/_ref/ref_f64: its sources promoted to FP64, all host threads) on the
 same workload: the whole solve to the 1e-6 stop, run in --steps chunks that
 carry the state (u, v, p) from one chunk to the next; a solve that exceeds
---ref-time-cap seconds is extrapolated with the reference's converged
-iteration count.  Both arms also report, under cpu_baseline.as_shipped_fp32,
-the reference as shipped (FP32 throughout, oracle/_ref/ref_f32) solving the
-same design the same way; the FP64 build stays the reported value because
-this library computes in FP64.
+--ref-time-cap seconds runs its remaining iterations (to the reference's
+converged count) at the rate of its last chunk.  Both arms also report, under
+cpu_baseline.as_shipped_fp32, the reference as shipped (FP32 throughout,
+oracle/_ref/ref_f32) on the same design (the reference arm only when its FP64
+solve took under two minutes); the FP64 build stays the reported value
+because this library computes in FP64.
 """
 from __future__ import annotations
 
@@ -65,6 +78,11 @@ METRIC = "converged solves/s (1e-6 outer residual)"
 EPS = 1e-6
 MAX_OUTER = 200000
 L2_FLUSH_BYTES = 512 << 20  # > 126 MB L2
+
+
+# The reference's own FP64 fixed point of each workload's design, from
+# tests/golden/make_converged.py (committed fixtures).
+ORACLE_FIXTURES = {"network": "network_500x250", "density": "density_1000x500"}
 
 
 def workload(name: str):
@@ -97,6 +115,56 @@ def algorithmic_bytes(design, hist: np.ndarray, s: int = 8) -> float:
     kp = np.where(hist[:, 5] < design.maxPressureIter, hist[:, 5] + 1, design.maxPressureIter)
     per = 6 * (nU + nV) + 6 * (ku * nU + kv * nV) + 3 * nP + 12 * kp * nP + 9 * MN
     return float(s * per.sum())
+
+
+# ---------------------------------------------------------------------------
+# error against the FP64 oracle's fixed point
+# ---------------------------------------------------------------------------
+def oracle_fixture(name):
+    """The committed fixed point of the reference's FP64 solve of a design
+    (tests/golden/converged/<name>.npz), or None."""
+    path = os.path.join(REPO, "tests", "golden", "converged", f"{name}.npz")
+    return np.load(path) if name and os.path.exists(path) else None
+
+
+def fluid_mask_p(design) -> np.ndarray:
+    mask = np.zeros((design.M + 1, design.N + 1), dtype=bool)
+    mask[1:design.M, 1:design.N] = design.gamma[:design.M - 1, :design.N - 1] > 0.5
+    return mask
+
+
+def errors_vs_fixture(design, fields, dp: float, fx) -> dict:
+    """Relative L2 of u, v and fluid-cell p and relative full dP against the
+    fixture's fixed point (on the fixture's every stride-th row and column)."""
+    st = int(fx["stride"])
+
+    def rel(a, b):
+        nb = float(np.linalg.norm(b))
+        return float(np.linalg.norm(a - b)) / nb if nb > 0 else float(np.linalg.norm(a - b))
+    mask = fluid_mask_p(design)[::st, ::st]
+    out = {k: rel(fields[k][::st, ::st], fx[k].astype(np.float64)) for k in ("u", "v")}
+    out["p"] = rel(fields["p"][::st, ::st][mask], fx["p"].astype(np.float64)[mask])
+    out["dP"] = abs(dp - float(fx["dp_full"])) / abs(float(fx["dp_full"]))
+    return out
+
+
+def oracle_error_block(solver, design, fx, fixture: str, eps_fixed: float = 1e-10, max_outer: int = 400000) -> dict:
+    """error_vs_fp64_oracle of a solver left at its 1e-6 stop: its fields
+    against the reference's FP64 fixed point; then the same solve continued to
+    the 1e-10 residual and compared again; beside them the reference's own
+    1e-6 stop state against its fixed point."""
+    f = solver.download()
+    at_stop = errors_vs_fixture(design, f, solver.full_dp(), fx)
+    h = solver.solve(max_outer, eps=eps_fixed)
+    f = solver.download()
+    at_fixed = errors_vs_fixture(design, f, solver.full_dp(), fx)
+    return {"at_1e-6_stop": at_stop, "at_1e-10": dict(at_fixed, outer_iterations_after_stop=int(len(h))),
+            "reference_own_1e-6_stop": {"u": float(fx["stop_err_u"]), "v": float(fx["stop_err_v"]),
+                                        "p": float(fx["stop_err_p"]), "dP": float(fx["stop_err_dp"])},
+            "oracle": "the reference's own FP64 solve (its sources promoted to double) run to the 1e-10 "
+                      f"residual: tests/golden/converged/{fixture}.npz",
+            "note": "relative L2 on u, v and fluid-cell p, relative full dP; any run stopped at 1e-6 sits about "
+                    "as far from the fixed point as the reference's own 1e-6 stop does"}
 
 
 # ---------------------------------------------------------------------------
@@ -214,10 +282,12 @@ def reference_solve(design, threads: int, est_iters: int, chunks: int, time_cap:
     the 1e-6 stop, in ``chunks`` calls that carry the state (u, v, p); its own
     timer around the calculateStep loop is summed.  A solve still running
     after ``time_cap`` seconds is extrapolated to ``est_iters`` outer
-    iterations."""
+    iterations: the remaining ones at the rate of its last chunk (the
+    latest, cheapest part of the trajectory it reached)."""
     from oracle import reference
     chunk = max(100, -(-int(1.3 * est_iters) // max(1, chunks)))
     state, total_s, done, n_chunks, converged, per_chunk_ms = None, 0.0, 0, 0, False, []
+    last_rate = 0.0
     t0 = time.perf_counter()
     while not converged and done < MAX_OUTER and time.perf_counter() - t0 < time_cap:
         out = reference.run(design, chunk, precision=precision, eps=EPS, stop_on_conv=True, threads=threads,
@@ -225,6 +295,7 @@ def reference_solve(design, threads: int, est_iters: int, chunks: int, time_cap:
         total_s += float(out["elapsed"][0])
         per_chunk_ms.append(1e3 * float(out["elapsed"][0]))
         done += len(out["err"])
+        last_rate = float(out["elapsed"][0]) / max(1, len(out["err"]))
         n_chunks += 1
         converged = bool(max(out["residU"][-1], out["residV"][-1], out["residMassDof"][-1]) <= EPS)
         state = {k: out[k] for k in ("u", "v", "p")}
@@ -233,11 +304,14 @@ def reference_solve(design, threads: int, est_iters: int, chunks: int, time_cap:
         sample = (f"the whole solve from the zero state to the 1e-6 stop ({done} outer iterations) in {n_chunks} "
                   f"chunks of <= {chunk} iterations carrying the state")
     else:
-        value = done / total_s / est_iters
-        sample = (f"{done} outer iterations from the zero state (time cap {time_cap:.0f} s) extrapolated to "
-                  f"{est_iters} iterations")
+        est = total_s + max(0, est_iters - done) * last_rate
+        value = 1.0 / est
+        sample = (f"{done} outer iterations from the zero state (time cap {time_cap:.0f} s), the remaining "
+                  f"{max(0, est_iters - done)} of the reference's {est_iters} to the 1e-6 stop at the rate of the "
+                  f"last chunk ({1e3 * last_rate:.2f} ms per outer iteration)")
     return {"value": value, "sample": sample, "iters": done, "converged": converged, "chunks": n_chunks,
-            "ms_per_chunk": float(np.mean(per_chunk_ms)), "ms_per_outer_iteration": 1e3 * total_s / max(1, done)}
+            "ms_per_chunk": float(np.mean(per_chunk_ms)), "ms_per_outer_iteration": 1e3 * total_s / max(1, done),
+            "seconds": total_s}
 
 
 def as_shipped_fp32(design, threads: int, est_iters: int, time_cap: float):
@@ -253,33 +327,85 @@ def as_shipped_fp32(design, threads: int, est_iters: int, time_cap: float):
             "converged": r["converged"], "ms_per_outer_iteration": r["ms_per_outer_iteration"], "sample": r["sample"]}
 
 
-def cpu_baseline(design, iters_per_solve: int, starts, sample_iters: int, threads: int) -> dict:
-    """Time the reference's calculateStep loop on ``sample_iters`` outer
-    iterations from each start state; extrapolate converged solves/s."""
+def cpu_baseline(design, hist: np.ndarray, starts, threads: int, chunk_s: float = 3.0, chunks: int = 2,
+                 precision: str = "f64") -> dict:
+    """The reference's own build (oracle/_ref/ref_f64; ref_f32 with
+    precision "f32") on a bounded sample of the solve, extrapolated to the
+    whole solve with a per-iteration cost model.
+
+    Sample: from each state of ``starts`` (the zero state and states along
+    this design's trajectory) the reference runs ``chunks`` consecutive chunks
+    of about ``chunk_s`` seconds each (a 2-iteration probe sizes them),
+    carrying its state; its own timer gives each chunk's time and its records
+    the chunk's inner iteration counts.  Model: one outer iteration costs
+    c0 + c1 (pIters + 1) + c2 (uSweeps + vSweeps), fitted by non-negative least
+    squares over the chunks.  The whole solve's time is the model summed over
+    ``hist``, the inner counts of the solve being timed (this library's FP64
+    solve of the same design: the reference's arithmetic, so its counts are the
+    reference's up to the order of the grid-wide sums)."""
+    from scipy.optimize import nnls
+
     from oracle import reference
-    kind = "reference"
-    per_it = []
-    if reference.available("f64"):
-        for st in starts:
-            out = reference.run(design, sample_iters, precision="f64", threads=threads, init=st)
-            per_it.append(float(out["elapsed"][0]) / len(out["err"]))
-    else:  # the oracle restatement (single thread) when the reference binary is absent
-        from oracle import restatement as rs
-        kind, threads = "port", 1
-        for st in starts:
-            f = rs.new_fields(design)
-            if st is not None:
-                for k in ("u", "v", "p"):
-                    f[k][...] = st[k]
-            t = time.perf_counter()
-            rs.solve(design, f, sample_iters, stop_on_conv=False)
-            per_it.append((time.perf_counter() - t) / sample_iters)
-    s_per_it = float(np.mean(per_it))
-    return {"value": 1.0 / (s_per_it * iters_per_solve), "unit": "solves/s", "cores": threads, "kind": kind,
-            "ms_per_outer_iteration": 1e3 * s_per_it,
-            "sample": f"{sample_iters} outer iterations from each of {len(starts)} states along the FP64 trajectory "
-                      f"of this design, extrapolated to a converged solve of {iters_per_solve} outer iterations "
-                      f"(the reference's own count for this workload where known)"}
+    if not reference.available(precision):
+        return None
+    rows, times, n_iters, t0 = [], [], 0, time.perf_counter()
+    for st in starts:
+        probe = reference.run(design, 2, precision=precision, threads=threads, init=st)
+        per = max(float(probe["elapsed"][0]) / 2, 1e-5)
+        n = int(max(2, min(20000, chunk_s / per)))
+        state = st
+        for _ in range(chunks):
+            out = reference.run(design, n, precision=precision, threads=threads, init=state)
+            k = len(out["err"])
+            rows.append([k, float(np.sum(out["pIters"] + 1)), float(np.sum(out["uSweeps"] + out["vSweeps"]))])
+            times.append(float(out["elapsed"][0]))
+            n_iters += k
+            state = {q: out[q] for q in ("u", "v", "p")}
+    A, t = np.array(rows), np.array(times)
+    coef, _ = nnls(A, t)
+    fit = A @ coef
+    T = float(coef[0] * len(hist) + coef[1] * np.sum(hist[:, 5] + 1) + coef[2] * np.sum(hist[:, 6] + hist[:, 7]))
+    return {"value": 1.0 / T, "unit": "solves/s", "cores": threads, "kind": "reference",
+            "precision": "f64 (the reference's sources promoted to double)" if precision == "f64"
+            else "f32 (the reference as shipped)",
+            "ms_per_outer_iteration": 1e3 * T / len(hist),
+            "model_ms": {"per_outer_iteration": 1e3 * coef[0], "per_pcg_iteration": 1e3 * coef[1],
+                         "per_jacobi_sweep": 1e3 * coef[2]},
+            "model_fit_rel_rms": float(np.sqrt(np.mean(((fit - t) / t) ** 2))),
+            "sample": (f"{n_iters} outer iterations of the reference in {len(times)} timed chunks of about "
+                       f"{chunk_s:.0f} s from {len(starts)} states along this design's trajectory "
+                       f"({time.perf_counter() - t0:.0f} s of wall time), extrapolated to the whole solve "
+                       f"({len(hist)} outer iterations) with a per-iteration cost model linear in the inner "
+                       f"iteration counts")}
+
+
+def port_baseline(design, hist: np.ndarray, starts, chunk_s: float = 3.0) -> dict:
+    """cpu_baseline's sample and cost model with the oracle's C restatement
+    (one thread) in place of the reference's build, when that is absent."""
+    from scipy.optimize import nnls
+
+    from oracle import restatement as rs
+    rows, times, n_iters = [], [], 0
+    for st in starts:
+        f = rs.new_fields(design)
+        if st is not None:
+            for k in ("u", "v", "p"):
+                f[k][...] = st[k]
+        t = time.perf_counter()
+        rs.solve(design, f, 2, stop_on_conv=False)
+        n = int(max(2, min(20000, chunk_s / max((time.perf_counter() - t) / 2, 1e-6))))
+        t = time.perf_counter()
+        hh = rs.solve(design, f, n, stop_on_conv=False)
+        times.append(time.perf_counter() - t)
+        rows.append([len(hh), float(np.sum(hh[:, 5] + 1)), float(np.sum(hh[:, 6] + hh[:, 7]))])
+        n_iters += len(hh)
+    coef, _ = nnls(np.array(rows), np.array(times))
+    T = float(coef[0] * len(hist) + coef[1] * np.sum(hist[:, 5] + 1) + coef[2] * np.sum(hist[:, 6] + hist[:, 7]))
+    return {"value": 1.0 / T, "unit": "solves/s", "cores": 1, "kind": "port",
+            "ms_per_outer_iteration": 1e3 * T / len(hist),
+            "sample": (f"{n_iters} outer iterations of the oracle's C restatement (one thread) from {len(starts)} "
+                       f"states along this design's trajectory, extrapolated to the whole solve with a "
+                       f"per-iteration cost model linear in the inner iteration counts")}
 
 
 # ---------------------------------------------------------------------------
@@ -352,28 +478,49 @@ def run_b200(args) -> None:
     e2e_s = max_over_ranks(time.perf_counter() - t0, world, local)
     barrier(world)
 
-    # ---- CPU baseline (rank 0, N = 1 only) ----
+    # ---- error against the FP64 oracle's fixed point (untimed) ----
+    oracle_err = None
+    fx = oracle_fixture(ORACLE_FIXTURES.get(args.workload))
+    if fx is not None:
+        solver.reset_fields()
+        solver.solve(args.max_outer, eps=EPS)
+        oracle_err = oracle_error_block(solver, design, fx, ORACLE_FIXTURES[args.workload])
+
+    # ---- the plain FP64 path on the same design, when this line is another precision ----
+    plain = None
+    if precision != cps.CPS_FP64:
+        with cps.Solver(design, precision=cps.CPS_FP64, device=device) as sp:
+            sp.reset_fields()
+            sp.solve(args.max_outer, eps=EPS)  # warm-up
+            ms_plain = []
+            for _ in range(max(1, min(args.steps, 5))):
+                sp.reset_fields()
+                sp.kernel_timing(reset=True)
+                hp = sp.solve(args.max_outer, eps=EPS)
+                ms_plain.append(sp.kernel_timing(reset=True)[0])
+            plain = {"value": 1e3 / float(np.mean(ms_plain)), "unit": "solves/s",
+                     "outer_iterations_per_solve": int(len(hp)),
+                     "speedup": value / (1e3 / float(np.mean(ms_plain)))}
+
+    # ---- CPU baseline (rank 0, N = 1 only): a bounded sample of the reference ----
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
-        from oracle import reference
-        cpu_iters = REFERENCE_ITERS.get(args.workload, iters_per_solve)
-        if reference.available("f64"):
-            # the reference's own solve to its own stop, bounded by --cpu-time-cap
-            r = reference_solve(design, host_cores(), cpu_iters, 4, args.cpu_time_cap)
-            cpu = {"value": r["value"], "unit": "solves/s", "cores": host_cores(), "kind": "reference",
-                   "precision": "f64 (the reference's sources promoted to double)",
-                   "ms_per_outer_iteration": r["ms_per_outer_iteration"], "sample": r["sample"]}
-            shipped = as_shipped_fp32(design, host_cores(), cpu_iters, args.cpu_time_cap)
+        starts = [None]
+        for frac in (0.2, 0.4, 0.6, 0.8):
+            solver.reset_fields()
+            solver.solve(max(1, int(frac * iters_per_solve)), eps=0.0)
+            f = solver.download()
+            starts.append({k: f[k] for k in ("u", "v", "p")})
+        cpu = cpu_baseline(design, h, starts, host_cores(), chunk_s=args.cpu_chunk_s)
+        if cpu is not None:
+            shipped = cpu_baseline(design, h, starts, host_cores(), chunk_s=args.cpu_chunk_s, chunks=1,
+                                   precision="f32")
             if shipped is not None:
+                shipped["note"] = ("the reference as shipped (FP32), extrapolated with this solve's FP64 inner "
+                                   "counts; its own FP32 trajectory differs")
                 cpu["as_shipped_fp32"] = shipped
-        else:  # the oracle port on samples along the trajectory when the reference binary is absent
-            starts = [None]
-            for frac in (0.25, 0.5, 0.75):
-                solver.reset_fields()
-                solver.solve(max(1, int(frac * iters_per_solve)), eps=0.0)
-                f = solver.download()
-                starts.append({k: f[k] for k in ("u", "v", "p")})
-            cpu = cpu_baseline(design, cpu_iters, starts, args.cpu_sample_iters, host_cores())
+        else:
+            cpu = port_baseline(design, h, starts)
 
     solver.close()
     if rank != 0:
@@ -410,6 +557,10 @@ def run_b200(args) -> None:
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
     }
+    if oracle_err is not None:
+        line["error_vs_fp64_oracle"] = oracle_err
+    if plain is not None:
+        line["vs_plain_fp64_gpu"] = plain
     if cpu is not None:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
@@ -572,14 +723,16 @@ def run_reference(args) -> None:
         return
     design, cfg = workload(args.workload)
     if not reference.available("f64"):
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_f64 is not built (make -C oracle ref)"}))
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_f64 is not built (make -C oracle ref REF=<reference checkout>)"}))
         return
     threads = host_cores()
     for _ in range(args.warmup):
         reference.run(design, 10, precision="f64", threads=threads)
     r = reference_solve(design, threads, REFERENCE_ITERS.get(args.workload, 20000), args.steps, args.ref_time_cap)
     value, sample, done, chunks = r["value"], r["sample"], r["iters"], r["chunks"]
-    shipped = as_shipped_fp32(design, threads, REFERENCE_ITERS.get(args.workload, 20000), args.ref_time_cap)
+    # the as-shipped FP32 build beside it, when the FP64 solve was short enough to repeat
+    shipped = (as_shipped_fp32(design, threads, REFERENCE_ITERS.get(args.workload, 20000), args.ref_time_cap)
+               if r["seconds"] < 120.0 else None)
     print(json.dumps({
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": chunks,
         "warmup": args.warmup, "ms_per_step": r["ms_per_chunk"], "higher_is_better": True,
@@ -781,13 +934,14 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="network", choices=["straight", "network", "density", "mix", "served", "thermal"])
+    ap.add_argument("--workload", default="density", choices=["straight", "network", "density", "mix", "served", "thermal"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--cpu-sample-iters", type=int, default=200,
-                    help="CPU baseline without the reference binary: oracle-port iterations per sampled state")
+    ap.add_argument("--cpu-chunk-s", type=float, default=3.0,
+                    help="CPU baseline: seconds per timed chunk of the reference (5 states x 2 chunks, FP64; "
+                         "5 x 1 more for the as-shipped FP32 build)")
     ap.add_argument("--cpu-time-cap", type=float, default=90.0,
-                    help="CPU baseline: seconds after which the reference's solve is extrapolated")
-    ap.add_argument("--ref-time-cap", type=float, default=600.0,
+                    help="thermal CPU baseline: seconds after which the port's solve is extrapolated")
+    ap.add_argument("--ref-time-cap", type=float, default=480.0,
                     help="reference arm: seconds after which an unfinished solve is extrapolated")
     ap.add_argument("--ref-design-cap", type=float, default=45.0,
                     help="reference arm, mix: seconds per design after which its solve is extrapolated")

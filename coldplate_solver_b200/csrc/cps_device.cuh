@@ -715,17 +715,22 @@ __device__ __forceinline__ double sou_correction(const DesignView& d, const X& x
   return Sdc;
 }
 
-// Momentum assembly at one unknown (momentum_solver.cpp:203-296) fused with
-// Jacobi sweep 1 (jacobi_solver.cpp:49-57, x0 = current velocity).  Returns the
-// squared residual of sweep 1 (0 when no sweep is run).
-//   FP64:  b = Sp, x1 = x0 + (b - A x0)/aP.
-//   mixed: b = r0 = Sp - A x0 (FP64 defect), delta1 = r0/aP (delta0 = 0).
-template <bool IsU, typename T, bool Pseudo>
-__device__ __forceinline__ double assemble_point(const DesignView& d, const LayoutA& L, int i, int j, bool sweep,
-                                                 double cfl) {
-  constexpr bool kMixed = sizeof(T) == 4;
-  const Inner<T>& w = inner<T>(d);
-  const int M = d.M, N = d.N, P = d.P;
+// The momentum row of one unknown (momentum_solver.cpp:203-296): the
+// coefficients of its unknown neighbours (negated; 0 where the neighbour is
+// not an unknown), the relaxed diagonal aP, the source Sp with the neighbours
+// that are not unknowns folded in at their current values, the current
+// velocity, and h / aP0 (dE for U, dN for V) in dOut.  Phase A and the
+// re-assembling sweep 2 both evaluate it from the same staged inputs, so they
+// get the same bits.
+struct MomRow {
+  double cE, cW, cN, cS, aP, Sp, velCur;
+  bool hasE, hasW, hasN, hasS;
+};
+
+template <bool IsU, bool Pseudo>
+__device__ __forceinline__ MomRow momentum_row(const DesignView& d, const LayoutA& L, int i, int j, double cfl,
+                                               double& dOut) {
+  const int M = d.M, N = d.N;
   const auto& u = L.u;
   const auto& v = L.v;
   const double mv = d.maxVel;
@@ -748,55 +753,109 @@ __device__ __forceinline__ double assemble_point(const DesignView& d, const Layo
   const double aN = d.Dn + maxd(0.0, -Fn), aS = d.Dn + maxd(0.0, Fs);
   const double sumA = aE + aW + aN + aS;
   const auto& X = IsU ? u : v;
-  const double velCur = X(i, j);
-  const double transCoeff = (Pseudo && d.pseudo) ? trans_implicit(d, cfl, velCur) : 0.0;
+  MomRow m;
+  m.velCur = X(i, j);
+  const double transCoeff = (Pseudo && d.pseudo) ? trans_implicit(d, cfl, m.velCur) : 0.0;
   const double brinkmanDrag = alphaLocal * d.vol;
   double aP0 = sumA + (Fe - Fw + Fn - Fs) + transCoeff + d.sinkDiag + brinkmanDrag;
   aP0 = maxd(aP0, 1e-10);
-  const double aP = aP0 / d.uvAlpha;
+  m.aP = aP0 / d.uvAlpha;
   double Sp = IsU ? (L.p(i, j) - L.p(i, j + 1)) * d.hy : (L.p(i, j) - L.p(i + 1, j)) * d.hx;
-  Sp += transCoeff * velCur;
-  Sp += d.relax * aP0 * velCur;
+  Sp += transCoeff * m.velCur;
+  Sp += d.relax * aP0 * m.velCur;
   if (d.conv == 1) Sp += sou_correction<IsU>(d, X, i, j, Fe, Fw, Fn, Fs);
-  if (IsU) AT(d.dE, i, j) = d.hy / aP0; else AT(d.dN, i, j) = d.hx / aP0;
+  dOut = (IsU ? d.hy : d.hx) / aP0;
   const int iHi = IsU ? M - 1 : M - 2, jHi = IsU ? N - 2 : N - 1;
-  const bool hasE = j + 1 <= jHi, hasW = j - 1 >= 1, hasN = i + 1 <= iHi, hasS = i - 1 >= 1;
-  const double xE = X(i, j + 1), xW = X(i, j - 1), xN = X(i + 1, j), xS = X(i - 1, j);
-  double cE = 0.0, cW = 0.0, cN = 0.0, cS = 0.0;
-  if (hasE) cE = -aE; else Sp += aE * xE;
-  if (hasW) cW = -aW; else Sp += aW * xW;
-  if (hasN) cN = -aN; else Sp += aN * xN;
-  if (hasS) cS = -aS; else Sp += aS * xS;
-  T* c = IsU ? w.cU : w.cV;
-  const long long ps = d.planeStride;
-  const size_t o = (size_t)i * P + j;
-  c[o] = (T)cE;
-  c[o + ps] = (T)cW;
-  c[o + 2 * ps] = (T)cN;
-  c[o + 3 * ps] = (T)cS;
-  c[o + 4 * ps] = (T)aP;
+  m.hasE = j + 1 <= jHi;
+  m.hasW = j - 1 >= 1;
+  m.hasN = i + 1 <= iHi;
+  m.hasS = i - 1 >= 1;
+  m.cE = m.cW = m.cN = m.cS = 0.0;
+  if (m.hasE) m.cE = -aE; else Sp += aE * X(i, j + 1);
+  if (m.hasW) m.cW = -aW; else Sp += aW * X(i, j - 1);
+  if (m.hasN) m.cN = -aN; else Sp += aN * X(i + 1, j);
+  if (m.hasS) m.cS = -aS; else Sp += aS * X(i - 1, j);
+  m.Sp = Sp;
+  return m;
+}
+
+// The row times the current velocities (sweep 1's x0), in the reference's CSR
+// order S, W, P, E, N (jacobi_solver.cpp:49-55).
+template <bool IsU>
+__device__ __forceinline__ double row_times_current(const MomRow& m, const LayoutA& L, int i, int j) {
+  const auto& X = IsU ? L.u : L.v;
   double Ax = 0.0;
-  if (hasS) Ax += cS * xS;
-  if (hasW) Ax += cW * xW;
-  Ax += aP * velCur;
-  if (hasE) Ax += cE * xE;
-  if (hasN) Ax += cN * xN;
-  const double r = Sp - Ax;
-  if (kMixed) {
-    (IsU ? w.bU : w.bV)[o] = (T)r;
-    if (!sweep) {
-      (IsU ? w.xU0 : w.xV0)[o] = (T)0.0;
-      return 0.0;
-    }
-    (IsU ? w.xU1 : w.xV1)[o] = (T)(r / aP);
-    return r * r;
-  }
-  (IsU ? w.bU : w.bV)[o] = (T)Sp;
+  if (m.hasS) Ax += m.cS * X(i - 1, j);
+  if (m.hasW) Ax += m.cW * X(i, j - 1);
+  Ax += m.aP * m.velCur;
+  if (m.hasE) Ax += m.cE * X(i, j + 1);
+  if (m.hasN) Ax += m.cN * X(i + 1, j);
+  return Ax;
+}
+
+// Momentum assembly at one unknown fused with Jacobi sweep 1
+// (jacobi_solver.cpp:49-57, x0 = current velocity).  Stores dE or dN and the
+// sweep's result; the row itself is not stored (a second sweep re-assembles
+// it).  Returns the squared residual of sweep 1 (0 when no sweep is run).
+//   FP64:  b = Sp, x1 = x0 + (b - A x0)/aP.
+//   mixed: b = r0 = Sp - A x0 (FP64 defect), delta1 = r0/aP (delta0 = 0).
+template <bool IsU, typename T, bool Pseudo>
+__device__ __forceinline__ double assemble_point(const DesignView& d, const LayoutA& L, int i, int j, bool sweep,
+                                                 double cfl) {
+  constexpr bool kMixed = sizeof(T) == 4;
+  const Inner<T>& w = inner<T>(d);
+  double dv;
+  const MomRow m = momentum_row<IsU, Pseudo>(d, L, i, j, cfl, dv);
+  const size_t o = (size_t)i * d.P + j;
+  (IsU ? d.dE : d.dN)[o] = dv;
   if (!sweep) {
-    (IsU ? w.xU0 : w.xV0)[o] = (T)velCur;
+    (IsU ? w.xU0 : w.xV0)[o] = kMixed ? (T)0.0 : (T)m.velCur;
     return 0.0;
   }
-  (IsU ? w.xU1 : w.xV1)[o] = (T)(velCur + r / aP);
+  const double r = m.Sp - row_times_current<IsU>(m, L, i, j);
+  if (kMixed) {
+    (IsU ? w.xU1 : w.xV1)[o] = (T)(r / m.aP);
+    return r * r;
+  }
+  (IsU ? w.xU1 : w.xV1)[o] = (T)(m.velCur + r / m.aP);
+  return r * r;
+}
+
+// Jacobi sweep 2 at one unknown (jacobi_solver.cpp:49-57) with the row
+// re-assembled from the staged inputs of phase A (the same bits phase A
+// computed), in the storage type T the later sweeps read: the row and its
+// source (FP64: b = Sp; mixed: b = r0) are stored for them when `store`.
+template <bool IsU, typename T, bool Pseudo>
+__device__ __forceinline__ double sweep2_point(const DesignView& d, const LayoutA& L, int i, int j, double cfl,
+                                               const T* __restrict__ xin, T* __restrict__ xout, bool store) {
+  constexpr bool kMixed = sizeof(T) == 4;
+  const Inner<T>& w = inner<T>(d);
+  const int P = d.P;
+  double dv;
+  const MomRow m = momentum_row<IsU, Pseudo>(d, L, i, j, cfl, dv);
+  const size_t o = (size_t)i * P + j;
+  const T cE = (T)m.cE, cW = (T)m.cW, cN = (T)m.cN, cS = (T)m.cS, aPt = (T)m.aP;
+  const T bt = kMixed ? (T)(m.Sp - row_times_current<IsU>(m, L, i, j)) : (T)m.Sp;
+  if (store) {
+    T* c = IsU ? w.cU : w.cV;
+    const long long ps = d.planeStride;
+    c[o] = cE;
+    c[o + ps] = cW;
+    c[o + 2 * ps] = cN;
+    c[o + 3 * ps] = cS;
+    c[o + 4 * ps] = aPt;
+    (IsU ? w.bU : w.bV)[o] = bt;
+  }
+  double Ax = 0.0;
+  if (m.hasS) Ax += (double)cS * (double)xin[o - P];
+  if (m.hasW) Ax += (double)cW * (double)xin[o - 1];
+  const double aP = (double)aPt;
+  const double x0 = (double)xin[o];
+  Ax += aP * x0;
+  if (m.hasE) Ax += (double)cE * (double)xin[o + 1];
+  if (m.hasN) Ax += (double)cN * (double)xin[o + P];
+  const double r = (double)bt - Ax;
+  xout[o] = (T)(x0 + r / aP);
   return r * r;
 }
 
@@ -1693,10 +1752,29 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
     T* xoutV = (k & 1) ? w.xV1 : w.xV0;
     double s[2] = {0.0, 0.0};
     const bool au = actU, av = actV;
-    for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
-      if (au && j <= N - 2) s[0] += sweep_point<true, T>(d, i, j, xinU, xoutU);
-      if (av && i <= M - 2) s[1] += sweep_point<false, T>(d, i, j, xinV, xoutV);
-    });
+    if (k == 2) {
+      // sweep 2 re-assembles the rows from phase A's staged inputs and stores
+      // them for the sweeps after it
+      const bool store = d.maxMomIter > 2;
+      for_each_tile<LayoutA>(
+          d, g.rank, g.nblk, tbuf,
+          [&](const LayoutA& L) {
+            L.u.stage(d.u, P, M);
+            L.v.stage(d.v, P, M);
+            L.p.stage(d.p, P, M);
+            L.a.stage(d.alpha, P, M - 1);
+          },
+          [&](const LayoutA& L, int i, int j, bool inside) {
+            if (!inside) return;
+            if (au && j <= N - 2) s[0] += sweep2_point<true, T, Pseudo>(d, L, i, j, cfl, xinU, xoutU, store);
+            if (av && i <= M - 2) s[1] += sweep2_point<false, T, Pseudo>(d, L, i, j, cfl, xinV, xoutV, store);
+          });
+    } else {
+      for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
+        if (au && j <= N - 2) s[0] += sweep_point<true, T>(d, i, j, xinU, xoutU);
+        if (av && i <= M - 2) s[1] += sweep_point<false, T>(d, i, j, xinV, xoutV);
+      });
+    }
     if (!g.template sync_reduce<2, 0u>(s, smem)) return -1;
     if (au) { kU = k; actU = !(s[0] < d.thrU) && kU < d.maxMomIter; }
     if (av) { kV = k; actV = !(s[1] < d.thrV) && kV < d.maxMomIter; }

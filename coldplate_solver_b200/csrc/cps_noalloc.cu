@@ -22,15 +22,19 @@
 //     each call clears what must start at zero (barrier, status, counters), and
 //     calls that overlap on the GPU (another stream, another host thread) race
 //     on it -- serialise them;
-//   * the first call on a device looks the array's device address up with
-//     cudaGetSymbolAddress (the name is only a host-side stand-in); make that
-//     first call before any stream capture.
+//   * the array's name is only a host-side stand-in, never a device address:
+//     every call looks the address up with cudaGetSymbolAddress in the
+//     calling thread's current context (an allocation-free lookup), so a
+//     call under a context of the caller's own, or after cudaDeviceReset,
+//     gets that context's copy of the array; the first call in a process
+//     also loads the kernel's module, so make it before any stream capture;
+//   * the call runs on the caller's stream only and synchronises that stream
+//     before it returns.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
-#include <mutex>
 #include <string>
 
 #include "../../include/cps.h"
@@ -50,10 +54,6 @@ constexpr size_t kScratchBytes = kPlanesBytes + kRingBytes + kHistBytes + kFlags
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_mutex;
-unsigned char* g_scratch_addr[kMaxDevices] = {};  // device address of g_noalloc_scratch per device
-int g_noalloc_ctas[kMaxDevices] = {};
 // Errors are returned as a status; the reason is printed to stderr on one line.
 cps_status fail(cps_status s, const std::string& m) {
   std::fprintf(stderr, "cps_solve_noalloc: %s\n", m.c_str());
@@ -100,30 +100,27 @@ extern "C" cps_status cps_solve_noalloc(const cps_desc* desc, int pitch, const d
     return fail(CPS_ERR_ARG, "every device buffer is required");
   if (max_outer == 0) return CPS_OK;
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return fail(CPS_ERR_CUDA, "no device");
+  if (cudaGetDevice(&dev) != cudaSuccess) return fail(CPS_ERR_CUDA, "no device");
+  // Set-up, with the caller's device current: the address of the static array
+  // in the current context (its host-side name is not a device address), and
+  // the co-resident CTAs of the cooperative launch.  None of these calls
+  // allocates.
   unsigned char* scratch = nullptr;
-  int ctas = 0;
   {
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_scratch_addr[dev]) {
-      // Once per device, with that device current: the address of the static
-      // array on this device (its host-side name is not a device address).
-      void* ptr = nullptr;
-      cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-      if (e != cudaSuccess) return fail(CPS_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-      int per_sm = 0, sms = 0;
-      e = cudaFuncSetAttribute((const void*)cps_noalloc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)cps::tile_smem_bytes<double>());
-      if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cps_noalloc_kernel, cps::kThreads,
-                                                          cps::tile_smem_bytes<double>());
-      if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      if (e != cudaSuccess || per_sm < 1) return fail(CPS_ERR_CUDA, "occupancy query failed");
-      g_noalloc_ctas[dev] = std::min(sms * per_sm, kNoAllocMaxCtas);
-      g_scratch_addr[dev] = static_cast<unsigned char*>(ptr);
-    }
-    scratch = g_scratch_addr[dev];
-    ctas = g_noalloc_ctas[dev];
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess) return fail(CPS_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    scratch = static_cast<unsigned char*>(ptr);
+  }
+  int per_sm = 0, sms = 0;
+  {
+    cudaError_t e = cudaFuncSetAttribute((const void*)cps_noalloc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)cps::tile_smem_bytes<double>());
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cps_noalloc_kernel, cps::kThreads,
+                                                        cps::tile_smem_bytes<double>());
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess || per_sm < 1) return fail(CPS_ERR_CUDA, "occupancy query failed");
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
 
@@ -170,10 +167,12 @@ extern "C" cps_status cps_solve_noalloc(const cps_desc* desc, int pitch, const d
   int* status = reinterpret_cast<int*>(flags + 64);
   int* done = status + 1;
 
+  // The grid cps_create picks for the same design: the fewest rounds of tiles
+  // per CTA the co-resident CTAs allow, spread evenly.
   const int tiles = ((d.M - 1 + cps::kTileI - 1) / cps::kTileI) * ((d.N - 1 + cps::kTileJ - 1) / cps::kTileJ);
-  int sms = 0;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int grid = std::max(1, std::min(std::min(ctas, std::max(1, sms)), std::max(1, (tiles + 1) / 2)));
+  const int cap = std::max(1, std::min(sms * per_sm, kNoAllocMaxCtas));
+  const int rounds = (tiles + cap - 1) / cap;
+  const int grid = std::max(1, std::min(std::min((tiles + rounds - 1) / rounds, cap), tiles));
 
   // The outputs the iteration writes only in part start from zero, as the
   // reference's fields do (SIMPLE.cpp:188-197); the shared scratch's barrier,
@@ -196,10 +195,11 @@ extern "C" cps_status cps_solve_noalloc(const cps_desc* desc, int pitch, const d
   const int nd = hflags[1];
   if (n_done) *n_done = nd;
   if (history && nd > 0) {
-    double h[128 * 8];  // host stack staging, 128 iterations per copy
+    double h[128 * 8];  // host stack staging, 128 iterations per copy, on the caller's stream
     for (int k0 = 0; k0 < nd; k0 += 128) {
       const int cnt = std::min(128, nd - k0);
-      e = cudaMemcpy(h, hist + (size_t)8 * k0, sizeof(double) * 8 * cnt, cudaMemcpyDeviceToHost);
+      e = cudaMemcpyAsync(h, hist + (size_t)8 * k0, sizeof(double) * 8 * cnt, cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
       if (e != cudaSuccess) return fail(CPS_ERR_CUDA, std::string("history copy: ") + cudaGetErrorString(e));
       for (int k = 0; k < cnt; ++k) {
         const double* r = h + 8 * k;

@@ -328,8 +328,14 @@ cps_status cps_get_history(cps_ctx* ctx, int n, cps_step_out* history);
  * until the process exits; designs need (M+1)*pitch <= 131072 elements or are
  * rejected with CPS_ERR_ARG (reason printed to stderr).  Every call on a device
  * shares that array: calls overlapping on the GPU race, so serialise them.
- * The first call on a device looks up the array's device address; make it
- * before any stream capture. */
+ * Each call looks the array's device address up in the calling thread's
+ * current context (an allocation-free lookup), so it works under whichever
+ * context the caller has made current; the first call in a process also
+ * loads the kernel's module, so make it before any stream capture.  Elements
+ * outside the logical matrices (the columns past each width, row M of the v
+ * plane) are never read and may hold anything.  The call works on `stream`
+ * only and synchronises it before returning; its grid is the one cps_create
+ * would pick for the same design. */
 cps_status cps_solve_noalloc(const cps_desc* desc, int pitch, const double* alpha, const double* gamma, double* u,
                              double* v, double* p, double* pStar, double* uStar, double* vStar, double* dE,
                              double* dN, double inletVelocity, int max_outer, double eps, cps_step_out* history,

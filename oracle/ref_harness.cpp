@@ -33,6 +33,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <optional>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -153,6 +154,78 @@ real mass_residual_dof(const SIMPLE& s) {
   return out;
 }
 
+// The physical constants of a case (SIMPLE.h:334-335, 240-244; SIMPLE.cpp:65-66).
+void configure_physics(SIMPLE& s, std::map<std::string, Record>& recs) {
+  s.hx = static_cast<real>(getd(recs, "hx"));
+  s.hy = static_cast<real>(getd(recs, "hy"));
+  s.rho = static_cast<real>(getd(recs, "rho"));
+  s.eta = static_cast<real>(getd(recs, "eta"));
+  s.brinkmanKMin = static_cast<real>(getd(recs, "kmin"));
+  s.brinkmanQ = static_cast<real>(getd(recs, "q"));
+  s.brinkmanAlphaMax = s.eta / std::max(s.brinkmanKMin, static_cast<real>(1e-20));  // SIMPLE.cpp:65-66
+}
+
+// The solver configuration of a case: the public members SIMPLE.h documents
+// (SIMPLE.h:68-358), set after construction as a driver would.
+void configure_solver(SIMPLE& s, std::map<std::string, Record>& recs) {
+  s.targetVel = static_cast<real>(getd(recs, "U_in"));
+  s.inletVelocity = s.targetVel;
+  s.convectionScheme = geti(recs, "conv");
+  s.enableTwoPointFiveD = geti(recs, "twoFiveD") != 0;
+  s.enableConvectionScaling = geti(recs, "convScale") != 0;
+  s.Ht_channel = static_cast<real>(getd(recs, "Ht"));
+  s.twoPointFiveDSinkMultiplier = static_cast<real>(getd(recs, "sinkMult"));
+  s.uvAlpha = static_cast<real>(getd(recs, "uvAlpha"));
+  s.pAlpha = static_cast<real>(getd(recs, "pAlpha"));
+  s.pTol = static_cast<real>(getd(recs, "pTol"));
+  s.maxPressureIter = geti(recs, "maxPIter");
+  s.momentumTol = static_cast<real>(getd(recs, "momTol"));
+  s.maxMomentumIter = geti(recs, "maxMomIter");
+  s.pressureSolverType = recs.count("solverType") ? geti(recs, "solverType") : 1;  // 1 = Parallel CG
+  s.momentumSolverType = recs.count("momType") ? geti(recs, "momType") : 1;  // iterations.cpp:109
+  s.enablePseudoTimeStepping = false; // SIMPLE.h:262 default
+  if (recs.count("pseudoI")) {
+    // The pseudo-transient term and its CFL controllers (SIMPLE.h:255-313), in the
+    // layout of oracle/simple_oracle_impl.h (ip[8..15], dp[11..27]).
+    const std::vector<int32_t>& pi = recs["pseudoI"].i;
+    const std::vector<double>& pd = recs["pseudoD"].d;
+    if (pi.size() != 8 || pd.size() != 17) throw std::runtime_error("bad pseudo records");
+    s.enablePseudoTimeStepping = pi[0] != 0;
+    s.useLocalPseudoTime = pi[1] != 0;
+    s.enableSER = pi[2] != 0;
+    s.enableLineSearch = pi[3] != 0;
+    s.enableCflRamp = pi[4] != 0;
+    s.serUseMaxResid = pi[5] != 0;
+    s.serMinIter = pi[6];
+    s.lsMaxTries = pi[7];
+    s.timeStepMultiplier = static_cast<real>(pd[0]);
+    s.minPseudoSpeed = static_cast<real>(pd[1]);
+    s.pseudoCFLInitial = static_cast<real>(pd[2]);
+    s.pseudoCFLMax = static_cast<real>(pd[3]);
+    s.cflRampStartRes = static_cast<real>(pd[4]);
+    s.cflRampExponent = static_cast<real>(pd[5]);
+    s.cflRampSmooth = static_cast<real>(pd[6]);
+    s.serCFLMin = static_cast<real>(pd[7]);
+    s.serCFLMax = static_cast<real>(pd[8]);
+    s.serSmooth = static_cast<real>(pd[9]);
+    s.serMaxIncrease = static_cast<real>(pd[10]);
+    s.serMaxDecrease = static_cast<real>(pd[11]);
+    s.lsAlphaMin = static_cast<real>(pd[12]);
+    s.lsAlphaReduce = static_cast<real>(pd[13]);
+    s.lsResidIncreaseTol = static_cast<real>(pd[14]);
+    // The constructor's set-up with these values (SIMPLE.cpp:68-82): the global
+    // pseudo time step from the domain length and the target velocity; the
+    // starting CFL number.
+    real domainLength = s.N * s.hx;
+    real velRef = std::max(s.targetVel, static_cast<real>(1e-6));
+    s.timeStep = s.timeStepMultiplier * domainLength / velRef;
+    s.pseudoCFL = static_cast<real>(pd[16]);
+    if (s.enableCflRamp) s.pseudoCFL = s.pseudoCFLInitial;
+  }
+  s.usePressureDropConvergence = false;
+  s.saveStateInterval = 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -163,7 +236,8 @@ int main(int argc, char** argv) {
   try {
     auto recs = read_records(argv[1]);
     const int M = geti(recs, "M"), N = geti(recs, "N");
-    const int mode = geti(recs, "mode");  // 0 = iterate, 1 = alpha from gamma, 2 = runIterations, 3 = files
+    const int mode = geti(recs, "mode");  // 0 = iterate, 1 = alpha from gamma, 2 = runIterations, 3 = files,
+                                          // 4 = a design loop in one process
     if (mode == 3) {
       // The reference's own file handling on files the caller put in ./ExportFiles:
       // the constructor reads fluid_params.txt and geometry_fluid.txt and builds
@@ -210,16 +284,72 @@ int main(int argc, char** argv) {
       }
       std::fclose(f);
     }
+    if (mode == 4) {
+      // A design loop in one process.  Object A runs maxOuter steps of design A
+      // (alpha, gamma) from the zero state and is destroyed; a new object B runs
+      // maxOuter steps of design B (alpha2, gamma2); then B's alpha and gamma
+      // are set in place to design A's and u, v, p to zero (a new design on the
+      // same object), and it runs maxOuter steps again.  Phase k writes its
+      // err and pressure iterations as errK/pItersK and its fields as uK/vK/pK
+      // (k = 1, 2, 3).  With the drop-in, the in-place edit is announced with
+      // b200Invalidate, as a maintainer's driver would.
+      const int maxOuter = geti(recs, "maxOuter");
+      Writer w(argv[2]);
+      auto phase = [&](SIMPLE& s, int k) {
+        std::vector<double> err;
+        std::vector<int32_t> pIt;
+        for (int it = 0; it < maxOuter; ++it) {
+          s.inletVelocity = s.targetVel;
+          int pi = 0;
+          err.push_back(static_cast<double>(s.calculateStep(pi)));
+          pIt.push_back(pi);
+        }
+#ifdef CPS_DROPIN
+        if (s.pressureSolverType >= 5) b200SyncFieldsToHost(s);
+#endif
+        const std::string n = std::to_string(k);
+        w.d(("err" + n).c_str(), err);
+        w.i(("pIters" + n).c_str(), pIt);
+        w.matrix(("u" + n).c_str(), s.u);
+        w.matrix(("v" + n).c_str(), s.v);
+        w.matrix(("p" + n).c_str(), s.p);
+      };
+      auto setup = [&](SIMPLE& s, const char* alphaKey, const char* gammaKey) {
+        omp_set_num_threads(geti(recs, "threads"));
+        configure_physics(s, recs);
+        configure_solver(s, recs);
+        load_grid(recs, alphaKey, s.alpha);
+        load_grid(recs, gammaKey, s.gamma);
+      };
+      // One storage for both objects, so that B is constructed at A's address
+      // (the drop-in must tell the new object from the old one).
+      std::optional<SIMPLE> obj;
+      obj.emplace();
+      setup(*obj, "alpha", "gamma");
+      phase(*obj, 1);
+      obj.reset();
+      obj.emplace();
+      SIMPLE& b = *obj;
+      setup(b, "alpha2", "gamma2");
+      phase(b, 2);
+      load_grid(recs, "alpha", b.alpha);
+      load_grid(recs, "gamma", b.gamma);
+      b.u.setZero();
+      b.v.setZero();
+      b.p.setZero();
+#ifdef CPS_DROPIN
+      b200Invalidate(b);
+#endif
+      phase(b, 3);
+#ifdef CPS_DROPIN
+      b200Release();
+#endif
+      return 0;
+    }
     SIMPLE s;
     omp_set_num_threads(geti(recs, "threads"));  // SIMPLE.cpp:89 forces numThreads=8
 
-    s.hx = static_cast<real>(getd(recs, "hx"));
-    s.hy = static_cast<real>(getd(recs, "hy"));
-    s.rho = static_cast<real>(getd(recs, "rho"));
-    s.eta = static_cast<real>(getd(recs, "eta"));
-    s.brinkmanKMin = static_cast<real>(getd(recs, "kmin"));
-    s.brinkmanQ = static_cast<real>(getd(recs, "q"));
-    s.brinkmanAlphaMax = s.eta / std::max(s.brinkmanKMin, static_cast<real>(1e-20));  // SIMPLE.cpp:65-66
+    configure_physics(s, recs);
 
     Writer w(argv[2]);
     if (mode == 1) {
@@ -230,62 +360,7 @@ int main(int argc, char** argv) {
       return 0;
     }
 
-    s.targetVel = static_cast<real>(getd(recs, "U_in"));
-    s.inletVelocity = s.targetVel;
-    s.convectionScheme = geti(recs, "conv");
-    s.enableTwoPointFiveD = geti(recs, "twoFiveD") != 0;
-    s.enableConvectionScaling = geti(recs, "convScale") != 0;
-    s.Ht_channel = static_cast<real>(getd(recs, "Ht"));
-    s.twoPointFiveDSinkMultiplier = static_cast<real>(getd(recs, "sinkMult"));
-    s.uvAlpha = static_cast<real>(getd(recs, "uvAlpha"));
-    s.pAlpha = static_cast<real>(getd(recs, "pAlpha"));
-    s.pTol = static_cast<real>(getd(recs, "pTol"));
-    s.maxPressureIter = geti(recs, "maxPIter");
-    s.momentumTol = static_cast<real>(getd(recs, "momTol"));
-    s.maxMomentumIter = geti(recs, "maxMomIter");
-    s.pressureSolverType = recs.count("solverType") ? geti(recs, "solverType") : 1;  // 1 = Parallel CG
-    s.momentumSolverType = recs.count("momType") ? geti(recs, "momType") : 1;  // iterations.cpp:109
-    s.enablePseudoTimeStepping = false; // SIMPLE.h:262 default
-    if (recs.count("pseudoI")) {
-      // The pseudo-transient term and its CFL controllers (SIMPLE.h:255-313), in the
-      // layout of oracle/simple_oracle_impl.h (ip[8..15], dp[11..27]).
-      const std::vector<int32_t>& pi = recs["pseudoI"].i;
-      const std::vector<double>& pd = recs["pseudoD"].d;
-      if (pi.size() != 8 || pd.size() != 17) throw std::runtime_error("bad pseudo records");
-      s.enablePseudoTimeStepping = pi[0] != 0;
-      s.useLocalPseudoTime = pi[1] != 0;
-      s.enableSER = pi[2] != 0;
-      s.enableLineSearch = pi[3] != 0;
-      s.enableCflRamp = pi[4] != 0;
-      s.serUseMaxResid = pi[5] != 0;
-      s.serMinIter = pi[6];
-      s.lsMaxTries = pi[7];
-      s.timeStepMultiplier = static_cast<real>(pd[0]);
-      s.minPseudoSpeed = static_cast<real>(pd[1]);
-      s.pseudoCFLInitial = static_cast<real>(pd[2]);
-      s.pseudoCFLMax = static_cast<real>(pd[3]);
-      s.cflRampStartRes = static_cast<real>(pd[4]);
-      s.cflRampExponent = static_cast<real>(pd[5]);
-      s.cflRampSmooth = static_cast<real>(pd[6]);
-      s.serCFLMin = static_cast<real>(pd[7]);
-      s.serCFLMax = static_cast<real>(pd[8]);
-      s.serSmooth = static_cast<real>(pd[9]);
-      s.serMaxIncrease = static_cast<real>(pd[10]);
-      s.serMaxDecrease = static_cast<real>(pd[11]);
-      s.lsAlphaMin = static_cast<real>(pd[12]);
-      s.lsAlphaReduce = static_cast<real>(pd[13]);
-      s.lsResidIncreaseTol = static_cast<real>(pd[14]);
-      // The constructor's set-up with these values (SIMPLE.cpp:68-82): the global
-      // pseudo time step from the domain length and the target velocity; the
-      // starting CFL number.
-      real domainLength = s.N * s.hx;
-      real velRef = std::max(s.targetVel, static_cast<real>(1e-6));
-      s.timeStep = s.timeStepMultiplier * domainLength / velRef;
-      s.pseudoCFL = static_cast<real>(pd[16]);
-      if (s.enableCflRamp) s.pseudoCFL = s.pseudoCFLInitial;
-    }
-    s.usePressureDropConvergence = false;
-    s.saveStateInterval = 0;
+    configure_solver(s, recs);
 
     load_grid(recs, "alpha", s.alpha);
     load_grid(recs, "gamma", s.gamma);
@@ -360,7 +435,7 @@ int main(int argc, char** argv) {
       hCfl.push_back(s.pseudoCFL);
       hSer.insert(hSer.end(), {(double)s.serResidPrev, (double)s.lsCurrentAlpha, (double)s.lsBacktrackCount});
 #ifdef CPS_DROPIN
-      if (s.pressureSolverType == 5) b200SyncFieldsToHost(s);  // uStar/vStar for the residual below
+      if (s.pressureSolverType >= 5) b200SyncFieldsToHost(s);  // uStar/vStar for the residual below
 #endif
       real massDof = mass_residual_dof(s);
       hU.push_back(s.residU);
@@ -375,7 +450,7 @@ int main(int argc, char** argv) {
       if (stopOnConv && conv <= eps) break;
     }
 #ifdef CPS_DROPIN
-    if (s.pressureSolverType == 5) b200SyncFieldsToHost(s);  // fields live on the GPU between steps
+    if (s.pressureSolverType >= 5) b200SyncFieldsToHost(s);  // fields live on the GPU between steps
 #endif
     w.d("residU", hU);
     w.d("residV", hV);

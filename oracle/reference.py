@@ -59,16 +59,19 @@ def case_records(design, max_outer: int, eps: float = 1e-6, stop_on_conv: bool =
 
 
 def run(design, max_outer: int, precision: str = "f64", eps: float = 1e-6, stop_on_conv: bool = False,
-        threads: int = 1, init: Optional[Dict[str, np.ndarray]] = None, timeout: float = 3600) -> Dict[str, np.ndarray]:
+        threads: int = 1, init: Optional[Dict[str, np.ndarray]] = None, timeout: float = 3600,
+        solver_type: int = 5) -> Dict[str, np.ndarray]:
     """Run the reference's calculateStep loop on ``design``; fields come back
-    reshaped to the reference's shapes."""
+    reshaped to the reference's shapes.  With precision "dropin" the steps
+    run through the B200 drop-in (pressureSolverType = ``solver_type``: 5
+    FP64, 6 mixed precision)."""
     if not available(precision):
-        raise FileNotFoundError(f"{binary(precision)} not built (make -C oracle ref)")
+        raise FileNotFoundError(f"{binary(precision)} not built (make -C oracle ref REF=<reference checkout>)")
     with tempfile.TemporaryDirectory(prefix="cps_ref_") as tmp:
         cpath, opath = os.path.join(tmp, "case.bin"), os.path.join(tmp, "out.bin")
         rec = case_records(design, max_outer, eps, stop_on_conv, threads, init)
         if precision == "dropin":
-            rec["solverType"] = [5]
+            rec["solverType"] = [int(solver_type)]
         casefile.write_records(cpath, rec)
         env = dict(os.environ, OMP_NUM_THREADS=str(threads))
         proc = subprocess.run([binary(precision), cpath, opath], cwd=tmp, env=env, stdout=subprocess.DEVNULL,
@@ -82,6 +85,41 @@ def run(design, max_outer: int, precision: str = "f64", eps: float = 1e-6, stop_
     for k, s in shapes.items():
         out[k] = out[k].reshape(s)
     out["planes"] = out["planes"].reshape(4, 6)
+    return out
+
+
+def run_design_loop(design_a, design_b, n: int, precision: str = "f64", threads: int = 1,
+                    solver_type: int = 5, timeout: float = 3600) -> Dict[str, np.ndarray]:
+    """Harness mode 4, a design loop in one process: a SIMPLE object runs ``n``
+    steps of ``design_a`` from the zero state and is destroyed; a new object,
+    constructed in the same storage, runs ``n`` steps of ``design_b``; then its
+    alpha and gamma are set to ``design_a``'s and u, v, p to zero in place, and
+    it runs ``n`` steps again.  The two designs share the grid and solver
+    settings of ``design_a``.  Returns errK, pItersK, uK, vK, pK for the phases
+    K = 1, 2, 3.  With precision "dropin" the steps run through the B200
+    drop-in (pressureSolverType = ``solver_type``: 5 FP64, 6 mixed)."""
+    if not available(precision):
+        raise FileNotFoundError(f"{binary(precision)} not built (make -C oracle ref REF=<reference checkout>)")
+    if (design_a.M, design_a.N) != (design_b.M, design_b.N):
+        raise ValueError("the two designs must share the grid")
+    with tempfile.TemporaryDirectory(prefix="cps_ref_") as tmp:
+        cpath, opath = os.path.join(tmp, "case.bin"), os.path.join(tmp, "out.bin")
+        rec = case_records(design_a, n, 0.0, False, threads, None, mode=4)
+        rec["alpha2"], rec["gamma2"] = design_b.alpha, design_b.gamma
+        if precision == "dropin":
+            rec["solverType"] = [int(solver_type)]
+        casefile.write_records(cpath, rec)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        proc = subprocess.run([binary(precision), cpath, opath], cwd=tmp, env=env, stdout=subprocess.DEVNULL,
+                              stderr=subprocess.PIPE, timeout=timeout)
+        if proc.returncode != 0:
+            raise RuntimeError(f"reference harness failed: {proc.stderr.decode()[-2000:]}")
+        out = casefile.read_records(opath)
+    M, N = design_a.M, design_a.N
+    for k in (1, 2, 3):
+        out[f"u{k}"] = out[f"u{k}"].reshape(M + 1, N)
+        out[f"v{k}"] = out[f"v{k}"].reshape(M, N + 1)
+        out[f"p{k}"] = out[f"p{k}"].reshape(M + 1, N + 1)
     return out
 
 
@@ -99,7 +137,7 @@ def run_iterations(design, max_iterations: int, window: int, percent: float, ram
     them, 6 significant digits), the final fields and ``logs``: the texts of
     the residuals.txt and pressure_drop_history.txt it wrote."""
     if not available(precision):
-        raise FileNotFoundError(f"{binary(precision)} not built (make -C oracle ref)")
+        raise FileNotFoundError(f"{binary(precision)} not built (make -C oracle ref REF=<reference checkout>)")
     with tempfile.TemporaryDirectory(prefix="cps_ref_") as tmp:
         cpath, opath = os.path.join(tmp, "case.bin"), os.path.join(tmp, "out.bin")
         rec = case_records(design, max_iterations, 0.0, False, threads, None, mode=2, x_core=x_core)
@@ -135,7 +173,7 @@ def run_io(files: Dict[str, str], restart: Optional[Dict[str, str]] = None,
     alpha, u, v, p)
     and ``written``: every file left in ExportFiles, as text."""
     if not available(precision):
-        raise FileNotFoundError(f"{binary(precision)} not built (make -C oracle ref)")
+        raise FileNotFoundError(f"{binary(precision)} not built (make -C oracle ref REF=<reference checkout>)")
     with tempfile.TemporaryDirectory(prefix="cps_ref_io_") as tmp:
         os.makedirs(os.path.join(tmp, "ExportFiles"))
         for name, text in files.items():
@@ -199,7 +237,7 @@ def run_thermal_outputs(T: np.ndarray, gamma: np.ndarray, dx: float, dy: float, 
     Params::dx(), dy()) and the bytes of the files it writes."""
     path = os.path.join(REF_DIR, "thermal_out")
     if not os.access(path, os.X_OK):
-        raise FileNotFoundError(f"{path} not built (make -C oracle ref)")
+        raise FileNotFoundError(f"{path} not built (make -C oracle ref REF=<reference checkout>)")
     Ny, Nx = gamma.shape
     with tempfile.TemporaryDirectory(prefix="cps_thout_") as tmp:
         cpath, opath = os.path.join(tmp, "case.bin"), os.path.join(tmp, "out.bin")
@@ -239,7 +277,7 @@ def run_thermal_assembly(Nx: int, Ny: int, dx: float, dy: float, gamma: np.ndarr
     ("stdout": the temperature ranges and the energy balance)."""
     path = os.path.join(REF_DIR, "thermal_asm")
     if not os.access(path, os.X_OK):
-        raise FileNotFoundError(f"{path} not built (make -C oracle ref)")
+        raise FileNotFoundError(f"{path} not built (make -C oracle ref REF=<reference checkout>)")
     with tempfile.TemporaryDirectory(prefix="cps_thasm_") as tmp:
         cpath, opath = os.path.join(tmp, "case.bin"), os.path.join(tmp, "out.bin")
         casefile.write_records(cpath, {

@@ -3,7 +3,7 @@ own code (oracle/_ref/ref_f64 = the reference promoted to double, ref_f32 =
 as shipped), run with one OpenMP thread so every reduction is sequential.
 
 Run from the repository root where the reference sources are available:
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref REF=<reference checkout> && python tests/golden/make_golden.py
 The fixtures are committed; tests read them without the reference present.
 
 `python tests/golden/make_golden.py NAME ...` writes only the named flow

@@ -1,0 +1,121 @@
+"""Converged-state parity with the reference's own FP64 solve, on the
+workloads' designs: the 500 x 250 channel network, the 1000 x 500 density
+field, a design of the 64-design mix solved inside a batch, and a request of
+the served stream solved through the serving loop (mixed precision).
+
+The oracle is the reference's own code (its sources promoted to double) run
+from the zero state to the 1e-10 outer residual, committed as fixtures by
+tests/golden/make_converged.py.  At 1e-10 both runs sit on the discrete fixed
+point of the SIMPLE iteration, which no longer depends on the order of the
+grid-wide sums (at the 1e-6 stop the reference differs from itself by ~1e-4
+between thread counts; the fixtures record how far its own 1e-6 stop sits from
+its fixed point).  Tolerances: u, v and fluid-cell p within 1e-6 relative L2,
+the full inlet-outlet total-pressure drop within 1e-5 relative; the fixtures
+hold every stride-th row and column (stride 2 for the 1000 x 500 design) in
+float32, whose rounding (6e-8) is far below those bounds.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from coldplate_solver_b200 import cps, geometry
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CONVERGED = os.path.join(HERE, "golden", "converged")
+REL_FIELD = 1e-6
+REL_DP = 1e-5
+EPS_FIXED = 1e-10
+MAX_OUTER = 400000
+
+
+def fixture(name):
+    path = os.path.join(CONVERGED, name + ".npz")
+    if not os.path.exists(path):
+        pytest.skip(f"fixture {name} not generated (tests/golden/make_converged.py)")
+    return np.load(path)
+
+
+def design_of(z):
+    gen, args = str(z["generator"]), json.loads(str(z["args"]))
+    if gen == "channel_network":
+        return geometry.channel_network(**args)
+    if gen == "density_field":
+        return geometry.density_field(**args)
+    if gen == "batch_mix":
+        return geometry.batch_mix(args["n"])[args["k"]]
+    if gen == "served_stream":
+        return geometry.served_stream(args["n"])[args["k"]][1]
+    raise ValueError(gen)
+
+
+def rel(a, b):
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / nb if nb > 0 else np.linalg.norm(a - b)
+
+
+def fluid_mask_p(d):
+    mask = np.zeros((d.M + 1, d.N + 1), dtype=bool)
+    mask[1:d.M, 1:d.N] = d.gamma[:d.M - 1, :d.N - 1] > 0.5
+    return mask
+
+
+def assert_fixed_point(d, z, fields, dp):
+    st = int(z["stride"])
+    assert (int(z["M"]), int(z["N"])) == (d.M, d.N)
+    for k in ("u", "v"):
+        e = rel(fields[k][::st, ::st], z[k].astype(np.float64))
+        assert e <= REL_FIELD, (k, e)
+    mask = fluid_mask_p(d)[::st, ::st]
+    e = rel(fields["p"][::st, ::st][mask], z["p"].astype(np.float64)[mask])
+    assert e <= REL_FIELD, ("p", e)
+    dpr = float(z["dp_full"])
+    assert abs(dp - dpr) <= REL_DP * abs(dpr), (dp, dpr)
+
+
+@pytest.mark.parametrize("name,precision", [("network_500x250", cps.CPS_FP64), ("density_1000x500", cps.CPS_FP64),
+                                            ("network_500x250", cps.CPS_MIXED)])
+def test_single_design_reaches_the_reference_fixed_point(name, precision):
+    z = fixture(name)
+    d = design_of(z)
+    with cps.Solver(d, precision=precision) as s:
+        h = s.solve(MAX_OUTER, eps=1e-6)
+        assert max(h[-1, 0], h[-1, 1], h[-1, 3]) <= 1e-6
+        # the stop iteration is chaotic (it moves with the order of the sums), the count stays in range
+        assert 0.5 * int(z["n_stop"]) <= len(h) <= 2.0 * int(z["n_stop"]), (len(h), int(z["n_stop"]))
+        h2 = s.solve(MAX_OUTER, eps=EPS_FIXED)
+        assert len(h2) < MAX_OUTER and max(h2[-1, 0], h2[-1, 1], h2[-1, 3]) <= EPS_FIXED
+        f = s.download()
+        assert_fixed_point(d, z, f, s.full_dp())
+
+
+def test_mix_design_in_a_batch_reaches_the_reference_fixed_point():
+    """mix design 47 solved with three other designs of the mix by the batched
+    kernel (groups of CTAs taking designs from the device work queue)."""
+    from coldplate_solver_b200 import batch
+    z = fixture("mix47_258x129")
+    mix = geometry.batch_mix(64)
+    designs = [mix[47], mix[62], mix[50], mix[13]]
+    with batch.BatchRunner(designs, precision=cps.CPS_FP64, mode={"group_ctas": 64}) as br:
+        res, _, _ = br.run(eps=EPS_FIXED, max_outer=MAX_OUTER, visit=4096)
+        assert all(r["converged"] for r in res), res
+        s = br.solvers[0]
+        assert_fixed_point(designs[0], z, s.download(), s.full_dp())
+
+
+def test_served_request_reaches_the_reference_fixed_point():
+    """Request 14 of the served stream (137 x 68 cells, 2.5-D) among four
+    requests through the serving loop (continuous batching, mixed precision)."""
+    from coldplate_solver_b200 import serve
+    z = fixture("served14_137x68")
+    stream = geometry.served_stream(32)
+    picked = [stream[k] for k in (14, 12, 9, 4)]
+    srv = serve.Server(precision=cps.CPS_MIXED, eps=EPS_FIXED, max_outer=MAX_OUTER, keep_fields=True, visit=2000,
+                       mode={"group_ctas": 32})
+    st = srv.run([(0.0, d) for _, d in picked], real_time=False)
+    r = st.requests[0]
+    assert r.converged, (r.outer_iterations, r.last)
+    assert_fixed_point(picked[0][1], z, r.fields, r.dp)

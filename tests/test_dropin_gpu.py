@@ -59,3 +59,46 @@ def test_reference_driver_with_pseudo_transient(mom):
     np.testing.assert_allclose(a["pseudoCFL"], b["pseudoCFL"], rtol=1e-9)
     for k in FIELDS:
         assert rel(a[k], b[k]) <= 1e-10, (k, rel(a[k], b[k]))
+
+
+def test_design_loop_in_one_process():
+    """Two designs of one grid through the reference's own driver in one
+    process (harness mode 4): object A runs design A and is destroyed, a new
+    object B in the same storage runs design B, then B is edited in place back
+    to design A from the zero state.  Each phase through the drop-in equals the
+    same phase of the unpatched FP64 reference: the new object is told from
+    the old one at the same address, and the in-place edit reaches the GPU."""
+    from oracle import reference
+    if not (reference.available("dropin") and reference.available("f64")):
+        pytest.skip("reference binaries not built in this checkout")
+    da = geometry.channel_network(M=40, N=72, h=20e-6, wmin=4, wmax=8, seed=5)
+    db = geometry.channel_network(M=40, N=72, h=20e-6, wmin=4, wmax=8, seed=11)
+    assert not np.array_equal(da.gamma, db.gamma)
+    n = 20
+    a = reference.run_design_loop(da, db, n, precision="dropin")
+    b = reference.run_design_loop(da, db, n, precision="f64")
+    for k in (1, 2, 3):
+        assert np.array_equal(a[f"pIters{k}"], b[f"pIters{k}"]), k
+        np.testing.assert_allclose(a[f"err{k}"], b[f"err{k}"], rtol=1e-8, atol=1e-300)
+        for f in ("u", "v", "p"):
+            assert rel(a[f"{f}{k}"], b[f"{f}{k}"]) <= 1e-10, (k, f, rel(a[f"{f}{k}"], b[f"{f}{k}"]))
+    # phase 3 is design A from the zero state again; phase 2 is another design
+    assert rel(a["u3"], a["u1"]) <= 1e-10
+    assert rel(a["u2"], a["u1"]) > 1e-3
+
+
+def test_mixed_precision_through_the_registry():
+    """pressureSolverType = 6 selects the mixed-precision path (FP32 inner
+    solves inside the FP64 defect correction): after 10 outer iterations it
+    stays within the mixed path's per-step tolerance (1e-3 relative) of the
+    FP64 reference."""
+    from oracle import reference
+    if not (reference.available("dropin") and reference.available("f64")):
+        pytest.skip("reference binaries not built in this checkout")
+    d = geometry.channel_network(M=40, N=72, h=20e-6, wmin=4, wmax=8, seed=5)
+    a = reference.run(d, 10, precision="dropin", solver_type=6)
+    b = reference.run(d, 10, precision="f64")
+    for k in ("u", "v", "p"):
+        assert rel(a[k], b[k]) <= 1e-3, (k, rel(a[k], b[k]))
+    c = reference.run(d, 10, precision="dropin", solver_type=5)
+    assert rel(a["u"], c["u"]) > 0.0  # the registry value reached the library

@@ -26,22 +26,25 @@ class CallerBuffers:
     """Device buffers the caller owns (allocated here by the test, as the
     caller's own pool would), all with one row pitch."""
 
-    def __init__(self, design, pitch, init):
+    def __init__(self, design, pitch, init, pad=0.0):
+        """``pad``: the value of every element outside the logical matrices
+        (the columns past each matrix's width, row M of the v plane), as a
+        pool allocator may leave it."""
         import torch
         self.torch = torch
         M, N = design.M, design.N
         self.design, self.pitch = design, pitch
         dev = torch.device("cuda", 0)
 
-        def plane(rows, host=None, cols=None):
-            t = torch.zeros((rows, pitch), dtype=torch.float64, device=dev)
+        def plane(rows, host=None):
+            t = torch.full((rows, pitch), pad, dtype=torch.float64, device=dev)
             if host is not None:
-                t[:, :host.shape[1]] = torch.from_numpy(np.ascontiguousarray(host)).to(dev)
+                t[:host.shape[0], :host.shape[1]] = torch.from_numpy(np.ascontiguousarray(host)).to(dev)
             return t
         self.alpha = plane(M, design.alpha)
         self.gamma = plane(M, design.gamma)
         self.u = plane(M + 1, init["u"])
-        self.v = plane(M + 1, np.vstack([init["v"], np.zeros((1, N + 1))]))
+        self.v = plane(M + 1, init["v"])
         self.p = plane(M + 1, init["p"])
         self.out = {k: plane(M + 1) for k in ("pStar", "uStar", "vStar", "dE", "dN")}
 
@@ -56,11 +59,16 @@ class CallerBuffers:
         return {k: src[k][:rows.get(k, M + 1), :cols[k]].cpu().numpy() for k in OUT_FIELDS}
 
 
-def call_noalloc(lib, design, buf, n, eps=0.0):
+def call_noalloc(lib, design, buf, n, eps=0.0, stream=None):
+    """One call on ``stream`` (a torch stream; default: torch's current one),
+    after the work already queued on torch's current stream."""
     desc, keep = cps.make_desc(design)
     hist = (cps.CpsStepOut * n)()
     nd = ctypes.c_int(0)
-    stream = ctypes.c_void_p(buf.torch.cuda.current_stream().cuda_stream)
+    torch = buf.torch
+    if stream is not None:
+        stream.wait_stream(torch.cuda.current_stream())
+    stream = ctypes.c_void_p((stream or torch.cuda.current_stream()).cuda_stream)
     st = lib.cps_solve_noalloc(ctypes.byref(desc), buf.pitch, buf.ptr(buf.alpha), buf.ptr(buf.gamma), buf.ptr(buf.u),
                                buf.ptr(buf.v), buf.ptr(buf.p), buf.ptr(buf.out["pStar"]), buf.ptr(buf.out["uStar"]),
                                buf.ptr(buf.out["vStar"]), buf.ptr(buf.out["dE"]), buf.ptr(buf.out["dN"]),
@@ -114,3 +122,30 @@ def test_noalloc_rejects_designs_beyond_the_static_scratch():
     st = lib.cps_solve_noalloc(ctypes.byref(desc), 320, None, None, None, None, None, None, None, None, None, None,
                                0.1, 5, 0.0, None, ctypes.byref(nd), None)
     assert st == cps.CPS_ERR_ARG and nd.value == 0
+
+
+def test_noalloc_ignores_padding_and_runs_on_the_callers_stream():
+    """Caller buffers straight from a pool carry whatever the padding held
+    before: with NaN in every element outside the logical matrices, on a
+    non-default stream, two calls in a row still match cps_solve."""
+    import torch
+    lib = cps.load_library()
+    d = geometry.channel_network(M=48, N=100, h=20e-6, wmin=4, wmax=8, seed=8)
+    rng = np.random.default_rng(9)
+    init = {"u": rng.normal(0, 0.05, (d.M + 1, d.N)), "v": rng.normal(0, 0.02, (d.M, d.N + 1)),
+            "p": rng.normal(0, 5.0, (d.M + 1, d.N + 1))}
+    pitch = ((d.N + 1 + 31) // 32) * 32 + 32
+    buf = CallerBuffers(d, pitch, init, pad=float("nan"))
+    side = torch.cuda.Stream()
+    with cps.Solver(d) as ref:
+        ref.upload_fields(init["u"], init["v"], init["p"])
+        for call in range(2):
+            h_ref = ref.solve(10, eps=0.0)
+            f_ref = ref.download()
+            h = call_noalloc(lib, d, buf, 10, stream=side)
+            f = buf.fields()
+            assert np.array_equal(h[:, 5:], h_ref[:, 5:]), (call, h[:, 5:], h_ref[:, 5:])
+            np.testing.assert_allclose(h[:, :5], h_ref[:, :5], rtol=1e-8, atol=1e-300)
+            for k in OUT_FIELDS:
+                assert np.isfinite(f[k]).all(), (call, k)
+                assert rel(f[k], f_ref[k]) <= REL_STEP, (call, k, rel(f[k], f_ref[k]))
