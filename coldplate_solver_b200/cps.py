@@ -280,6 +280,7 @@ class Solver:
                  pcg_variant: int = CPS_PCG_REFERENCE):
         self.lib = load_library()
         self.design = design
+        self.precision, self.device = precision, device
         desc, keep = make_desc(design, precision, device, grid_ctas, pcg_variant)
         ctx = _P()
         st = self.lib.cps_create(ctypes.byref(desc), ctypes.byref(ctx))

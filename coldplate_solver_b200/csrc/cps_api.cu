@@ -91,11 +91,12 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_grid_kernel
   cps::GridGroup g{bar, red, rc.status, blockIdx.x, gridDim.x, 0u, 0ull};
   cps::load_pseudo(d, s_pr);
   __syncthreads();
+  cps::SweepHint hint{2, 2};
   for (int it = 0; it < rc.n_outer; ++it) {
     double out[8];
     const int r = cps::outer_iteration<T, cps::GridGroup, Monitor>(
         d, g, smem, tile_smem, out, it + 1 == rc.n_outer, rc.stop_on_conv != 0, rc.eps, rc.iter0 + it,
-        rc.dplog ? rc.dplog + (size_t)4 * it : nullptr, rc.dp_converged, &s_pr);
+        rc.dplog ? rc.dplog + (size_t)4 * it : nullptr, rc.dp_converged, &s_pr, &hint);
     if (r < 0) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       for (int k = 0; k < 8; ++k) rc.hist[(size_t)it * 8 + k] = out[k];
@@ -138,10 +139,11 @@ __global__ void __launch_bounds__(cps::kThreads) cps_cluster_kernel(const cps::B
     g.status = &res->status;
     double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int done = 0;
+    cps::SweepHint hint{2, 2};
     for (int it = 0; it < item.n_outer; ++it) {
       const int r = cps::outer_iteration<T, cps::ClusterGroup, false, Pseudo>(
           item.view, g, smem, tile_smem, out, it + 1 == item.n_outer, item.stop_on_conv != 0, item.eps, item.iter0 + it,
-          nullptr, nullptr, &s_pr);
+          nullptr, nullptr, &s_pr, &hint);
       done = it + 1;
       if (g.rank == 0 && threadIdx.x == 0 && item.hist && it < item.hist_cap)
         for (int k = 0; k < 8; ++k) item.hist[(size_t)it * 8 + k] = out[k];
@@ -198,10 +200,11 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_group_kerne
     g.status = &res->status;
     double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int done = 0;
+    cps::SweepHint hint{2, 2};
     for (int it = 0; it < item.n_outer; ++it) {
       const int r = cps::outer_iteration<T, cps::GridGroup, false, Pseudo>(
           item.view, g, smem, tile_smem, out, it + 1 == item.n_outer, item.stop_on_conv != 0, item.eps, item.iter0 + it,
-          nullptr, nullptr, &s_pr);
+          nullptr, nullptr, &s_pr, &hint);
       if (r < 0) return;  // a bounded wait expired; the design's status says so
       done = it + 1;
       if (g.rank == 0 && threadIdx.x == 0 && item.hist && it < item.hist_cap)
@@ -252,10 +255,11 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_wave_kernel
                    blockIdx.x - (unsigned)first[grp], (unsigned)K, 0u, 0ull};
   double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int done = 0;
+  cps::SweepHint hint{2, 2};
   for (int it = 0; it < item.n_outer; ++it) {
     const int r = cps::outer_iteration<T, cps::GridGroup, false, Pseudo>(
         item.view, g, smem, tile_smem, out, it + 1 == item.n_outer, item.stop_on_conv != 0, item.eps, item.iter0 + it,
-        nullptr, nullptr, &s_pr);
+        nullptr, nullptr, &s_pr, &hint);
     if (r < 0) return;  // a bounded wait expired; the design's status says so
     done = it + 1;
     if (g.rank == 0 && threadIdx.x == 0 && item.hist && it < item.hist_cap)

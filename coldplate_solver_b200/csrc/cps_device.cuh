@@ -144,6 +144,13 @@ struct PseudoRun {
   int count, pad;
 };
 
+// The Jacobi sweep counts of a design's last outer iteration, carried from one
+// outer iteration to the next by every thread (the counts come from grid-wide
+// reductions, so every thread holds the same values).
+struct SweepHint {
+  int kU, kV;
+};
+
 template <typename T> __device__ __forceinline__ const Inner<T>& inner(const DesignView& d);
 template <> __device__ __forceinline__ const Inner<double>& inner<double>(const DesignView& d) { return d.f64; }
 template <> __device__ __forceinline__ const Inner<float>& inner<float>(const DesignView& d) { return d.f32; }
@@ -793,15 +800,31 @@ __device__ __forceinline__ double row_times_current(const MomRow& m, const Layou
   return Ax;
 }
 
+// Stores the row of one unknown and its source (FP64: b = Sp; mixed: b = r0)
+// in the storage type T the Jacobi sweeps read.
+template <bool IsU, typename T>
+__device__ __forceinline__ void store_row(const DesignView& d, size_t o, T cE, T cW, T cN, T cS, T aP, T b) {
+  const Inner<T>& w = inner<T>(d);
+  T* c = IsU ? w.cU : w.cV;
+  const long long ps = d.planeStride;
+  c[o] = cE;
+  c[o + ps] = cW;
+  c[o + 2 * ps] = cN;
+  c[o + 3 * ps] = cS;
+  c[o + 4 * ps] = aP;
+  (IsU ? w.bU : w.bV)[o] = b;
+}
+
 // Momentum assembly at one unknown fused with Jacobi sweep 1
-// (jacobi_solver.cpp:49-57, x0 = current velocity).  Stores dE or dN and the
-// sweep's result; the row itself is not stored (a second sweep re-assembles
-// it).  Returns the squared residual of sweep 1 (0 when no sweep is run).
+// (jacobi_solver.cpp:49-57, x0 = current velocity).  Stores dE or dN, the
+// sweep's result and, with `storeRow`, the row for the sweeps after it (a
+// second sweep re-assembles the row when it was not stored).  Returns the
+// squared residual of sweep 1 (0 when no sweep is run).
 //   FP64:  b = Sp, x1 = x0 + (b - A x0)/aP.
 //   mixed: b = r0 = Sp - A x0 (FP64 defect), delta1 = r0/aP (delta0 = 0).
 template <bool IsU, typename T, bool Pseudo>
 __device__ __forceinline__ double assemble_point(const DesignView& d, const LayoutA& L, int i, int j, bool sweep,
-                                                 double cfl) {
+                                                 double cfl, bool storeRow) {
   constexpr bool kMixed = sizeof(T) == 4;
   const Inner<T>& w = inner<T>(d);
   double dv;
@@ -813,6 +836,8 @@ __device__ __forceinline__ double assemble_point(const DesignView& d, const Layo
     return 0.0;
   }
   const double r = m.Sp - row_times_current<IsU>(m, L, i, j);
+  if (storeRow)
+    store_row<IsU, T>(d, o, (T)m.cE, (T)m.cW, (T)m.cN, (T)m.cS, (T)m.aP, kMixed ? (T)r : (T)m.Sp);
   if (kMixed) {
     (IsU ? w.xU1 : w.xV1)[o] = (T)(r / m.aP);
     return r * r;
@@ -836,16 +861,7 @@ __device__ __forceinline__ double sweep2_point(const DesignView& d, const Layout
   const size_t o = (size_t)i * P + j;
   const T cE = (T)m.cE, cW = (T)m.cW, cN = (T)m.cN, cS = (T)m.cS, aPt = (T)m.aP;
   const T bt = kMixed ? (T)(m.Sp - row_times_current<IsU>(m, L, i, j)) : (T)m.Sp;
-  if (store) {
-    T* c = IsU ? w.cU : w.cV;
-    const long long ps = d.planeStride;
-    c[o] = cE;
-    c[o + ps] = cW;
-    c[o + 2 * ps] = cN;
-    c[o + 3 * ps] = cS;
-    c[o + 4 * ps] = aPt;
-    (IsU ? w.bU : w.bV)[o] = bt;
-  }
+  if (store) store_row<IsU, T>(d, o, cE, cW, cN, cS, aPt, bt);
   double Ax = 0.0;
   if (m.hasS) Ax += (double)cS * (double)xin[o - P];
   if (m.hasW) Ax += (double)cW * (double)xin[o - 1];
@@ -1713,13 +1729,19 @@ constexpr size_t tile_smem_bytes() {
 template <typename T, class Group, bool Monitor = false, bool Pseudo = true>
 __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char* tbuf, double (&out)[8],
                                bool lastIter, bool stopOnConv, double eps, int iter = 0, double* dplog = nullptr,
-                               int* dpConverged = nullptr, PseudoRun* pr = nullptr) {
+                               int* dpConverged = nullptr, PseudoRun* pr = nullptr, SweepHint* hint = nullptr) {
   const Inner<T>& w = inner<T>(d);
   const int M = d.M, N = d.N, P = d.P;
   // ---- A: assembly + sweep 1 (or the explicit update) ----
   const double cfl = (Pseudo && d.pseudo && pr) ? pr->cfl : 0.0;
   const bool expl = d.momExplicit != 0;
   const bool anySweep = !expl && d.maxMomIter > 0;
+  // Rows are stored in phase A when the last outer iteration needed a second
+  // sweep of that component (the sweep counts change slowly); otherwise a
+  // second sweep re-assembles them.  Both give the same bits.
+  const bool canSweep2 = anySweep && d.maxMomIter > 1;
+  const bool storeU = canSweep2 && (!hint || hint->kU >= 2);
+  const bool storeV = canSweep2 && (!hint || hint->kV >= 2);
   double red2[2] = {0.0, 0.0};
   for_each_tile<LayoutA>(
       d, g.rank, g.nblk, tbuf,
@@ -1736,8 +1758,8 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
           if (i <= M - 2) explicit_point<false, T, Pseudo>(d, L, i, j, cfl);
           return;
         }
-        if (j <= N - 2) red2[0] += assemble_point<true, T, Pseudo>(d, L, i, j, anySweep, cfl);
-        if (i <= M - 2) red2[1] += assemble_point<false, T, Pseudo>(d, L, i, j, anySweep, cfl);
+        if (j <= N - 2) red2[0] += assemble_point<true, T, Pseudo>(d, L, i, j, anySweep, cfl, storeU);
+        if (i <= M - 2) red2[1] += assemble_point<false, T, Pseudo>(d, L, i, j, anySweep, cfl, storeV);
       });
   if (!g.template sync_reduce<2, 0u>(red2, smem)) return -1;
   int kU = anySweep ? 1 : 0, kV = kU;
@@ -1752,9 +1774,9 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
     T* xoutV = (k & 1) ? w.xV1 : w.xV0;
     double s[2] = {0.0, 0.0};
     const bool au = actU, av = actV;
-    if (k == 2) {
-      // sweep 2 re-assembles the rows from phase A's staged inputs and stores
-      // them for the sweeps after it
+    if (k == 2 && ((au && !storeU) || (av && !storeV))) {
+      // sweep 2 of a component whose rows phase A did not store re-assembles
+      // them from the same staged inputs and stores them for the sweeps after it
       const bool store = d.maxMomIter > 2;
       for_each_tile<LayoutA>(
           d, g.rank, g.nblk, tbuf,
@@ -1766,8 +1788,12 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
           },
           [&](const LayoutA& L, int i, int j, bool inside) {
             if (!inside) return;
-            if (au && j <= N - 2) s[0] += sweep2_point<true, T, Pseudo>(d, L, i, j, cfl, xinU, xoutU, store);
-            if (av && i <= M - 2) s[1] += sweep2_point<false, T, Pseudo>(d, L, i, j, cfl, xinV, xoutV, store);
+            if (au && j <= N - 2)
+              s[0] += storeU ? sweep_point<true, T>(d, i, j, xinU, xoutU)
+                             : sweep2_point<true, T, Pseudo>(d, L, i, j, cfl, xinU, xoutU, store);
+            if (av && i <= M - 2)
+              s[1] += storeV ? sweep_point<false, T>(d, i, j, xinV, xoutV)
+                             : sweep2_point<false, T, Pseudo>(d, L, i, j, cfl, xinV, xoutV, store);
           });
     } else {
       for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
@@ -1778,6 +1804,10 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
     if (!g.template sync_reduce<2, 0u>(s, smem)) return -1;
     if (au) { kU = k; actU = !(s[0] < d.thrU) && kU < d.maxMomIter; }
     if (av) { kV = k; actV = !(s[1] < d.thrV) && kV < d.maxMomIter; }
+  }
+  if (hint) {
+    hint->kU = kU;
+    hint->kV = kV;
   }
   const T* xfU = (kU & 1) ? w.xU1 : w.xU0;
   const T* xfV = (kV & 1) ? w.xV1 : w.xV0;

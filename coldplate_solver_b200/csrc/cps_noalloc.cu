@@ -67,10 +67,11 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_noalloc_ker
   __shared__ double smem[cps::kRedWidth * 8];
   extern __shared__ __align__(16) char tile_smem[];
   cps::GridGroup g{bar, red, rc.status, blockIdx.x, gridDim.x, 0u, 0ull};
+  cps::SweepHint hint{2, 2};
   for (int it = 0; it < rc.n_outer; ++it) {
     double out[8];
     const int r = cps::outer_iteration<double>(d, g, smem, tile_smem, out, it + 1 == rc.n_outer,
-                                               rc.stop_on_conv != 0, rc.eps);
+                                               rc.stop_on_conv != 0, rc.eps, 0, nullptr, nullptr, nullptr, &hint);
     if (r < 0) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       for (int k = 0; k < 8; ++k) rc.hist[(size_t)it * 8 + k] = out[k];

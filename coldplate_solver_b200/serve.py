@@ -64,10 +64,13 @@ class ServeStats:
 class Server:
     def __init__(self, budget_bytes: float = 120e9, visit: int = 300, cluster_ctas: Optional[int] = None,
                  precision: int = cps.CPS_MIXED, device: int = 0, max_inflight: int = 256, eps: float = 1e-6,
-                 max_outer: int = 200000, keep_fields: bool = False, mode: Optional[dict] = None):
+                 max_outer: int = 200000, keep_fields: bool = False, mode: Optional[dict] = None,
+                 keep: Sequence[int] = ()):
         """``mode``: placement keyword of :func:`cps.batch_solve`
         (default: :func:`batch.default_mode`); ``cluster_ctas`` is shorthand
-        for ``mode={"cluster_ctas": cluster_ctas}``."""
+        for ``mode={"cluster_ctas": cluster_ctas}``.  ``keep_fields`` keeps
+        every request's final fields (Request.fields), ``keep`` those of the
+        requests with these indices in the stream."""
         self.budget = int(budget_bytes)
         self.visit = visit
         if mode is None:
@@ -79,6 +82,7 @@ class Server:
         self.eps = eps
         self.max_outer = max_outer
         self.keep_fields = keep_fields
+        self.keep = set(keep)
 
     def run(self, stream: Sequence[Tuple[float, Design]], real_time: bool = True) -> ServeStats:
         """Serve ``stream`` (arrival time in s, design).  With ``real_time``
@@ -122,7 +126,7 @@ class Server:
                 if r.converged or r.status != 0 or r.outer_iterations >= self.max_outer:
                     r.finished = end
                     r.dp = s.full_dp()
-                    if self.keep_fields:
+                    if self.keep_fields or r.rid in self.keep:
                         r.fields = s.download()
                     s.close()
                     used -= fp

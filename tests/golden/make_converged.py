@@ -3,24 +3,34 @@ reference solver's own code (oracle/_ref/ref_f64: the reference's sources
 promoted to double), run on all host cores.
 
 For each design the reference solves from the zero state to its own 1e-6
-stop (max(residU, residV, residMassDof) <= 1e-6), and then, carrying the state
-(u, v, p), on to the 1e-10 residual, where the state is the discrete fixed
-point of the SIMPLE iteration and no longer depends on the summation order of
-the run (the reference differs from itself by ~1e-4 between OpenMP thread
-counts at the 1e-6 stop, and by ~1e-9 at 1e-10).  Stored per design:
+stop (max(residU, residV, residMassDof) <= 1e-6) with the design's settings,
+and then, carrying the state (u, v, p), on to the 1e-10 residual with tight
+inner tolerances (TIGHT: PCG pTol 1e-10 with up to 1000 iterations, Jacobi
+momentumTol 1e-10).  With the reference's default inner tolerances the
+outer residual of these designs does not fall much below 1e-6: the PCG, held
+to an absolute ||r|| < 1e-4, takes one step per outer iteration there, and the
+residual wanders between ~3e-7 and ~4e-6 (the 1e-6 stop is one of its dips,
+which is why the stop iteration moves with the order of the sums).  The
+inner tolerances do not enter the fixed point of the iteration -- at a fixed
+point the Jacobi and PCG corrections vanish, so it is the solution of the
+discrete momentum and continuity equations -- and with tight ones the outer
+residual falls geometrically; on the 137 x 68 served design the state at
+residual 1e-8 is within 1.2e-8 relative of the state at the 1e-12 floor.
+Stored per design:
 
   u, v, p        the fixed point (float32: its rounding, 6e-8 relative, is far
                  below the 1e-6 tolerance of the tests), every ``stride``-th
                  row and column (stride 2 for the 1000 x 500 design, 1 else)
-  planes         the four sampled planes of the fixed point (core in/out,
-                 x = 0, x = N hx; flowArea, massFlux, avgStatic, avgDynamic,
+  planes         the four sampled planes of the fixed point (x = 0, x = N hx,
+                 core in, core out; flowArea, massFlux, avgStatic, avgDynamic,
                  avgTotal, valid), FP64
   dp_full        full inlet-outlet total-pressure drop of the fixed point
-  n_stop, n_fixed            outer iterations to 1e-6 and on to 1e-10
+  n_stop, n_fixed            outer iterations to 1e-6 and then on to 1e-10
   stop_err_u/v/p, stop_err_dp  the reference's own 1e-6 stop state against
                  its fixed point (relative L2 on u, v and fluid-cell p,
                  relative dP): how far any run stopped at 1e-6 sits from the
                  fixed point
+  tight          the inner tolerances of the second stage (JSON)
   generator, args            how to rebuild the design (geometry module)
 
 Run from the repository root where the reference sources are available:
@@ -46,6 +56,7 @@ from oracle import reference  # noqa: E402
 OUT = os.path.join(HERE, "converged")
 EPS_STOP, EPS_FIXED = 1e-6, 1e-10
 MAX_OUTER = 400000
+TIGHT = {"pTol": 1e-10, "maxPressureIter": 1000, "momentumTol": 1e-10}
 
 
 def design_of(generator: str, args: dict):
@@ -83,7 +94,9 @@ def rel(a, b) -> float:
 
 
 def full_dp(planes: np.ndarray) -> float:
-    return float(planes[2, 4] - planes[3, 4])
+    """avgTotal(x = 0) - avgTotal(x = N hx): the harness samples x = 0, N hx,
+    core in, core out in that order."""
+    return float(planes[0, 4] - planes[1, 4])
 
 
 def make(name: str, threads: int) -> None:
@@ -95,8 +108,8 @@ def make(name: str, threads: int) -> None:
     n_stop = len(a["err"])
     print(f"{name}: 1e-6 stop after {n_stop} outer iterations ({time.time() - t0:.0f} s)", flush=True)
     stop = {k: a[k] for k in ("u", "v", "p")}
-    b = reference.run(d, MAX_OUTER, precision="f64", eps=EPS_FIXED, stop_on_conv=True, threads=threads, init=stop,
-                      timeout=24 * 3600)
+    b = reference.run(d.replace(**TIGHT), MAX_OUTER, precision="f64", eps=EPS_FIXED, stop_on_conv=True,
+                      threads=threads, init=stop, timeout=24 * 3600)
     n_fixed = len(b["err"])
     last = max(b["residU"][-1], b["residV"][-1], b["residMassDof"][-1])
     if last > EPS_FIXED:
@@ -112,7 +125,7 @@ def make(name: str, threads: int) -> None:
         planes=b["planes"], dp_full=dp_fixed, dp_stop=dp_stop, n_stop=n_stop, n_fixed=n_fixed,
         stop_err_u=rel(a["u"], b["u"]), stop_err_v=rel(a["v"], b["v"]),
         stop_err_p=rel(a["p"][mask], b["p"][mask]), stop_err_dp=abs(dp_stop - dp_fixed) / abs(dp_fixed),
-        residual_fixed=last, threads=threads, generator=generator, args=json.dumps(args))
+        residual_fixed=last, threads=threads, tight=json.dumps(TIGHT), generator=generator, args=json.dumps(args))
     print(f"{name}: {n_stop} + {n_fixed} outer iterations, dP {dp_fixed:.9g} Pa (at the 1e-6 stop {dp_stop:.9g}), "
           f"{time.time() - t0:.0f} s", flush=True)
 

@@ -26,14 +26,15 @@ def run_bench(*args):
 @pytest.mark.skipif(not (reference.available("f64") and reference.available("f32")),
                     reason="oracle/_ref/ref_f64 and ref_f32 not built")
 def test_reference_arm_line():
-    d = run_bench("--impl", "reference", "--workload", "straight", "--steps", "1", "--warmup", "0")
+    d = run_bench("--impl", "reference", "--workload", "straight", "--steps", "1", "--warmup", "0",
+                  "--ref-threads", "1")
     for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
               "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
         assert k in d, k
     assert d["impl"] == "reference" and d["unit"] == "solves/s" and d["value"] > 0
     assert d["config"]["workload"] == "straight_channel_200x100_fou" and d["config"]["converged"]
     cb = d["cpu_baseline"]
-    assert cb["kind"] == "reference" and cb["value"] == d["value"] and cb["cores"] >= 1
+    assert cb["kind"] == "reference" and cb["value"] == d["value"] and cb["cores"] == 1
     assert cb["as_shipped_fp32"]["value"] > 0 and cb["as_shipped_fp32"]["converged"]
     assert d["e2e"] == {"value": d["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
 
