@@ -17,9 +17,12 @@
 // Launch, many designs (cps_batch_solve): one thread-block cluster per design
 // at a time; clusters take designs from a device work queue, synchronise with
 // the hardware cluster barrier and reduce through distributed shared memory.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -69,6 +72,7 @@ struct cps_ctx {
   double* hdplog = nullptr;  // pinned copy
   double* ddphist = nullptr; // device, the pressure-drop gate's windows (cudaMalloc'd by cps_set_dp_monitor)
   double* dpseudo = nullptr; // device, the CFL controllers' state (4 doubles)
+  cps::TensorMap* dtmaps = nullptr;  // device, the planes' TMA tensor maps (kTmCount), or null
   double pseudo_start = 0.0; // the controllers' starting CFL number
   int ramp_steps = 0;        // inlet velocity ramp of cps_solve (0: off)
   int iter = 0;              // outer-loop iteration index of the next iteration (monitor and gate)
@@ -87,8 +91,10 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_grid_kernel
                                                                 cps::GridBarrier* bar, double* red) {
   __shared__ double smem[(Monitor ? cps::kPlaneSums : cps::kRedWidth) * 8];
   __shared__ cps::PseudoRun s_pr;
-  extern __shared__ __align__(16) char tile_smem[];
+  extern __shared__ __align__(128) char tile_smem[];
   cps::GridGroup g{bar, red, rc.status, blockIdx.x, gridDim.x, 0u, 0ull};
+  if (!cps::tile_buffer_aligned(tile_smem, rc.status)) return;
+  cps::tma_barriers_init();
   cps::load_pseudo(d, s_pr);
   __syncthreads();
   cps::SweepHint hint{2, 2};
@@ -117,9 +123,11 @@ __global__ void __launch_bounds__(cps::kThreads) cps_cluster_kernel(const cps::B
   __shared__ __align__(16) cps::BatchItem s_item;
   __shared__ cps::PseudoRun s_pr;
   __shared__ int s_next;
-  extern __shared__ __align__(16) char tile_smem[];
+  extern __shared__ __align__(128) char tile_smem[];
   cps::cg::cluster_group cl = cps::cg::this_cluster();
   cps::ClusterGroup g{redbuf, nullptr, cl.block_rank(), cl.num_blocks(), 0u};
+  if (!cps::tile_buffer_aligned(tile_smem, &results[0].status)) return;
+  cps::tma_barriers_init();
   for (;;) {
     if (g.rank == 0 && threadIdx.x == 0) s_next = atomicAdd(queue, 1);
     cl.sync();
@@ -174,11 +182,13 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_group_kerne
   __shared__ double smem[cps::kRedWidth * 8];
   __shared__ __align__(16) cps::BatchItem s_item;
   __shared__ cps::PseudoRun s_pr;
-  extern __shared__ __align__(16) char tile_smem[];
+  extern __shared__ __align__(128) char tile_smem[];
   const unsigned grp = blockIdx.x / group_ctas;
   int* slot = slots + 2 * grp;  // [0] next queue index, [1] group status before a design is assigned
   cps::GridGroup g{bars + grp, rings + (size_t)grp * cps::kRedSlots * group_ctas * cps::kRedWidth, slot + 1,
                    blockIdx.x % group_ctas, (unsigned)group_ctas, 0u, 0ull};
+  if (!cps::tile_buffer_aligned(tile_smem, &results[0].status)) return;
+  cps::tma_barriers_init();
   for (;;) {
     g.status = slot + 1;
     if (g.rank == 0 && threadIdx.x == 0) slot[0] = atomicAdd(queue, 1);
@@ -234,7 +244,9 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_wave_kernel
   __shared__ double smem[cps::kRedWidth * 8];
   __shared__ __align__(16) cps::BatchItem s_item;
   __shared__ cps::PseudoRun s_pr;
-  extern __shared__ __align__(16) char tile_smem[];
+  extern __shared__ __align__(128) char tile_smem[];
+  if (!cps::tile_buffer_aligned(tile_smem, &results[which[0]].status)) return;
+  cps::tma_barriers_init();
   int lo = 0, hi = groups;  // first[lo] <= blockIdx.x < first[lo + 1]
   while (hi - lo > 1) {
     const int mid = (lo + hi) >> 1;
@@ -314,6 +326,7 @@ size_t footprint_bytes(int M, int N, int precision, size_t* plane_elems_out, int
   bytes += (size_t)kHistChunk * 8 * 8 + 64;                               // history + plane metrics
   bytes += (size_t)kHistChunk * 4 * 8;                                    // pressure-drop log
   bytes += 64;                                                            // CFL controllers' state
+  bytes += 128 + sizeof(cps::TensorMap) * cps::kTmCount;                  // TMA tensor maps
   return round_up(bytes, 256);
 }
 
@@ -323,6 +336,86 @@ bool write_pseudo_state(cps_ctx* c, double cfl, double prev, double alpha, int c
   const double h[4] = {cfl, prev, alpha, (double)count};
   return cuda_ok(c, cudaMemcpyAsync(c->dpseudo, h, sizeof(h), cudaMemcpyHostToDevice, c->stream), "h2d") &&
          cuda_ok(c, cudaStreamSynchronize(c->stream), "h2d");
+}
+
+// ---------------------------------------------------------------------------
+// TMA tensor maps of a context's planes: one 2-D map per (plane, window shape)
+// the staged phases copy, over the plane's rows 0..rmax and columns 0..P-1,
+// with the window's box (its shared-memory pitch x rows).  Out-of-range parts
+// of a box read as zero (the phases never use them).  Built once at
+// cps_create and kept in the context's slab.
+// ---------------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+template <typename E, class W>
+bool encode_map(PFN_cuTensorMapEncodeTiled_v12000 fn, cps::TensorMap* out, const E* base, int P, int rows) {
+  static_assert(sizeof(cps::TensorMap) == sizeof(CUtensorMap), "tensor map size");
+  const cuuint64_t dims[2] = {(cuuint64_t)P, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)P * sizeof(E)};
+  const cuuint32_t box[2] = {(cuuint32_t)W::kPitch, (cuuint32_t)W::kRows};
+  const cuuint32_t estr[2] = {1, 1};
+  static_assert(W::kPitch * sizeof(E) % 16 == 0 && W::kPitch <= 256 && W::kRows <= 256, "TMA box");
+  return fn(reinterpret_cast<CUtensorMap*>(out), sizeof(E) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+            2, const_cast<E*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <typename T>
+bool fill_maps(PFN_cuTensorMapEncodeTiled_v12000 fn, const cps::DesignView& v, const cps::Inner<T>& w, int M, int P,
+               cps::TensorMap* m) {
+  using LA = cps::LayoutA;
+  using LC = cps::LayoutC<T>;
+  using LD = cps::LayoutD<T>;
+  const int R = M + 1;  // rows 0..M
+  return encode_map<double, LA::WU>(fn, m + cps::kTmU_A, v.u, P, R) &&
+         encode_map<double, LA::WU>(fn, m + cps::kTmV_A, v.v, P, R) &&
+         encode_map<double, LA::WP>(fn, m + cps::kTmP_A, v.p, P, R) &&
+         encode_map<double, LA::WA>(fn, m + cps::kTmAlpha_A, v.alpha, P, M) &&
+         encode_map<T, typename LC::WUx>(fn, m + cps::kTmXU0_C, w.xU0, P, R) &&
+         encode_map<T, typename LC::WUx>(fn, m + cps::kTmXU1_C, w.xU1, P, R) &&
+         encode_map<double, typename LC::WUd>(fn, m + cps::kTmU_C, v.u, P, R) &&
+         encode_map<double, typename LC::WUd>(fn, m + cps::kTmDE_C, v.dE, P, R) &&
+         encode_map<T, typename LC::WVx>(fn, m + cps::kTmXV0_C, w.xV0, P, R) &&
+         encode_map<T, typename LC::WVx>(fn, m + cps::kTmXV1_C, w.xV1, P, R) &&
+         encode_map<double, typename LC::WVd>(fn, m + cps::kTmV_C, v.v, P, R) &&
+         encode_map<double, typename LC::WVd>(fn, m + cps::kTmDN_C, v.dN, P, R) &&
+         encode_map<double, typename LC::WG>(fn, m + cps::kTmG_C, v.gamma, P, M) &&
+         encode_map<T, typename LD::WX>(fn, m + cps::kTmPX_D, w.px, P, R) &&
+         encode_map<double, typename LD::WO>(fn, m + cps::kTmP_D, v.p, P, R) &&
+         encode_map<double, typename LD::WO>(fn, m + cps::kTmDE_D, v.dE, P, R) &&
+         encode_map<double, typename LD::WO>(fn, m + cps::kTmUS_D, v.us, P, R) &&
+         encode_map<double, typename LD::WO>(fn, m + cps::kTmDN_D, v.dN, P, R) &&
+         encode_map<double, typename LD::WO>(fn, m + cps::kTmVS_D, v.vs, P, R) &&
+         encode_map<double, typename LD::WG>(fn, m + cps::kTmG_D, v.gamma, P, M);
+}
+
+// The context's tensor maps, or false (the staged phases then copy element by
+// element): no driver entry point, an encoding refused, or CPS_STAGING=elements
+// in the environment (the element-wise path, for comparisons).
+bool build_tensor_maps(cps_ctx* c) {
+  const char* mode = std::getenv("CPS_STAGING");
+  if (mode && std::strcmp(mode, "elements") == 0) return false;
+  PFN_cuTensorMapEncodeTiled_v12000 fn = encode_tiled();
+  if (!fn) return false;
+  cps::TensorMap h[cps::kTmCount];
+  std::memset(h, 0, sizeof(h));
+  const bool ok = c->precision == CPS_MIXED ? fill_maps<float>(fn, c->view, c->view.f32, c->M, c->P, h)
+                                            : fill_maps<double>(fn, c->view, c->view.f64, c->M, c->P, h);
+  if (!ok) return false;
+  return cudaMemcpyAsync(c->dtmaps, h, sizeof(h), cudaMemcpyHostToDevice, c->stream) == cudaSuccess &&
+         cudaStreamSynchronize(c->stream) == cudaSuccess;
 }
 
 cps_status validate(const cps_desc* d) {
@@ -639,6 +732,7 @@ cps_status cps_create(const cps_desc* d, cps_ctx** out) {
   c->dplane = c->dhist + (size_t)kHistChunk * 8;
   c->dplog = c->dplane + 8;
   c->dpseudo = c->dplog + (size_t)4 * kHistChunk;
+  c->dtmaps = reinterpret_cast<cps::TensorMap*>(round_up(reinterpret_cast<size_t>(c->dpseudo + 8), 128));
 
   cps::DesignView& v = c->view;
   v.M = d->M; v.N = d->N; v.P = c->P;
@@ -670,6 +764,7 @@ cps_status cps_create(const cps_desc* d, cps_ctx** out) {
   std::memset(&v.f32, 0, sizeof(v.f32));
   if (d->precision == CPS_MIXED) bind_inner<float>(c, v.f32); else bind_inner<double>(c, v.f64);
   set_step_inputs(c, 0.0);
+  v.tm = build_tensor_maps(c) ? c->dtmaps : nullptr;
 
   if (!upload_plane(c, v.alpha, d->alpha, d->M, d->N, d->layout) ||
       !upload_plane(c, v.gamma, d->gamma, d->M, d->N, d->layout))

@@ -47,11 +47,15 @@
 // 32 elements, so a warp's 32 consecutive j are one 256-byte (FP64) or
 // 128-byte (FP32) segment.
 //
-// Phases A, C and D stage each tile's inputs, halo included, in shared memory
-// with cp.async, kStageDepth tiles ahead; C then evaluates u*, v* and z0 once
-// per tile over the halo instead of once per neighbour.  B, P1 and P2 read
-// global memory directly.  Per-point expressions and per-thread summation
-// order are the same either way, so the results do not depend on staging.
+// Phases A, C and D (and a Jacobi sweep 2 that re-assembles its rows) stage
+// each tile's inputs, halo included, in shared memory kStageDepth tiles
+// ahead: one TMA 2-D tile copy per window (cp.async.bulk.tensor, completing
+// on the stage buffer's mbarrier; this GPU's own memory only, no multicast),
+// or element-wise cp.async for designs without tensor maps.  C then evaluates
+// u*, v* and z0 once per tile over the halo instead of once per neighbour.  B,
+// P1 and P2 read global memory directly.  Per-point expressions and
+// per-thread summation order are the same either way, so the results do not
+// depend on staging.
 #pragma once
 #include <cuda_runtime.h>
 #include <cooperative_groups.h>
@@ -78,6 +82,23 @@ constexpr int kStageDepth = 3;  // tiles whose shared-memory copies are in fligh
 #endif
 constexpr int kResidentTiles = CPS_RESIDENT_TILES;  // register-resident PCG up to this many tiles per CTA
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s
+constexpr unsigned long long kTmaTimeoutNs = 1000000000ull;      // a tile copy that has not landed after 1 s
+constexpr unsigned long long kTmaDrainNs = 10000000ull;          // then wait up to 10 ms for the copies in flight
+
+// An encoded TMA tensor map (CUtensorMap: 128 bytes, 64-byte aligned), built
+// on the host by cuTensorMapEncodeTiled and kept in device memory.
+struct alignas(64) TensorMap {
+  unsigned long long w[16];
+};
+
+// The tensor maps of a design, one per (plane, window shape) the staged
+// phases copy: phase A (and a re-assembling sweep 2), phase C, phase D.
+enum TmaMap : int {
+  kTmU_A, kTmV_A, kTmP_A, kTmAlpha_A,
+  kTmXU0_C, kTmXU1_C, kTmU_C, kTmDE_C, kTmXV0_C, kTmXV1_C, kTmV_C, kTmDN_C, kTmG_C,
+  kTmPX_D, kTmP_D, kTmDE_D, kTmUS_D, kTmDN_D, kTmVS_D, kTmG_D,
+  kTmCount
+};
 
 enum DeviceStatus : int { kStatusOk = 0, kStatusTimeout = 1, kStatusDiverged = 2 };
 
@@ -135,6 +156,9 @@ struct DesignView {
   double serCFLMin, serCFLMax, serSmooth, serMaxIncrease, serMaxDecrease;
   double lsAlphaMin, lsAlphaReduce, lsTol;
   double* pseudoState;    // pseudoCFL, serResidPrev, lsCurrentAlpha, lsBacktrackCount (across launches)
+  // kTmCount tensor maps of this design's planes (TmaMap), or null: the staged
+  // phases then copy element by element
+  const TensorMap* tm;
 };
 
 // The CFL controllers' state while a design runs; every CTA keeps a copy in
@@ -328,6 +352,73 @@ __device__ __forceinline__ void cp_async_elem(E* smem_dst, const E* gsrc) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// mbarriers and TMA tile copies (sm_90+ PTX; CTA-local, no multicast).
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for the phase with the given parity to complete, at most `limit_ns`;
+// false when the limit passed first.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
+                                                  unsigned long long limit_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer_ns();
+  for (unsigned spins = 1;; ++spins) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((spins & 63u) == 0 && globaltimer_ns() - t0 > limit_ns) return false;
+  }
+}
+// One 2-D tile of `map` at element coordinates (x, y) into shared memory;
+// `bytes` (the box) is added to the barrier's expected transactions first.
+// x times the element size must be a multiple of 16 bytes (checked on the host
+// for every window shape).
+__device__ __forceinline__ void tma_load_2d(void* dst, const TensorMap* map, int x, int y, unsigned long long* bar,
+                                            unsigned bytes) {
+  mbar_expect_tx(bar, bytes);
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+      ::"r"(smem_u32(dst)), "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_shared() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// The CTA's stage-buffer mbarriers and the parity of each one's next phase
+// (one byte per buffer: thread 0 flips buffer b's byte while others may read
+// another buffer's).  Shared memory rather than registers, so that the
+// persistent kernels carry no extra live registers through their phases.
+__shared__ unsigned long long s_tma_bar[kStageDepth];
+__shared__ unsigned char s_tma_parity[kStageDepth];
+
+// Initialised once per launch by thread 0 (one arrival per phase: the issuing
+// thread's), made visible to the CTA and to the TMA unit.  Every persistent
+// kernel that runs the staged phases calls it first.
+__device__ __forceinline__ void tma_barriers_init() {
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < kStageDepth; ++b) {
+      mbar_init(s_tma_bar + b, 1);
+      s_tma_parity[b] = 0;
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fence_proxy_async_shared();
+  }
+  __syncthreads();
+}
 
 // ---------------------------------------------------------------------------
 // Block reduction of K values, fixed order (deterministic).  Bit k of MaxMask
@@ -548,24 +639,33 @@ struct ClusterGroup {
 // ---------------------------------------------------------------------------
 // Tile staging.  Every phase walks the CTA's tiles (kTileI x kTileJ points,
 // one point per thread) in a fixed order.  The values a tile reads, halo
-// included, are first copied into shared memory with cp.async, which holds no
-// registers while in flight; the copies of the next tile are issued before the
-// current tile is evaluated, and every point is then evaluated from shared
-// memory with the same expressions as the reference.  Within one phase no
-// point reads a value that another point of that phase writes, so staging a
-// tile ahead of the writes of the tile before it is exact.
+// included, are first copied into shared memory -- one TMA 2-D tile copy per
+// window completing on the stage buffer's mbarrier, or element-wise cp.async
+// when the design has no tensor maps -- and the copies of the next tiles are
+// issued before the current tile is evaluated; every point is then evaluated
+// from shared memory with the same expressions as the reference.  Within one
+// phase no point reads a value that another point of that phase writes, so
+// staging a tile ahead of the writes of the tile before it is exact.
+//
+// A window's rows start at a 16-byte column: tiles start at column
+// j0 = 1 + 32 t, so the first column j0 + C0 of a window sits kShift elements
+// into its 16-byte group for every tile, and the window is stored from column
+// j0 + C0 - kShift with a row pitch of kPitch elements (a multiple of 16 bytes).
+// That is the TMA box, whose x coordinate is then 16-byte aligned as TMA
+// requires; the element-wise copies use the same layout.
 // ---------------------------------------------------------------------------
 #define AT(a, i, j) (a)[(size_t)(i) * P + (j)]
 
 // Rows [r0, r0 + NR) x columns [c0, c0 + NC) of a pitched plane whose rows
-// 0..rmax and columns 0..P-1 exist, copied into dst[NR][NC].  Elements outside
-// the plane are not copied (and never read by the phases).
-template <int NR, int NC, typename E>
+// 0..rmax and columns 0..P-1 exist, copied element by element into dst (row
+// pitch PITCH, column c0 at SHIFT).  Elements outside the plane are not copied
+// (and never read by the phases).
+template <int NR, int NC, int PITCH, int SHIFT, typename E>
 __device__ __forceinline__ void stage_region(E* dst, const E* src, int P, int rmax, int r0, int c0) {
   for (int k = threadIdx.x; k < NR * NC; k += kThreads) {
     const int r = k / NC, c = k - r * NC;
     const int gi = r0 + r, gj = c0 + c;
-    if (gi >= 0 && gi <= rmax && gj >= 0 && gj < P) cp_async_elem(dst + k, src + (size_t)gi * P + gj);
+    if (gi >= 0 && gi <= rmax && gj >= 0 && gj < P) cp_async_elem(dst + r * PITCH + c + SHIFT, src + (size_t)gi * P + gj);
   }
 }
 
@@ -574,16 +674,32 @@ __device__ __forceinline__ void stage_region(E* dst, const E* src, int P, int rm
 template <typename E, int R0, int NR, int C0, int NC>
 struct Staged {
   using Elem = E;
-  static constexpr int kElems = NR * NC;
-  static constexpr int kPadded = (NR * NC + 3) & ~3;  // next window stays 16-byte aligned
-  static constexpr size_t kBytes = sizeof(E) * kPadded;
+  static constexpr int kAlign = 16 / (int)sizeof(E);                     // elements per 16 bytes
+  static constexpr int kShift = ((1 + C0) % kAlign + kAlign) % kAlign;    // column j0 + C0 within its 16-byte group
+  static constexpr int kPitch = (NC + kShift + kAlign - 1) / kAlign * kAlign;
+  static constexpr int kRows = NR;
+  static constexpr int kElems = NR * NC;  // logical elements
+  static constexpr unsigned kBoxBytes = (unsigned)(NR * kPitch * sizeof(E));
+  static constexpr size_t kBytes = (kBoxBytes + 127) / 128 * 128;  // the next window stays 128-byte aligned
   E* s;
   int i0, j0;
-  __device__ __forceinline__ E operator()(int i, int j) const { return s[(i - i0 - R0) * NC + (j - j0 - C0)]; }
-  __device__ __forceinline__ void stage(const E* src, int P, int rmax) const {
-    stage_region<NR, NC>(s, src, P, rmax, i0 + R0, j0 + C0);
+  __device__ __forceinline__ E operator()(int i, int j) const {
+    return s[(i - i0 - R0) * kPitch + (j - j0 - C0 + kShift)];
   }
-  // (i, j) of the k-th element, for loops that fill a window from registers
+  // the k-th logical element (row-major over NR x NC), for loops that fill a window
+  __device__ __forceinline__ E& ref(int k) const {
+    const int r = k / NC;
+    return s[r * kPitch + (k - r * NC) + kShift];
+  }
+  // the window as one TMA tile copy of `map` (issued by one thread)
+  __device__ __forceinline__ void tma(const TensorMap* map, unsigned long long* bar) const {
+    tma_load_2d(s, map, j0 + C0 - kShift, i0 + R0, bar, kBoxBytes);
+  }
+  // the window element by element (every thread of the CTA)
+  __device__ __forceinline__ void elems(const E* src, int P, int rmax) const {
+    stage_region<NR, NC, kPitch, kShift>(s, src, P, rmax, i0 + R0, j0 + C0);
+  }
+  // (i, j) of the k-th logical element
   __device__ __forceinline__ void coords(int k, int& i, int& j) const {
     const int r = k / NC;
     i = i0 + R0 + r;
@@ -591,16 +707,22 @@ struct Staged {
   }
 };
 
-// Column 0 of a plane (gamma's inlet column) for rows i0+R0 .. i0+R0+NR-1.
+// Column 0 of a plane (gamma's inlet column) for rows i0+R0 .. i0+R0+NR-1,
+// copied as the 16-byte column pair 0..1.
 template <int R0, int NR>
 struct StagedCol0 {
-  static constexpr int kPadded = (NR + 3) & ~3;
-  static constexpr size_t kBytes = sizeof(double) * kPadded;
+  static constexpr int kPitch = 2;
+  static constexpr int kRows = NR;
+  static constexpr unsigned kBoxBytes = (unsigned)(NR * kPitch * sizeof(double));
+  static constexpr size_t kBytes = (kBoxBytes + 127) / 128 * 128;
   double* s;
   int i0;
-  __device__ __forceinline__ double operator()(int row) const { return s[row - i0 - R0]; }
-  __device__ __forceinline__ void stage(const double* src, int P, int rmax) const {
-    stage_region<NR, 1>(s, src, P, rmax, i0 + R0, 0);
+  __device__ __forceinline__ double operator()(int row) const { return s[(row - i0 - R0) * kPitch]; }
+  __device__ __forceinline__ void tma(const TensorMap* map, unsigned long long* bar) const {
+    tma_load_2d(s, map, 0, i0 + R0, bar, kBoxBytes);
+  }
+  __device__ __forceinline__ void elems(const double* src, int P, int rmax) const {
+    stage_region<NR, 1, kPitch, 0>(s, src, P, rmax, i0 + R0, 0);
   }
 };
 
@@ -623,38 +745,82 @@ struct Carver {
 
 // Walk the CTA's tiles t = rank, rank + nblk, ... (the order every phase uses
 // for its per-thread sums).  Layout(buffer, i0, j0) names the tile's windows;
-// stage(L) issues the copies; compute(L, i, j, inside) evaluates the thread's
-// point (i, j) (inside: the point lies in 1..M-1 x 1..N-1; every thread of the
-// CTA calls compute, so compute may use __syncthreads).  kStageDepth tiles are
-// in flight.
-template <class Layout, class Stage, class Compute>
-__device__ __forceinline__ void for_each_tile(const DesignView& d, unsigned rank, unsigned nblk, char* tbuf,
-                                              Stage&& stage, Compute&& compute) {
+// with the design's tensor maps thread 0 issues a tile's copies with
+// stage_tma(L, tm, bar) and arrives on the buffer's mbarrier, else every
+// thread copies with stage_elems(L); compute(L, i, j, inside) evaluates the
+// thread's point (i, j) (inside: the point lies in 1..M-1 x 1..N-1; every
+// thread of the CTA calls compute, so compute may use __syncthreads).
+// kStageDepth tiles are in flight.  Every thread waits for a TMA buffer's
+// phase at most kTmaTimeoutNs; a copy that has not landed by then records
+// kStatusTimeout, the CTA waits up to kTmaDrainNs for its other copies in
+// flight and the walk returns false (the caller then stops).  tbuf is
+// 128-byte aligned.
+template <class Layout, class Group, class StageTma, class StageElems, class Compute>
+__device__ __forceinline__ bool for_each_tile(const DesignView& d, Group& g, char* tbuf, StageTma&& stage_tma,
+                                              StageElems&& stage_elems, Compute&& compute) {
+  const unsigned rank = g.rank, nblk = g.nblk;
   const int tilesJ = (d.N - 1 + kTileJ - 1) / kTileJ;
   const int tilesI = (d.M - 1 + kTileI - 1) / kTileI;
   const int nt = tilesI * tilesJ;
+  const TensorMap* tm = d.tm;
   auto buf = [&](int k) { return tbuf + (size_t)(k % kStageDepth) * Layout::kBytes; };
   auto at = [&](int t, int k) {
     return Layout(buf(k), 1 + (t / tilesJ) * kTileI, 1 + (t % tilesJ) * kTileJ);
   };
+  auto issue = [&](int t, int k) {
+    if (tm) {
+      if (threadIdx.x == 0) {
+        unsigned long long* bar = s_tma_bar + (k % kStageDepth);
+        stage_tma(at(t, k), tm, bar);
+        mbar_arrive(bar);
+      }
+    } else {
+      stage_elems(at(t, k));
+    }
+  };
+  if (tm) {
+    // earlier generic-proxy accesses to the buffers come before the copies
+    fence_proxy_async_shared();
+    __syncthreads();
+  }
 #pragma unroll
   for (int k = 0; k < kStageDepth - 1; ++k) {
     const int t = (int)rank + k * (int)nblk;
-    if (t < nt) stage(at(t, k));
-    cp_async_commit();
+    if (t < nt) issue(t, k);
+    if (!tm) cp_async_commit();
   }
   int k = 0;
   for (int t = (int)rank; t < nt; t += (int)nblk, ++k) {
     const int tn = t + (kStageDepth - 1) * (int)nblk;
-    if (tn < nt) stage(at(tn, k + kStageDepth - 1));
-    cp_async_commit();
-    cp_async_wait<kStageDepth - 1>();
-    __syncthreads();
+    if (tn < nt) issue(tn, k + kStageDepth - 1);
+    bool late = false;
+    if (tm) {
+      const int b = k % kStageDepth;
+      late = !mbar_wait_bounded(s_tma_bar + b, s_tma_parity[b], kTmaTimeoutNs);
+    } else {
+      cp_async_commit();
+      cp_async_wait<kStageDepth - 1>();
+    }
+    if (__syncthreads_or(late)) {
+      // a tile copy did not land: record it, wait (bounded) for this tile's
+      // and the later tiles' copies still in flight, and stop
+      if (threadIdx.x == 0 && g.status) atomicCAS(g.status, kStatusOk, kStatusTimeout);
+      for (int q = 0; q < kStageDepth; ++q)
+        if (t + q * (int)nblk < nt) {
+          const int b = (k + q) % kStageDepth;
+          mbar_wait_bounded(s_tma_bar + b, s_tma_parity[b], kTmaDrainNs);
+        }
+      return false;
+    }
     const Layout L = at(t, k);
     const int i = L.i0 + (threadIdx.x >> 5), j = L.j0 + (threadIdx.x & 31);
     compute(L, i, j, i <= d.M - 1 && j <= d.N - 1);
     __syncthreads();  // the buffer is restaged next round
+    // every thread has waited on this buffer's phase; the next wait on it is
+    // kStageDepth tiles later, after more barriers
+    if (tm && threadIdx.x == 0) s_tma_parity[k % kStageDepth] ^= 1u;
   }
+  return true;
 }
 
 // Tile iteration without staging: the same points in the same order, loads
@@ -1274,19 +1440,28 @@ struct LayoutD {
 };
 
 template <typename T, class Group>
-__device__ void correct_fields(const DesignView& d, Group& g, char* tbuf) {
+__device__ bool correct_fields(const DesignView& d, Group& g, char* tbuf) {
   const Inner<T>& w = inner<T>(d);
   const int M = d.M, N = d.N, P = d.P;
-  for_each_tile<LayoutD<T>>(
-      d, g.rank, g.nblk, tbuf,
+  return for_each_tile<LayoutD<T>>(
+      d, g, tbuf,
+      [](const LayoutD<T>& L, const TensorMap* tm, unsigned long long* bar) {
+        L.px.tma(tm + kTmPX_D, bar);
+        L.p.tma(tm + kTmP_D, bar);
+        L.dE.tma(tm + kTmDE_D, bar);
+        L.us.tma(tm + kTmUS_D, bar);
+        L.dN.tma(tm + kTmDN_D, bar);
+        L.vs.tma(tm + kTmVS_D, bar);
+        if (L.j0 == 1) L.g0.tma(tm + kTmG_D, bar);
+      },
       [&](const LayoutD<T>& L) {
-        L.px.stage(w.px, P, M);
-        L.p.stage(d.p, P, M);
-        L.dE.stage(d.dE, P, M);
-        L.us.stage(d.us, P, M);
-        L.dN.stage(d.dN, P, M);
-        L.vs.stage(d.vs, P, M);
-        if (L.j0 == 1) L.g0.stage(d.gamma, P, M - 1);
+        L.px.elems(w.px, P, M);
+        L.p.elems(d.p, P, M);
+        L.dE.elems(d.dE, P, M);
+        L.us.elems(d.us, P, M);
+        L.dN.elems(d.dN, P, M);
+        L.vs.elems(d.vs, P, M);
+        if (L.j0 == 1) L.g0.elems(d.gamma, P, M - 1);
       },
       [&](const LayoutD<T>& L, int i, int j, bool inside) {
         if (!inside) return;
@@ -1388,22 +1563,31 @@ __device__ __forceinline__ double final_velocity(double vel, T xf) {
 // residMassDof, non-finite flag (max); r.z, p.Ap (sum).
 template <typename T, class Group>
 __device__ bool mass_phase(const DesignView& d, Group& g, double* smem, char* tbuf, const T* xfU, const T* xfV,
-                           double (&rc)[7]) {
+                           int mapXU, int mapXV, double (&rc)[7]) {
   const Inner<T>& w = inner<T>(d);
   const int M = d.M, N = d.N, P = d.P;
   using L_t = LayoutC<T>;
   char* ext = tbuf + (size_t)kStageDepth * L_t::kBytes;
   const double mv = d.maxVel;
-  for_each_tile<L_t>(
-      d, g.rank, g.nblk, tbuf,
+  const bool ok = for_each_tile<L_t>(
+      d, g, tbuf,
+      [mapXU, mapXV](const L_t& L, const TensorMap* tm, unsigned long long* bar) {
+        L.xu.tma(tm + mapXU, bar);
+        L.u.tma(tm + kTmU_C, bar);
+        L.dE.tma(tm + kTmDE_C, bar);
+        L.xv.tma(tm + mapXV, bar);
+        L.v.tma(tm + kTmV_C, bar);
+        L.dN.tma(tm + kTmDN_C, bar);
+        if (L.j0 <= 2) L.g0.tma(tm + kTmG_C, bar);
+      },
       [&](const L_t& L) {
-        L.xu.stage(xfU, P, M);
-        L.u.stage(d.u, P, M);
-        L.dE.stage(d.dE, P, M);
-        L.xv.stage(xfV, P, M);
-        L.v.stage(d.v, P, M);
-        L.dN.stage(d.dN, P, M);
-        if (L.j0 <= 2) L.g0.stage(d.gamma, P, M - 1);
+        L.xu.elems(xfU, P, M);
+        L.u.elems(d.u, P, M);
+        L.dE.elems(d.dE, P, M);
+        L.xv.elems(xfV, P, M);
+        L.v.elems(d.v, P, M);
+        L.dN.elems(d.dN, P, M);
+        if (L.j0 <= 2) L.g0.elems(d.gamma, P, M - 1);
       },
       [&](const L_t& L, int i, int j, bool inside) {
         Carver c{ext};
@@ -1423,7 +1607,7 @@ __device__ bool mass_phase(const DesignView& d, Group& g, double* smem, char* tb
               val = clampd(final_velocity<T>(L.u(ii, jc), L.xu(ii, jc)), -mv, mv);
             }
           }
-          us.s[k] = val;
+          us.ref(k) = val;
         }
         for (int k = threadIdx.x; k < vs.kElems; k += kThreads) {
           int ii, jj;
@@ -1433,7 +1617,7 @@ __device__ bool mass_phase(const DesignView& d, Group& g, double* smem, char* tb
             const int jc = (jj >= N) ? N - 1 : jj;
             val = clampd(final_velocity<T>(L.v(ii, jc), L.xv(ii, jc)), -mv, mv);
           }
-          vs.s[k] = val;
+          vs.ref(k) = val;
         }
         __syncthreads();
         // z0 at every P-unknown of the tile and its one-cell ring
@@ -1456,7 +1640,7 @@ __device__ bool mass_phase(const DesignView& d, Group& g, double* smem, char* tb
             const double rr = (double)(T)b, dd = (double)(T)aP;
             z = (double)(T)((fabs(dd) > 1e-20) ? rr / dd : rr);
           }
-          z0.s[k] = z;
+          z0.ref(k) = z;
         }
         __syncthreads();
         if (!inside) return;
@@ -1522,6 +1706,7 @@ __device__ bool mass_phase(const DesignView& d, Group& g, double* smem, char* tb
           rc[6] += zc * (double)apt;
         }
       });
+  if (!ok) return false;
   return g.template sync_reduce<7, 0x1Fu>(rc, smem);
 }
 
@@ -1703,7 +1888,8 @@ __device__ bool dp_phase(const DesignView& d, Group& g, double* smem, char* tbuf
   return true;
 }
 
-// Dynamic shared memory a persistent kernel needs for storage type T.
+// Dynamic shared memory a persistent kernel needs for storage type T (the
+// tile buffers).
 template <typename T>
 constexpr size_t tile_smem_bytes() {
   constexpr size_t a = kStageDepth * LayoutA::kBytes;
@@ -1711,6 +1897,16 @@ constexpr size_t tile_smem_bytes() {
   constexpr size_t dd = kStageDepth * LayoutD<T>::kBytes;
   constexpr size_t m = a > c ? a : c;
   return m > dd ? m : dd;
+}
+
+// The kernels declare their dynamic shared memory (the tile buffers, where
+// TMA tile copies land) 128-byte aligned.  Checked once at the start of a
+// launch: a CTA whose buffer is not aligned records kStatusTimeout (the host
+// reports a failed device wait) and the launch does no work.
+__device__ __forceinline__ bool tile_buffer_aligned(const char* dyn, int* status) {
+  const bool bad = (smem_u32(dyn) & 127u) != 0;
+  if (bad && threadIdx.x == 0 && status) atomicCAS(status, kStatusOk, kStatusTimeout);
+  return !__syncthreads_or(bad);
 }
 
 // ---------------------------------------------------------------------------
@@ -1743,14 +1939,20 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
   const bool storeU = canSweep2 && (!hint || hint->kU >= 2);
   const bool storeV = canSweep2 && (!hint || hint->kV >= 2);
   double red2[2] = {0.0, 0.0};
-  for_each_tile<LayoutA>(
-      d, g.rank, g.nblk, tbuf,
-      [&](const LayoutA& L) {
-        L.u.stage(d.u, P, M);
-        L.v.stage(d.v, P, M);
-        L.p.stage(d.p, P, M);
-        L.a.stage(d.alpha, P, M - 1);
-      },
+  const auto tmaA = [](const LayoutA& L, const TensorMap* tm, unsigned long long* bar) {
+    L.u.tma(tm + kTmU_A, bar);
+    L.v.tma(tm + kTmV_A, bar);
+    L.p.tma(tm + kTmP_A, bar);
+    L.a.tma(tm + kTmAlpha_A, bar);
+  };
+  const auto elemsA = [&](const LayoutA& L) {
+    L.u.elems(d.u, P, M);
+    L.v.elems(d.v, P, M);
+    L.p.elems(d.p, P, M);
+    L.a.elems(d.alpha, P, M - 1);
+  };
+  const bool okA = for_each_tile<LayoutA>(
+      d, g, tbuf, tmaA, elemsA,
       [&](const LayoutA& L, int i, int j, bool inside) {
         if (!inside) return;
         if (expl) {
@@ -1761,7 +1963,7 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
         if (j <= N - 2) red2[0] += assemble_point<true, T, Pseudo>(d, L, i, j, anySweep, cfl, storeU);
         if (i <= M - 2) red2[1] += assemble_point<false, T, Pseudo>(d, L, i, j, anySweep, cfl, storeV);
       });
-  if (!g.template sync_reduce<2, 0u>(red2, smem)) return -1;
+  if (!okA || !g.template sync_reduce<2, 0u>(red2, smem)) return -1;
   int kU = anySweep ? 1 : 0, kV = kU;
   bool actU = anySweep && !(red2[0] < d.thrU) && kU < d.maxMomIter;
   bool actV = anySweep && !(red2[1] < d.thrV) && kV < d.maxMomIter;
@@ -1774,18 +1976,13 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
     T* xoutV = (k & 1) ? w.xV1 : w.xV0;
     double s[2] = {0.0, 0.0};
     const bool au = actU, av = actV;
+    bool okB = true;
     if (k == 2 && ((au && !storeU) || (av && !storeV))) {
       // sweep 2 of a component whose rows phase A did not store re-assembles
       // them from the same staged inputs and stores them for the sweeps after it
       const bool store = d.maxMomIter > 2;
-      for_each_tile<LayoutA>(
-          d, g.rank, g.nblk, tbuf,
-          [&](const LayoutA& L) {
-            L.u.stage(d.u, P, M);
-            L.v.stage(d.v, P, M);
-            L.p.stage(d.p, P, M);
-            L.a.stage(d.alpha, P, M - 1);
-          },
+      okB = for_each_tile<LayoutA>(
+          d, g, tbuf, tmaA, elemsA,
           [&](const LayoutA& L, int i, int j, bool inside) {
             if (!inside) return;
             if (au && j <= N - 2)
@@ -1801,7 +1998,7 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
         if (av && i <= M - 2) s[1] += sweep_point<false, T>(d, i, j, xinV, xoutV);
       });
     }
-    if (!g.template sync_reduce<2, 0u>(s, smem)) return -1;
+    if (!okB || !g.template sync_reduce<2, 0u>(s, smem)) return -1;
     if (au) { kU = k; actU = !(s[0] < d.thrU) && kU < d.maxMomIter; }
     if (av) { kV = k; actV = !(s[1] < d.thrV) && kV < d.maxMomIter; }
   }
@@ -1813,7 +2010,8 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
   const T* xfV = (kV & 1) ? w.xV1 : w.xV0;
   // ---- C: scatter, BCs, mass residual, PCG set-up ----
   double rc[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  if (!mass_phase<T>(d, g, smem, tbuf, xfU, xfV, rc)) return -1;
+  if (!mass_phase<T>(d, g, smem, tbuf, xfU, xfV, (kU & 1) ? kTmXU1_C : kTmXU0_C, (kV & 1) ? kTmXV1_C : kTmXV0_C, rc))
+    return -1;
   out[0] = rc[0];
   out[1] = rc[1];
   out[2] = rc[2];
@@ -1858,7 +2056,7 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
     out[5] = its;
   }
   // ---- D: pressure and velocity correction ----
-  correct_fields<T>(d, g, tbuf);
+  if (!correct_fields<T>(d, g, tbuf)) return -1;
   if constexpr (Monitor) {
     if (d.dpMonitor) {
       // ---- pressure-drop monitor and gate; its reduction is the barrier before the next A ----

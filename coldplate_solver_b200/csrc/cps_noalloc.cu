@@ -65,8 +65,8 @@ cps_status fail(cps_status s, const std::string& m) {
 __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_noalloc_kernel(cps::DesignView d, cps::RunControl rc,
                                                                       cps::GridBarrier* bar, double* red) {
   __shared__ double smem[cps::kRedWidth * 8];
-  extern __shared__ __align__(16) char tile_smem[];
-  cps::GridGroup g{bar, red, rc.status, blockIdx.x, gridDim.x, 0u, 0ull};
+  extern __shared__ __align__(128) char tile_smem[];
+  cps::GridGroup g{bar, red, rc.status, blockIdx.x, gridDim.x, 0u, 0ull};  // no tensor maps: element-wise staging
   cps::SweepHint hint{2, 2};
   for (int it = 0; it < rc.n_outer; ++it) {
     double out[8];
