@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_grid_kernel
   cps::tma_barriers_init();
   cps::load_pseudo(d, s_pr);
   __syncthreads();
-  cps::SweepHint hint{2, 2};
+  cps::SweepHint hint{2, 2, 2};
   for (int it = 0; it < rc.n_outer; ++it) {
     double out[8];
     const int r = cps::outer_iteration<T, cps::GridGroup, Monitor>(
@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(cps::kThreads) cps_cluster_kernel(const cps::B
     g.status = &res->status;
     double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int done = 0;
-    cps::SweepHint hint{2, 2};
+    cps::SweepHint hint{2, 2, 2};
     for (int it = 0; it < item.n_outer; ++it) {
       const int r = cps::outer_iteration<T, cps::ClusterGroup, false, Pseudo>(
           item.view, g, smem, tile_smem, out, it + 1 == item.n_outer, item.stop_on_conv != 0, item.eps, item.iter0 + it,
@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_group_kerne
     g.status = &res->status;
     double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int done = 0;
-    cps::SweepHint hint{2, 2};
+    cps::SweepHint hint{2, 2, 2};
     for (int it = 0; it < item.n_outer; ++it) {
       const int r = cps::outer_iteration<T, cps::GridGroup, false, Pseudo>(
           item.view, g, smem, tile_smem, out, it + 1 == item.n_outer, item.stop_on_conv != 0, item.eps, item.iter0 + it,
@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_wave_kernel
                    blockIdx.x - (unsigned)first[grp], (unsigned)K, 0u, 0ull};
   double out[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int done = 0;
-  cps::SweepHint hint{2, 2};
+  cps::SweepHint hint{2, 2, 2};
   for (int it = 0; it < item.n_outer; ++it) {
     const int r = cps::outer_iteration<T, cps::GridGroup, false, Pseudo>(
         item.view, g, smem, tile_smem, out, it + 1 == item.n_outer, item.stop_on_conv != 0, item.eps, item.iter0 + it,

@@ -77,6 +77,11 @@ constexpr int kRedSlots = 4;    // ring of reduction slots (grid group)
 #define CPS_MIN_BLOCKS 2
 #endif
 constexpr int kStageDepth = 3;  // tiles whose shared-memory copies are in flight at once
+// PCG with the CTA's unknowns in shared memory for designs of up to
+// SmemTiles<T> tiles per CTA (0: the global-memory PCG there).
+#ifndef CPS_SMEM_PCG
+#define CPS_SMEM_PCG 1
+#endif
 #ifndef CPS_RESIDENT_TILES
 #define CPS_RESIDENT_TILES 2
 #endif
@@ -173,6 +178,7 @@ struct PseudoRun {
 // reductions, so every thread holds the same values).
 struct SweepHint {
   int kU, kV;
+  int kP;  // the PCG's count (iterations after the first) of the last outer iteration
 };
 
 template <typename T> __device__ __forceinline__ const Inner<T>& inner(const DesignView& d);
@@ -1309,6 +1315,193 @@ __device__ int pcg_resident(const DesignView& d, Group& g, double* smem, double 
 }
 
 // ---------------------------------------------------------------------------
+// The same PCG with the CTA's unknowns in shared memory, for groups in which a
+// CTA owns more tiles than fit in registers but at most R (SmemTiles<T>): r,
+// z, p, Ap and the east/north face conductances of every point of the CTA's
+// tiles (mixed: also the diagonal and x) are loaded once, and each PCG
+// iteration then reads global memory only for the neighbours that lie in
+// another tile (the ring around each tile: z and p_{k-1}, copied with
+// cp.async for all tiles at once, each thread into halo slots only it reads).
+//   P1 reads p_{k-1} and z and writes only Ap, so no thread waits for another;
+//   P2 forms p_k = z + beta p_{k-1} at its own point with P1's expression,
+//   updates x, r, z and stores p_k and z to global memory for the other tiles.
+// FP64 forms the diagonal from the four conductances the way phase C did (the
+// stored conductances are phase C's summands, added in its order), and adds
+// alpha p to x in global memory with red.add (one rounding of x + (alpha p),
+// as P2's x + alpha p without a fused multiply-add).  The points, their order
+// and every sum are those of pcg_two_reductions, so the iterates are the same
+// bits.
+// ---------------------------------------------------------------------------
+constexpr int kHalo = 2 * kTileJ + 2 * kTileI;  // a tile's south row, north row, west column, east column
+
+template <typename T>
+struct SmemTiles {
+  static constexpr int value = sizeof(T) == 8 ? 7 : 12;
+};
+
+template <typename T, int R>
+struct PcgSmem {
+  static constexpr int kM = sizeof(T) == 4 ? R : 1;  // arrays the mixed mode keeps in addition
+  T r[R][kThreads], z[R][kThreads], p[R][kThreads], ap[R][kThreads], cE[R][kThreads], cN[R][kThreads];
+  T dg[kM][kThreads], x[kM][kThreads];
+  T zH[R][kHalo], pH[R][kHalo];      // z and p_{k-1} at the neighbours in other tiles
+  T cWH[R][kTileI], cSH[R][kTileJ];  // the west / south conductances at the tile's west / south edge
+};
+
+template <typename T, int R, class Group>
+__device__ int pcg_smem(const DesignView& d, Group& g, double* smem, char* tbuf, double rz0, double pAp0) {
+  constexpr bool kMixed = sizeof(T) == 4;
+  PcgSmem<T, R>& S = *reinterpret_cast<PcgSmem<T, R>*>(tbuf);
+  const Inner<T>& w = inner<T>(d);
+  const int M = d.M, N = d.N, P = d.P;
+  const int tilesJ = (N - 1 + kTileJ - 1) / kTileJ;
+  const int tilesI = (M - 1 + kTileI - 1) / kTileI;
+  const int nt = tilesI * tilesJ;
+  const int ty = threadIdx.x >> 5, tx = threadIdx.x & 31, th = threadIdx.x;
+  const int nk = (int)g.rank < nt ? (nt - 1 - (int)g.rank) / (int)g.nblk + 1 : 0;  // this CTA's tiles
+  T* const pg = w.pp0;  // p_k in global memory for the other tiles (read by P1 of the next iteration)
+  // the thread's point in its k-th tile; true: a pressure unknown
+  auto point = [&](int k, int& i, int& j) {
+    const int t = (int)g.rank + k * (int)g.nblk;
+    i = 1 + (t / tilesJ) * kTileI + ty;
+    j = 1 + (t % tilesJ) * kTileJ + tx;
+    return i <= M - 1 && j <= N - 2;
+  };
+  // the west / south conductances of the thread's point in tile k
+  auto cW = [&](int k, int j) -> T { return j > 1 ? (tx > 0 ? S.cE[k][th - 1] : S.cWH[k][ty]) : (T)0; };
+  auto cS = [&](int k, int i) -> T { return i > 1 ? (ty > 0 ? S.cN[k][th - kTileJ] : S.cSH[k][tx]) : (T)0; };
+  // the diagonal (pressure_solver.cpp:703-706 as phase C evaluates it)
+  auto diag = [&](int k, int i, int j) -> double {
+    if constexpr (kMixed) {
+      return (double)S.dg[k][th];
+    } else {
+      double aP = (double)S.cE[k][th] + (double)cW(k, j) + (double)S.cN[k][th] + (double)cS(k, i);
+      if (aP < 1e-20) aP = 1.0;
+      return aP;
+    }
+  };
+  // state from phase C: r0, z0, p0 = z0, A p0 and the conductances
+  for (int k = 0; k < nk; ++k) {
+    int i, j;
+    if (!point(k, i, j)) continue;
+    const size_t o = (size_t)i * P + j;
+    cp_async_elem(&S.r[k][th], w.pr + o);
+    cp_async_elem(&S.z[k][th], w.pz + o);
+    cp_async_elem(&S.p[k][th], w.pp0 + o);
+    cp_async_elem(&S.ap[k][th], w.pAp + o);
+    cp_async_elem(&S.cE[k][th], w.cx + o);
+    cp_async_elem(&S.cN[k][th], w.cy + o);
+    if constexpr (kMixed) {
+      cp_async_elem(&S.dg[k][th], w.pdiag + o);
+      S.x[k][th] = (T)0;  // phase C's x0
+    }
+    if (tx == 0 && j > 1) cp_async_elem(&S.cWH[k][ty], w.cx + o - 1);
+    if (ty == 0 && i > 1) cp_async_elem(&S.cSH[k][tx], w.cy + o - P);
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  double rz = rz0, beta = 0.0;
+  int it = 0;
+  for (; it < d.maxPIter; ++it) {
+    const double bt = beta;
+    // p = z + beta p (pressure_solver.cpp:181)
+    auto pk = [&](T zq, T pq) -> double { return (double)(T)((double)zq + bt * (double)pq); };
+    double s1[1] = {pAp0};  // iteration 0's p = z, A p and p.Ap come from phase C
+    if (it > 0) {
+      s1[0] = 0.0;
+      // the neighbours in other tiles, every tile's at once
+      for (int k = 0; k < nk; ++k) {
+        int i, j;
+        if (!point(k, i, j)) continue;
+        const size_t o = (size_t)i * P + j;
+        if (ty == 0 && i > 1) {
+          cp_async_elem(&S.zH[k][tx], w.pz + o - P);
+          cp_async_elem(&S.pH[k][tx], pg + o - P);
+        }
+        if (ty == kTileI - 1 && i < M - 1) {
+          cp_async_elem(&S.zH[k][kTileJ + tx], w.pz + o + P);
+          cp_async_elem(&S.pH[k][kTileJ + tx], pg + o + P);
+        }
+        if (tx == 0 && j > 1) {
+          cp_async_elem(&S.zH[k][2 * kTileJ + ty], w.pz + o - 1);
+          cp_async_elem(&S.pH[k][2 * kTileJ + ty], pg + o - 1);
+        }
+        if (tx == kTileJ - 1 && j + 1 <= N - 2) {
+          cp_async_elem(&S.zH[k][2 * kTileJ + kTileI + ty], w.pz + o + 1);
+          cp_async_elem(&S.pH[k][2 * kTileJ + kTileI + ty], pg + o + 1);
+        }
+      }
+      cp_async_commit();
+      cp_async_wait<0>();  // each thread reads only the halo slots it copied
+      for (int k = 0; k < nk; ++k) {
+        int i, j;
+        if (!point(k, i, j)) continue;
+        const double pc0 = pk(S.z[k][th], S.p[k][th]);
+        double Ap = 0.0;
+        if (i > 1) {
+          if (ty > 0) Ap += -(double)S.cN[k][th - kTileJ] * pk(S.z[k][th - kTileJ], S.p[k][th - kTileJ]);
+          else Ap += -(double)S.cSH[k][tx] * pk(S.zH[k][tx], S.pH[k][tx]);
+        }
+        if (j > 1) {
+          if (tx > 0) Ap += -(double)S.cE[k][th - 1] * pk(S.z[k][th - 1], S.p[k][th - 1]);
+          else Ap += -(double)S.cWH[k][ty] * pk(S.zH[k][2 * kTileJ + ty], S.pH[k][2 * kTileJ + ty]);
+        }
+        Ap += diag(k, i, j) * pc0;
+        if (j + 1 <= N - 2) {
+          const int q = 2 * kTileJ + kTileI + ty;
+          Ap += -(double)S.cE[k][th] *
+                (tx < kTileJ - 1 ? pk(S.z[k][th + 1], S.p[k][th + 1]) : pk(S.zH[k][q], S.pH[k][q]));
+        }
+        if (i < M - 1) {
+          const int q = kTileJ + tx;
+          Ap += -(double)S.cN[k][th] *
+                (ty < kTileI - 1 ? pk(S.z[k][th + kTileJ], S.p[k][th + kTileJ]) : pk(S.zH[k][q], S.pH[k][q]));
+        }
+        const T apt = (T)Ap;
+        S.ap[k][th] = apt;
+        s1[0] += pc0 * (double)apt;
+      }
+      if (!g.template sync_reduce<1, 0u>(s1, smem)) return -1;
+    }
+    const double pAp = s1[0];
+    if (fabs(pAp) < 1e-20) break;
+    const double alpha = rz / pAp;
+    double s2[2] = {0.0, 0.0};  // |r|^2, r.z
+    for (int k = 0; k < nk; ++k) {
+      int i, j;
+      if (!point(k, i, j)) continue;
+      const size_t o = (size_t)i * P + j;
+      const T pc = it > 0 ? (T)pk(S.z[k][th], S.p[k][th]) : S.p[k][th];  // p_it, as P1 formed it
+      S.p[k][th] = pc;
+      pg[o] = pc;
+      if constexpr (kMixed) {
+        const T xn = (T)((double)S.x[k][th] + alpha * (double)pc);
+        S.x[k][th] = xn;
+        w.px[o] = xn;
+      } else {
+        atomicAdd(reinterpret_cast<double*>(w.px) + o, alpha * (double)pc);  // x += alpha p (red.add)
+      }
+      const T rt = (T)((double)S.r[k][th] - alpha * (double)S.ap[k][th]);
+      S.r[k][th] = rt;
+      const double r = (double)rt;
+      s2[0] += r * r;
+      const double dgd = diag(k, i, j);
+      const T zt = (T)((fabs(dgd) > 1e-20) ? r / dgd : r);
+      S.z[k][th] = zt;
+      w.pz[o] = zt;
+      s2[1] += r * (double)zt;
+    }
+    if (!g.template sync_reduce<2, 0u>(s2, smem)) return -1;
+    if (sqrt(s2[0]) < d.pTol) break;
+    const double rzPrev = rz;
+    rz = s2[1];
+    beta = rz / rzPrev;
+  }
+  return it;
+}
+
+// ---------------------------------------------------------------------------
 // Single-reduction Jacobi-PCG (Chronopoulos-Gear recurrences), selected per
 // design by pcgSingleReduction: the same Krylov iterates as the reference's PCG in exact
 // arithmetic, with one grid-wide reduction per iteration instead of two.
@@ -1896,7 +2089,9 @@ constexpr size_t tile_smem_bytes() {
   constexpr size_t c = kStageDepth * LayoutC<T>::kBytes + LayoutC<T>::kExtraBytes;
   constexpr size_t dd = kStageDepth * LayoutD<T>::kBytes;
   constexpr size_t m = a > c ? a : c;
-  return m > dd ? m : dd;
+  constexpr size_t t = m > dd ? m : dd;
+  constexpr size_t q = CPS_SMEM_PCG ? sizeof(PcgSmem<T, SmemTiles<T>::value>) : 0;  // the PCG reuses the buffers
+  return t > q ? t : q;
 }
 
 // The kernels declare their dynamic shared memory (the tile buffers, where
@@ -2049,11 +2244,19 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
     out[5] = its;
   } else {
     const int tiles = ((M - 1 + kTileI - 1) / kTileI) * ((N - 1 + kTileJ - 1) / kTileJ);
-    const int its = (tiles <= kResidentTiles * (int)g.nblk)
-                        ? pcg_resident<T, kResidentTiles>(d, g, smem, rc[5], rc[6])
-                        : pcg_two_reductions<T>(d, g, smem, rc[5], rc[6]);
+    constexpr int kS = SmemTiles<T>::value;
+    int its;
+    if (tiles <= kResidentTiles * (int)g.nblk)
+      its = pcg_resident<T, kResidentTiles>(d, g, smem, rc[5], rc[6]);
+    else if (CPS_SMEM_PCG && tiles <= kS * (int)g.nblk && (!hint || hint->kP >= 2))
+      // the shared-memory form pays when the PCG runs several iterations (its
+      // loading costs about one); the last outer iteration's count decides
+      its = pcg_smem<T, kS>(d, g, smem, tbuf, rc[5], rc[6]);
+    else
+      its = pcg_two_reductions<T>(d, g, smem, rc[5], rc[6]);
     if (its < 0) return -1;
     out[5] = its;
+    if (hint) hint->kP = its;
   }
   // ---- D: pressure and velocity correction ----
   if (!correct_fields<T>(d, g, tbuf)) return -1;

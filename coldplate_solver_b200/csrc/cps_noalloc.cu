@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(cps::kThreads, CPS_MIN_BLOCKS) cps_noalloc_ker
   __shared__ double smem[cps::kRedWidth * 8];
   extern __shared__ __align__(128) char tile_smem[];
   cps::GridGroup g{bar, red, rc.status, blockIdx.x, gridDim.x, 0u, 0ull};  // no tensor maps: element-wise staging
-  cps::SweepHint hint{2, 2};
+  cps::SweepHint hint{2, 2, 2};
   for (int it = 0; it < rc.n_outer; ++it) {
     double out[8];
     const int r = cps::outer_iteration<double>(d, g, smem, tile_smem, out, it + 1 == rc.n_outer,
