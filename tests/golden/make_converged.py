@@ -76,6 +76,7 @@ def design_of(generator: str, args: dict):
 CASES = {
     "network_500x250": ("channel_network", {}, 1),
     "density_1000x500": ("density_field", {"Nx": 1000}, 2),
+    "density_500x250": ("density_field", {"Nx": 500}, 1),
     "mix47_258x129": ("batch_mix", {"n": 64, "k": 47}, 1),
     "served14_137x68": ("served_stream", {"n": 32, "k": 14}, 1),
 }

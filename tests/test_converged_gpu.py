@@ -3,6 +3,10 @@ workloads' designs: the 500 x 250 channel network, the 1000 x 500 density
 field, a design of the 64-design mix solved inside a batch, and a request of
 the served stream solved through the serving loop (mixed precision).
 
+Designs: the 500 x 250 channel network, the density-field generator at
+1000 x 500 and at 500 x 250 (FP64 and mixed precision), a design of the
+64-design mix solved inside a batch, and a request of the served stream.
+
 The oracle is the reference's own code (its sources promoted to double):
 from the zero state to its 1e-6 stop with the design's settings, then on to
 the 1e-10 outer residual with tight inner tolerances (the fixtures' ``tight``:
@@ -85,8 +89,9 @@ def assert_fixed_point(d, z, fields, dp):
     assert abs(dp - dpr) <= REL_DP * abs(dpr), (dp, dpr)
 
 
-@pytest.mark.parametrize("name,precision", [("network_500x250", cps.CPS_FP64), ("density_1000x500", cps.CPS_FP64),
-                                            ("network_500x250", cps.CPS_MIXED)])
+@pytest.mark.parametrize("name,precision", [("network_500x250", cps.CPS_FP64), ("network_500x250", cps.CPS_MIXED),
+                                            ("density_500x250", cps.CPS_FP64), ("density_500x250", cps.CPS_MIXED),
+                                            ("density_1000x500", cps.CPS_FP64)])
 def test_single_design_reaches_the_reference_fixed_point(name, precision):
     """The design's own settings to the 1e-6 stop, then, from that state, the
     tight inner tolerances to 1e-10 (a context with those settings)."""
