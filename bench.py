@@ -838,7 +838,15 @@ def run_many(args) -> None:
     torch.cuda.set_device(device)
     designs, arrivals, cfg = many_designs(args)
     precision = cps.CPS_MIXED if args.precision == "mixed" else cps.CPS_FP64
-    mode = batch.default_mode(device) if args.placement == "default" else json.loads(args.placement)
+    tuned = None
+    if args.placement == "auto" and args.workload == "mix":
+        # the project's autotuner: placement from zero- and warm-state probes,
+        # visit length from converged solves of a sample (untimed)
+        tuned = batch.autotune(designs, precision, device)
+        mode, args.visit = tuned.mode, tuned.visit
+    else:
+        mode = (batch.default_mode(device) if args.placement in ("default", "auto")
+                else json.loads(args.placement))
     n = len(designs)
     clocks = None
     oracle_err = None
@@ -978,6 +986,10 @@ def run_many(args) -> None:
     }
     if oracle_err:
         line["error_vs_fp64_oracle"] = oracle_err
+    if tuned is not None:
+        line["config"]["autotuned"] = {"placement": tuned.mode, "visit": tuned.visit,
+                                       "cell_updates_per_s": tuned.cell_updates_per_s,
+                                       "visit_device_ms": {str(k): v for k, v in tuned.visit_ms.items()}}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -1020,8 +1032,10 @@ def main() -> None:
     ap.add_argument("--designs", type=int, default=64, help="mix: designs of the 64-design mix to solve")
     ap.add_argument("--requests", type=int, default=32, help="served: requests in the stream")
     ap.add_argument("--visit", type=int, default=4096, help="mix/served: outer iterations per design per launch")
-    ap.add_argument("--placement", default="default",
-                    help='mix/served: JSON placement, e.g. \'{"group_ctas": 148}\' or \'{"tiles_per_cta": 8}\'')
+    ap.add_argument("--placement", default="auto",
+                    help='mix/served: "auto" (mix: the autotuner picks the placement and the visit length; '
+                         'served: the default placement), "default", or a JSON placement, e.g. '
+                         '\'{"group_ctas": 148}\' or \'{"tiles_per_cta": 8}\'')
     ap.add_argument("--thermal-nx", type=int, default=1000,
                     help="thermal: cells in x of the density-field design (y = x/2); 500 for small profiling captures")
     ap.add_argument("--max-outer", type=int, default=MAX_OUTER,

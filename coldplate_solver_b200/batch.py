@@ -11,8 +11,10 @@ once, and the designs in flight share the 126 MB L2) and the number of outer
 iterations a design runs per launch (its "visit": long visits amortise the
 launch, short ones let the host retire converged designs and admit new ones
 sooner).  :func:`autotune` times short visits of a sample of the actual
-designs for each candidate placement and keeps the fastest in cell-updates
-per second; results are cached per size bucket.
+designs for each candidate placement, from the zero state and from a warm
+state, keeps the fastest in cell-updates per second, and then picks the visit
+length by solving the sample to convergence once per candidate length;
+results are cached per size bucket.
 """
 from __future__ import annotations
 
@@ -63,17 +65,29 @@ def size_bucket(cells: float) -> int:
 @dataclass
 class TuneResult:
     mode: dict
-    cell_updates_per_s: Dict[str, float] = field(default_factory=dict)
+    visit: int = 4096
+    cell_updates_per_s: Dict[str, float] = field(default_factory=dict)  # per placement, zero + warm states
+    visit_ms: Dict[int, float] = field(default_factory=dict)  # device ms of the sample's converged solves per visit
 
 
 _CACHE: Dict[Tuple[int, int, int], TuneResult] = {}
 
 
-def autotune(designs: Sequence[Design], precision: int = cps.CPS_FP64, device: int = 0, sample: int = 8,
-             visit: int = 60, candidates: Optional[Sequence[dict]] = None, use_cache: bool = True) -> TuneResult:
-    """Pick the placement with the highest cell-updates/s on a sample of
-    ``designs`` (``visit`` outer iterations each, from the zero state, after a
-    short warm-up)."""
+def autotune(designs: Sequence[Design], precision: int = cps.CPS_FP64, device: int = 0, sample: int = 6,
+             probe: int = 200, warm: int = 1500, visits: Sequence[int] = (512, 2048, 8192),
+             candidates: Optional[Sequence[dict]] = None, eps: float = 1e-6, max_outer: int = 200000,
+             use_cache: bool = True) -> TuneResult:
+    """Pick the placement and the visit length for ``designs``.
+
+    Placement: every candidate runs ``probe`` outer iterations of a sample of
+    the designs twice, from the zero state (the early iterations, PCG at its
+    cap) and from the state after ``warm`` iterations (the regime that most of
+    a solve spends its iterations in); the placement with the most
+    cell-updates per second over both wins.  Visit: with that placement the
+    sample is solved to ``eps`` from the zero state once per candidate length,
+    converged designs leaving between launches as in :class:`BatchRunner`; the
+    length with the least device time wins.  Results are cached per size
+    bucket, precision and sample size."""
     cells = float(np.median([d.M * d.N for d in designs]))
     key = (size_bucket(cells), precision, min(sample, len(designs)))
     if use_cache and key in _CACHE:
@@ -85,24 +99,41 @@ def autotune(designs: Sequence[Design], precision: int = cps.CPS_FP64, device: i
     solvers = [cps.Solver(d, precision=precision, device=device) for d in chosen]
     rates: Dict[str, float] = {}
     best, best_rate = cands[0], -1.0
+    visit_ms: Dict[int, float] = {}
     try:
-        cps.batch_solve(solvers, 2, eps=0.0, **cands[0])  # warm-up (module load, first touch)
+        # the warm states, once
+        warm_fields = []
+        for s in solvers:
+            s.reset_fields()
+            s.solve(warm, eps=0.0)
+            warm_fields.append(s.download())
+        cps.batch_solve(solvers, 2, eps=0.0, **cands[0])  # module load, first touch
         for mode in cands:
-            for s in solvers:
-                s.reset_fields()
+            work, ms_total = 0.0, 0.0
             try:
-                res, ms = cps.batch_solve(solvers, visit, eps=0.0, **mode)
+                for start in ("zero", "warm"):
+                    for s, f in zip(solvers, warm_fields):
+                        s.reset_fields()
+                        if start == "warm":
+                            s.upload_fields(f["u"], f["v"], f["p"])
+                    res, ms = cps.batch_solve(solvers, probe, eps=0.0, **mode)
+                    work += sum(r["n_done"] * s.design.M * s.design.N for r, s in zip(res, solvers))
+                    ms_total += ms
             except cps.CpsError:
                 continue  # placement does not fit this device
-            work = sum(r["n_done"] * s.design.M * s.design.N for r, s in zip(res, solvers))
-            rate = work / (ms / 1e3) if ms > 0 else 0.0
+            rate = work / (ms_total / 1e3) if ms_total > 0 else 0.0
             rates[mode_label(mode)] = rate
             if rate > best_rate:
                 best, best_rate = mode, rate
+        for v in visits:
+            with BatchRunner(chosen, precision=precision, device=device, mode=best) as br:
+                _, ms, _ = br.run(eps=eps, max_outer=max_outer, visit=int(v))
+            visit_ms[int(v)] = ms
     finally:
         for s in solvers:
             s.close()
-    out = TuneResult(mode=dict(best), cell_updates_per_s=rates)
+    out = TuneResult(mode=dict(best), visit=min(visit_ms, key=visit_ms.get) if visit_ms else 4096,
+                     cell_updates_per_s=rates, visit_ms=visit_ms)
     _CACHE[key] = out
     return out
 
@@ -169,7 +200,8 @@ def solve_batch(designs: Sequence[Design], eps: float = 1e-6, max_outer: int = 2
     """Solve all designs to ``eps`` (placement ``mode`` or the autotuner's);
     returns (per-design results, device ms)."""
     if mode is None:
-        mode = autotune(designs, precision, device).mode
+        tuned = autotune(designs, precision, device)
+        mode, visit = tuned.mode, tuned.visit
     with BatchRunner(designs, precision, device, mode) as runner:
         res, ms, _ = runner.run(eps=eps, max_outer=max_outer, visit=visit, reset=False)
     return res, ms
