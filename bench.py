@@ -433,8 +433,19 @@ def run_b200(args) -> None:
     stream = torch.cuda.ExternalStream(solver.stream, device=device)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
 
-    def one_solve():
+    start = None
+    if args.start_outer > 0:
+        # a late state of the solve: the state after start_outer outer iterations from zero
         solver.reset_fields()
+        solver.solve(args.start_outer, eps=0.0)
+        f = solver.download()
+        start = tuple(np.ascontiguousarray(f[k]) for k in ("u", "v", "p"))
+
+    def one_solve():
+        if start is None:
+            solver.reset_fields()
+        else:
+            solver.upload_fields(*start)
         return solver.solve(args.max_outer, eps=EPS)
 
     hist = None
@@ -490,7 +501,7 @@ def run_b200(args) -> None:
     # ---- error against the FP64 oracle's fixed point (untimed) ----
     oracle_err = None
     fx = oracle_fixture(ORACLE_FIXTURES.get(args.workload))
-    if fx is not None:
+    if fx is not None and args.max_outer >= MAX_OUTER and args.start_outer == 0:
         solver.reset_fields()
         solver.solve(args.max_outer, eps=EPS)
         oracle_err = oracle_error_block(solver, design, fx, ORACLE_FIXTURES[args.workload])
@@ -550,7 +561,8 @@ def run_b200(args) -> None:
         "data": "synthetic (seeded generator)", "impl": "b200",
         "config": dict(cfg, l2="flushed between steps (512 MiB write)", precision=args.precision,
                        outer_iterations_per_solve=iters_per_solve, converged=converged,
-                       parallelism=f"replicas x{world}"),
+                       parallelism=f"replicas x{world}",
+                       **({"start_outer": args.start_outer} if args.start_outer else {})),
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
         "cell_updates_per_s": world * design.M * design.N * sum(iters) / total_s,
         "e2e": {"value": world * e2e_steps / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d,
@@ -856,6 +868,7 @@ def run_many(args) -> None:
         # shard with the batched kernel and the per-design results are gathered
         # once at the end.
         from coldplate_solver_b200 import shard
+        pos = {id(d): k for k, d in enumerate(designs)}  # a design's index, by identity (designs hold arrays)
         mine = [designs[k] for k in shard.assign(designs, world)[rank]]
         seq_mine, _ = plain_fp64_sequential(mine, [0.0] * len(mine), device)
         stats = {"ms_total": 0.0, "launches": 0, "wall": 0.0, "e2e_s": 0.0, "h2d": 0, "d2h": 0, "clocks": None}
@@ -864,7 +877,7 @@ def run_many(args) -> None:
             """This rank's designs: warm-up visits, the timed steps, the
             untimed error check against the oracle fixtures, then one e2e run
             from host memory to converged fields on the host."""
-            idx = [designs.index(d) for d in ds]
+            idx = [pos[id(d)] for d in ds]
             with batch.BatchRunner(ds, precision=precision, device=device, mode=mode) as br:
                 for _ in range(args.warmup):  # module load, first touch; short visits from the zero state
                     br.run(eps=EPS, max_outer=100, visit=100)
@@ -904,9 +917,9 @@ def run_many(args) -> None:
         gathered = [None] * world
         if world > 1:
             import torch.distributed as dist
-            dist.all_gather_object(gathered, [(designs.index(d), r) for d, r in zip(mine, seq_mine)])
+            dist.all_gather_object(gathered, [(pos[id(d)], r) for d, r in zip(mine, seq_mine)])
         else:
-            gathered = [[(designs.index(d), r) for d, r in zip(mine, seq_mine)]]
+            gathered = [[(pos[id(d)], r) for d, r in zip(mine, seq_mine)]]
         for part in gathered:
             for k, r in part:
                 seq[k] = r
@@ -1038,6 +1051,9 @@ def main() -> None:
                          '\'{"group_ctas": 148}\' or \'{"tiles_per_cta": 8}\'')
     ap.add_argument("--thermal-nx", type=int, default=1000,
                     help="thermal: cells in x of the density-field design (y = x/2); 500 for small profiling captures")
+    ap.add_argument("--start-outer", type=int, default=0,
+                    help="straight/network/density: start every solve from the state after this many outer "
+                         "iterations from zero (small profiling captures of the late phase)")
     ap.add_argument("--max-outer", type=int, default=MAX_OUTER,
                     help="cap on outer iterations per solve (small profiling captures; the line then says converged=false)")
     args = ap.parse_args()

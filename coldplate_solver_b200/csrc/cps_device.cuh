@@ -66,8 +66,12 @@ namespace cps {
 namespace cg = cooperative_groups;
 
 constexpr int kThreads = 256;   // 8 warps
-constexpr int kTileI = 8;       // tile rows (one warp per row)
-constexpr int kTileJ = 32;      // tile columns (one lane per column)
+#ifndef CPS_TILE_J
+#define CPS_TILE_J 32
+#endif
+constexpr int kTileJ = CPS_TILE_J;         // tile columns (16, 32 or 64; consecutive threads, consecutive j)
+constexpr int kTileI = kThreads / kTileJ;  // tile rows; one point per thread
+static_assert(kTileJ == 16 || kTileJ == 32 || kTileJ == 64, "tile width");
 constexpr int kRedWidth = 8;    // doubles per CTA per reduction slot
 constexpr int kPlaneSums = 20;  // the pressure-drop monitor's reduction (own ring region)
 constexpr int kRedSlots = 4;    // ring of reduction slots (grid group)
@@ -654,7 +658,7 @@ struct ClusterGroup {
 // staging a tile ahead of the writes of the tile before it is exact.
 //
 // A window's rows start at a 16-byte column: tiles start at column
-// j0 = 1 + 32 t, so the first column j0 + C0 of a window sits kShift elements
+// j0 = 1 + kTileJ t, so the first column j0 + C0 of a window sits kShift elements
 // into its 16-byte group for every tile, and the window is stored from column
 // j0 + C0 - kShift with a row pitch of kPitch elements (a multiple of 16 bytes).
 // That is the TMA box, whose x coordinate is then 16-byte aligned as TMA
@@ -819,7 +823,7 @@ __device__ __forceinline__ bool for_each_tile(const DesignView& d, Group& g, cha
       return false;
     }
     const Layout L = at(t, k);
-    const int i = L.i0 + (threadIdx.x >> 5), j = L.j0 + (threadIdx.x & 31);
+    const int i = L.i0 + (int)threadIdx.x / kTileJ, j = L.j0 + (int)threadIdx.x % kTileJ;
     compute(L, i, j, i <= d.M - 1 && j <= d.N - 1);
     __syncthreads();  // the buffer is restaged next round
     // every thread has waited on this buffer's phase; the next wait on it is
@@ -835,7 +839,7 @@ template <class F>
 __device__ __forceinline__ void for_each_point(const DesignView& d, unsigned rank, unsigned nblk, F&& f) {
   const int tilesJ = (d.N - 1 + kTileJ - 1) / kTileJ;
   const int tilesI = (d.M - 1 + kTileI - 1) / kTileI;
-  const int ty = threadIdx.x >> 5, tx = threadIdx.x & 31;
+  const int ty = (int)threadIdx.x / kTileJ, tx = (int)threadIdx.x % kTileJ;
   for (int t = rank; t < tilesI * tilesJ; t += nblk) {
     const int i = 1 + (t / tilesJ) * kTileI + ty;
     const int j = 1 + (t % tilesJ) * kTileJ + tx;
@@ -1217,7 +1221,7 @@ __device__ int pcg_resident(const DesignView& d, Group& g, double* smem, double 
   const int tilesJ = (N - 1 + kTileJ - 1) / kTileJ;
   const int tilesI = (M - 1 + kTileI - 1) / kTileI;
   const int nt = tilesI * tilesJ;
-  const int ty = threadIdx.x >> 5, tx = threadIdx.x & 31;
+  const int ty = (int)threadIdx.x / kTileJ, tx = (int)threadIdx.x % kTileJ;
   bool on[R];
   int ii[R], jj[R];
   size_t oo[R];
@@ -1357,7 +1361,7 @@ __device__ int pcg_smem(const DesignView& d, Group& g, double* smem, char* tbuf,
   const int tilesJ = (N - 1 + kTileJ - 1) / kTileJ;
   const int tilesI = (M - 1 + kTileI - 1) / kTileI;
   const int nt = tilesI * tilesJ;
-  const int ty = threadIdx.x >> 5, tx = threadIdx.x & 31, th = threadIdx.x;
+  const int ty = (int)threadIdx.x / kTileJ, tx = (int)threadIdx.x % kTileJ, th = threadIdx.x;
   const int nk = (int)g.rank < nt ? (nt - 1 - (int)g.rank) / (int)g.nblk + 1 : 0;  // this CTA's tiles
   T* const pg = w.pp0;  // p_k in global memory for the other tiles (read by P1 of the next iteration)
   // the thread's point in its k-th tile; true: a pressure unknown
