@@ -851,11 +851,14 @@ def run_many(args) -> None:
     designs, arrivals, cfg = many_designs(args)
     precision = cps.CPS_MIXED if args.precision == "mixed" else cps.CPS_FP64
     tuned = None
+    tile_j = 32
+    if args.visit is None:
+        args.visit = 512 if args.workload == "served" else 4096
     if args.placement == "auto" and args.workload == "mix":
         # the project's autotuner: placement from zero- and warm-state probes,
         # visit length from converged solves of a sample (untimed)
         tuned = batch.autotune(designs, precision, device)
-        mode, args.visit = tuned.mode, tuned.visit
+        mode, args.visit, tile_j = tuned.mode, tuned.visit, tuned.tile_j
     else:
         mode = (batch.default_mode(device) if args.placement in ("default", "auto")
                 else json.loads(args.placement))
@@ -878,7 +881,7 @@ def run_many(args) -> None:
             untimed error check against the oracle fixtures, then one e2e run
             from host memory to converged fields on the host."""
             idx = [pos[id(d)] for d in ds]
-            with batch.BatchRunner(ds, precision=precision, device=device, mode=mode) as br:
+            with batch.BatchRunner(ds, precision=precision, device=device, mode=mode, tile_j=tile_j) as br:
                 for _ in range(args.warmup):  # module load, first touch; short visits from the zero state
                     br.run(eps=EPS, max_outer=100, visit=100)
                 with ClockSampler(device) as ck:
@@ -898,7 +901,7 @@ def run_many(args) -> None:
                         row["error_vs_fp64_oracle"] = oracle_error_block(s_, designs[k], fx, MIX_FIXTURES[k])
                     out.append(row)
             t1 = time.perf_counter()
-            with batch.BatchRunner(ds, precision=precision, device=device, mode=mode) as br2:
+            with batch.BatchRunner(ds, precision=precision, device=device, mode=mode, tile_j=tile_j) as br2:
                 br2.run(eps=EPS, max_outer=MAX_OUTER, visit=args.visit, reset=False)
                 fields = [s_.download() for s_ in br2.solvers]
             stats["e2e_s"] = time.perf_counter() - t1
@@ -940,6 +943,7 @@ def run_many(args) -> None:
         seq_ms = sum(r["ms"] for r in seq)
         srv = serve.Server(mode=mode, precision=precision, device=device, visit=args.visit, max_outer=MAX_OUTER,
                            keep=set(SERVED_FIXTURES))
+        cfg["order"] = f"{srv.order} first within every epoch"
         warm = [(0.0, d) for d in designs[: min(4, n)]]
         for _ in range(args.warmup):
             serve.Server(mode=mode, precision=precision, device=device, visit=100, max_outer=100).run(
@@ -978,6 +982,7 @@ def run_many(args) -> None:
         "dtype": "f64" if precision == cps.CPS_FP64 else "f32+f64", "data": "synthetic (seeded generator)",
         "impl": "b200",
         "config": dict(cfg, precision=args.precision, placement=mode, visit=args.visit, eps=EPS,
+                       tile=f"{256 // tile_j}x{tile_j}",
                        converged=f"{converged}/{n}", warmup="visits of 100 outer iterations per design",
                        l2="working set larger than L2 (all designs resident)"),
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
@@ -1001,7 +1006,10 @@ def run_many(args) -> None:
         line["error_vs_fp64_oracle"] = oracle_err
     if tuned is not None:
         line["config"]["autotuned"] = {"placement": tuned.mode, "visit": tuned.visit,
+                                       "tile": f"{256 // tuned.tile_j}x{tuned.tile_j}",
                                        "cell_updates_per_s": tuned.cell_updates_per_s,
+                                       "tile_cell_updates_per_s": {f"{256 // k}x{k}": v for k, v in
+                                                                   tuned.tile_cell_updates_per_s.items()},
                                        "visit_device_ms": {str(k): v for k, v in tuned.visit_ms.items()}}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -1044,7 +1052,9 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--designs", type=int, default=64, help="mix: designs of the 64-design mix to solve")
     ap.add_argument("--requests", type=int, default=32, help="served: requests in the stream")
-    ap.add_argument("--visit", type=int, default=4096, help="mix/served: outer iterations per design per launch")
+    ap.add_argument("--visit", type=int, default=None,
+                    help="mix/served: outer iterations per design per launch (default: mix 4096 or the autotuner's; "
+                         "served 512)")
     ap.add_argument("--placement", default="auto",
                     help='mix/served: "auto" (mix: the autotuner picks the placement and the visit length; '
                          'served: the default placement), "default", or a JSON placement, e.g. '

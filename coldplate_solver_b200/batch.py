@@ -10,11 +10,13 @@ more CTAs shorten one design's phases, fewer CTAs let more designs run at
 once, and the designs in flight share the 126 MB L2) and the number of outer
 iterations a design runs per launch (its "visit": long visits amortise the
 launch, short ones let the host retire converged designs and admit new ones
-sooner).  :func:`autotune` times short visits of a sample of the actual
-designs for each candidate placement, from the zero state and from a warm
-state, keeps the fastest in cell-updates per second, and then picks the visit
-length by solving the sample to convergence once per candidate length;
-results are cached per size bucket.
+sooner), and the tile shape (8 x 32, 16 x 16 or 4 x 64 points per tile, one
+library per shape: the halo a tile stages and the tiles a CTA walks).
+:func:`autotune` times short visits of a sample of the actual designs for each
+candidate placement, from the zero state and from a warm state, keeps the
+fastest in cell-updates per second, times the other tile shapes with that
+placement the same way, and then picks the visit length by solving the sample
+to convergence once per candidate length; results are cached per size bucket.
 """
 from __future__ import annotations
 
@@ -66,28 +68,48 @@ def size_bucket(cells: float) -> int:
 class TuneResult:
     mode: dict
     visit: int = 4096
+    tile_j: int = 32
     cell_updates_per_s: Dict[str, float] = field(default_factory=dict)  # per placement, zero + warm states
+    tile_cell_updates_per_s: Dict[int, float] = field(default_factory=dict)  # per tile width, chosen placement
     visit_ms: Dict[int, float] = field(default_factory=dict)  # device ms of the sample's converged solves per visit
 
 
 _CACHE: Dict[Tuple[int, int, int], TuneResult] = {}
 
 
+def _probe_rate(solvers, warm_fields, probe: int, mode: dict) -> float:
+    """Cell-updates per second of ``probe`` outer iterations of the sample
+    from the zero state and from its warm states, with placement ``mode``."""
+    work, ms_total = 0.0, 0.0
+    for start in ("zero", "warm"):
+        for s, f in zip(solvers, warm_fields):
+            s.reset_fields()
+            if start == "warm":
+                s.upload_fields(f["u"], f["v"], f["p"])
+        res, ms = cps.batch_solve(solvers, probe, eps=0.0, **mode)
+        work += sum(r["n_done"] * s.design.M * s.design.N for r, s in zip(res, solvers))
+        ms_total += ms
+    return work / (ms_total / 1e3) if ms_total > 0 else 0.0
+
+
 def autotune(designs: Sequence[Design], precision: int = cps.CPS_FP64, device: int = 0, sample: int = 6,
              probe: int = 200, warm: int = 1500, visits: Sequence[int] = (512, 2048, 8192),
-             candidates: Optional[Sequence[dict]] = None, eps: float = 1e-6, max_outer: int = 200000,
-             use_cache: bool = True) -> TuneResult:
-    """Pick the placement and the visit length for ``designs``.
+             candidates: Optional[Sequence[dict]] = None, tile_widths: Sequence[int] = cps.TILE_WIDTHS,
+             eps: float = 1e-6, max_outer: int = 200000, use_cache: bool = True) -> TuneResult:
+    """Pick the placement, the tile shape and the visit length for ``designs``.
 
     Placement: every candidate runs ``probe`` outer iterations of a sample of
     the designs twice, from the zero state (the early iterations, PCG at its
     cap) and from the state after ``warm`` iterations (the regime that most of
     a solve spends its iterations in); the placement with the most
-    cell-updates per second over both wins.  Visit: with that placement the
-    sample is solved to ``eps`` from the zero state once per candidate length,
-    converged designs leaving between launches as in :class:`BatchRunner`; the
-    length with the least device time wins.  Results are cached per size
-    bucket, precision and sample size."""
+    cell-updates per second over both wins.  Tile shape: with that placement
+    every width of ``tile_widths`` is timed the same way (the 8 x 32 default
+    included; a shape's warm states are its own, the same states to rounding).
+    Visit: with that placement and shape the sample is solved to ``eps`` from
+    the zero state once per candidate length, converged designs leaving
+    between launches as in :class:`BatchRunner`; the length with the least
+    device time wins.  Results are cached per size bucket, precision and
+    sample size."""
     cells = float(np.median([d.M * d.N for d in designs]))
     key = (size_bucket(cells), precision, min(sample, len(designs)))
     if use_cache and key in _CACHE:
@@ -96,44 +118,61 @@ def autotune(designs: Sequence[Design], precision: int = cps.CPS_FP64, device: i
     rng = np.random.default_rng(0)
     idx = rng.choice(len(designs), size=min(sample, len(designs)), replace=False)
     chosen = [designs[int(k)] for k in idx]
-    solvers = [cps.Solver(d, precision=precision, device=device) for d in chosen]
     rates: Dict[str, float] = {}
+    tile_rates: Dict[int, float] = {}
     best, best_rate = cands[0], -1.0
     visit_ms: Dict[int, float] = {}
-    try:
-        # the warm states, once
+
+    def sample_at(tile_j: int):
+        solvers = [cps.Solver(d, precision=precision, device=device, tile_j=tile_j) for d in chosen]
         warm_fields = []
         for s in solvers:
             s.reset_fields()
             s.solve(warm, eps=0.0)
             warm_fields.append(s.download())
+        return solvers, warm_fields
+
+    solvers, warm_fields = sample_at(32)
+    try:
         cps.batch_solve(solvers, 2, eps=0.0, **cands[0])  # module load, first touch
         for mode in cands:
-            work, ms_total = 0.0, 0.0
             try:
-                for start in ("zero", "warm"):
-                    for s, f in zip(solvers, warm_fields):
-                        s.reset_fields()
-                        if start == "warm":
-                            s.upload_fields(f["u"], f["v"], f["p"])
-                    res, ms = cps.batch_solve(solvers, probe, eps=0.0, **mode)
-                    work += sum(r["n_done"] * s.design.M * s.design.N for r, s in zip(res, solvers))
-                    ms_total += ms
+                rate = _probe_rate(solvers, warm_fields, probe, mode)
             except cps.CpsError:
                 continue  # placement does not fit this device
-            rate = work / (ms_total / 1e3) if ms_total > 0 else 0.0
             rates[mode_label(mode)] = rate
             if rate > best_rate:
                 best, best_rate = mode, rate
-        for v in visits:
-            with BatchRunner(chosen, precision=precision, device=device, mode=best) as br:
-                _, ms, _ = br.run(eps=eps, max_outer=max_outer, visit=int(v))
-            visit_ms[int(v)] = ms
     finally:
         for s in solvers:
             s.close()
+    best_tile = 32
+    if 32 in tile_widths:
+        tile_rates[32] = best_rate
+    else:
+        best_rate = -1.0
+    for tj in tile_widths:
+        if tj == 32:
+            continue
+        solvers, warm_fields = sample_at(tj)
+        try:
+            cps.batch_solve(solvers, 2, eps=0.0, **best)
+            rate = _probe_rate(solvers, warm_fields, probe, best)
+        except cps.CpsError:
+            continue
+        finally:
+            for s in solvers:
+                s.close()
+        tile_rates[tj] = rate
+        if rate > best_rate:
+            best_tile, best_rate = tj, rate
+    for v in visits:
+        with BatchRunner(chosen, precision=precision, device=device, mode=best, tile_j=best_tile) as br:
+            _, ms, _ = br.run(eps=eps, max_outer=max_outer, visit=int(v))
+        visit_ms[int(v)] = ms
     out = TuneResult(mode=dict(best), visit=min(visit_ms, key=visit_ms.get) if visit_ms else 4096,
-                     cell_updates_per_s=rates, visit_ms=visit_ms)
+                     tile_j=best_tile, cell_updates_per_s=rates, tile_cell_updates_per_s=tile_rates,
+                     visit_ms=visit_ms)
     _CACHE[key] = out
     return out
 
@@ -147,12 +186,14 @@ class BatchRunner:
     ``mode`` is the keyword of :func:`cps.batch_solve` that places designs:
     ``{"tiles_per_cta": R}`` (groups sized to each design, in waves),
     ``{"group_ctas": K}`` (groups of K CTAs of one cooperative launch) or
-    ``{"cluster_ctas": C}`` (one thread-block cluster per design)."""
+    ``{"cluster_ctas": C}`` (one thread-block cluster per design).
+    ``tile_j``: the tile shape's width (all designs of a batch share it)."""
 
     def __init__(self, designs: Sequence[Design], precision: int = cps.CPS_MIXED, device: int = 0,
-                 mode: Optional[dict] = None):
+                 mode: Optional[dict] = None, tile_j: int = 32):
         self.designs = list(designs)
-        self.solvers = [cps.Solver(d, precision=precision, device=device) for d in self.designs]
+        self.tile_j = tile_j
+        self.solvers = [cps.Solver(d, precision=precision, device=device, tile_j=tile_j) for d in self.designs]
         self.mode = dict(mode or default_mode(device))
 
     def close(self) -> None:
@@ -196,12 +237,12 @@ class BatchRunner:
 
 def solve_batch(designs: Sequence[Design], eps: float = 1e-6, max_outer: int = 200000,
                 precision: int = cps.CPS_FP64, mode: Optional[dict] = None, visit: int = 4096,
-                device: int = 0) -> Tuple[List[dict], float]:
-    """Solve all designs to ``eps`` (placement ``mode`` or the autotuner's);
-    returns (per-design results, device ms)."""
+                device: int = 0, tile_j: int = 32) -> Tuple[List[dict], float]:
+    """Solve all designs to ``eps`` (placement ``mode``, or the autotuner's
+    placement, tile shape and visit); returns (per-design results, device ms)."""
     if mode is None:
         tuned = autotune(designs, precision, device)
-        mode, visit = tuned.mode, tuned.visit
-    with BatchRunner(designs, precision, device, mode) as runner:
+        mode, visit, tile_j = tuned.mode, tuned.visit, tuned.tile_j
+    with BatchRunner(designs, precision, device, mode, tile_j=tile_j) as runner:
         res, ms, _ = runner.run(eps=eps, max_outer=max_outer, visit=visit, reset=False)
     return res, ms

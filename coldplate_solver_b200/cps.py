@@ -16,6 +16,15 @@ from .geometry import Design
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libcps.so")
+TILE_WIDTHS = (32, 16, 64)  # the tile shapes built: 8 x 32 (libcps.so), 16 x 16, 4 x 64
+
+
+def lib_path(tile_j: int = 32) -> str:
+    """The library whose kernels evaluate tiles of ``tile_j`` columns
+    (256 / tile_j rows)."""
+    if tile_j not in TILE_WIDTHS:
+        raise ValueError(f"tile width {tile_j} is not built (have {TILE_WIDTHS})")
+    return LIB_PATH if tile_j == 32 else os.path.join(_PKG, f"libcps_t{tile_j}.so")
 
 CPS_OK = 0
 CPS_ERR_ARG, CPS_ERR_OOM, CPS_ERR_CUDA, CPS_ERR_TIMEOUT, CPS_ERR_DIVERGED, CPS_ERR_STATE = -1, -2, -3, -4, -5, -6
@@ -207,16 +216,17 @@ SIGNATURES = {
     "cps_save_logs": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(CpsStepOut), _P, _P,
                                      ctypes.c_double]),
     "cps_version": (ctypes.c_char_p, []),
+    "cps_tile_shape": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
 }
 
-_lib: Optional[ctypes.CDLL] = None
+_libs: Dict[str, ctypes.CDLL] = {}
 
 
 def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
-    """Load libcps.so and bind every exported entry point (raises if missing)."""
-    global _lib
-    if _lib is not None and path == LIB_PATH:
-        return _lib
+    """Load libcps.so (or a tile-shape variant) once and bind every exported
+    entry point (raises if missing)."""
+    if path in _libs:
+        return _libs[path]
     if not os.path.exists(path):
         raise RuntimeError(f"{path} is not built; run `python -c 'import __graft_entry__ as g; g.build()'`")
     lib = ctypes.CDLL(path)
@@ -224,9 +234,18 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if path == LIB_PATH:
-        _lib = lib
+    _libs[path] = lib
     return lib
+
+
+def tile_shape(lib: Optional[ctypes.CDLL] = None) -> tuple:
+    """(rows, columns) of the tiles a library's kernels evaluate."""
+    lib = lib or load_library()
+    r, c = ctypes.c_int(0), ctypes.c_int(0)
+    st = lib.cps_tile_shape(ctypes.byref(r), ctypes.byref(c))
+    if st != CPS_OK:
+        raise CpsError(st, lib.cps_last_error(None).decode())
+    return r.value, c.value
 
 
 def _dptr(a: Optional[np.ndarray]):
@@ -277,8 +296,11 @@ class Solver:
     """
 
     def __init__(self, design: Design, precision: int = CPS_FP64, device: int = 0, grid_ctas: int = 0,
-                 pcg_variant: int = CPS_PCG_REFERENCE):
-        self.lib = load_library()
+                 pcg_variant: int = CPS_PCG_REFERENCE, tile_j: int = 32):
+        """``tile_j``: tile columns of the kernels (a library per shape, see
+        :data:`TILE_WIDTHS`); designs solved in one batch share it."""
+        self.lib = load_library(lib_path(tile_j))
+        self.tile_j = tile_j
         self.design = design
         self.precision, self.device = precision, device
         desc, keep = make_desc(design, precision, device, grid_ctas, pcg_variant)
@@ -461,6 +483,8 @@ def batch_solve(solvers, max_outer: int, eps: float = 1e-6, cluster_ctas: int = 
     if not solvers:
         return [], 0.0
     lib = solvers[0].lib
+    if any(s.lib is not lib for s in solvers):
+        raise ValueError("the designs of one batch must share one tile shape (one library)")
     n = len(solvers)
     ctxs = (_P * n)(*[s.ctx for s in solvers])
     uin = np.ascontiguousarray([s.inletVelocity if inlet_velocities is None else inlet_velocities[k]

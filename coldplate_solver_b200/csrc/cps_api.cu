@@ -644,6 +644,13 @@ extern "C" {
 
 const char* cps_version(void) { return "cps 0.2 (sm_100a)"; }
 
+cps_status cps_tile_shape(int* rows, int* cols) {
+  if (!rows || !cols) return fail(nullptr, CPS_ERR_ARG, "null output");
+  *rows = cps::kTileI;
+  *cols = cps::kTileJ;
+  return CPS_OK;
+}
+
 const char* cps_last_error(const cps_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
 
 cps_status cps_barrier_selftest(int device, int ctas, double* kernel_ms) {

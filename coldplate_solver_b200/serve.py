@@ -12,6 +12,17 @@ requests that arrived meanwhile, so new work overlaps with designs already on
 the device.  A design's result does not depend on the mix it ran in: its
 group computes exactly what it would compute alone.
 
+Order: a request is answered at the end of the epoch in which it converged,
+so an epoch that advances every in-flight design makes a small request wait
+for the visits of all the large ones.  With ``order="smallest"`` (default) an
+epoch advances only the ``epoch_designs`` smallest in-flight designs (by cell
+count: the outer iterations to converge grow with the design's size, so this
+is shortest-job-first on an estimate of the work left), as many as keep every
+group of CTAs busy; the others stay resident and wait.  ``"arrival"``
+advances every in-flight design in every epoch.  Short visits (a few hundred
+outer iterations) keep epochs short, so a converged design is answered soon
+after it converges.
+
 Latency of a request = time from its arrival to the end of the epoch in which
 it converged (queueing + admission + solve).
 """
@@ -26,6 +37,18 @@ import numpy as np
 
 from . import batch, cps
 from .geometry import Design
+
+
+def concurrent_groups(mode: dict, device: int = 0) -> int:
+    """Designs a placement advances at once: the resident CTAs (two per SM)
+    over the CTAs per design (groups sized to a design: taken as 8)."""
+    try:
+        import torch
+        sms = torch.cuda.get_device_properties(device).multi_processor_count
+    except Exception:  # noqa: BLE001 - no torch/GPU: B200 count
+        sms = 148
+    ctas = mode.get("group_ctas") or mode.get("cluster_ctas") or 0
+    return max(1, (2 * sms) // ctas) if ctas else 8
 
 
 @dataclass
@@ -65,12 +88,19 @@ class Server:
     def __init__(self, budget_bytes: float = 120e9, visit: int = 300, cluster_ctas: Optional[int] = None,
                  precision: int = cps.CPS_MIXED, device: int = 0, max_inflight: int = 256, eps: float = 1e-6,
                  max_outer: int = 200000, keep_fields: bool = False, mode: Optional[dict] = None,
-                 keep: Sequence[int] = ()):
+                 keep: Sequence[int] = (), order: str = "smallest", epoch_designs: int = 0):
         """``mode``: placement keyword of :func:`cps.batch_solve`
         (default: :func:`batch.default_mode`); ``cluster_ctas`` is shorthand
         for ``mode={"cluster_ctas": cluster_ctas}``.  ``keep_fields`` keeps
         every request's final fields (Request.fields), ``keep`` those of the
-        requests with these indices in the stream."""
+        requests with these indices in the stream.  ``order``: "smallest"
+        (an epoch advances the ``epoch_designs`` smallest in-flight designs;
+        0: twice the groups the placement runs at once) or "arrival" (every
+        in-flight design, every epoch)."""
+        if order not in ("smallest", "arrival"):
+            raise ValueError(f"order must be 'smallest' or 'arrival', not {order!r}")
+        self.order = order
+        self.epoch_designs = int(epoch_designs) if epoch_designs > 0 else 2 * concurrent_groups(mode, device)
         self.budget = int(budget_bytes)
         self.visit = visit
         if mode is None:
@@ -115,12 +145,17 @@ class Server:
                 if pending:
                     time.sleep(max(0.0, min(pending[0].arrival - (time.perf_counter() - t0), 0.05)))
                 continue
-            res, ms = cps.batch_solve([s for _, s, _ in inflight], self.visit, eps=self.eps, **self.mode)
+            if self.order == "smallest":
+                inflight.sort(key=lambda e: (e[0].design.M * e[0].design.N, e[0].rid))
+                run, waiting = inflight[:self.epoch_designs], inflight[self.epoch_designs:]
+            else:
+                run, waiting = inflight, []
+            res, ms = cps.batch_solve([s for _, s, _ in run], self.visit, eps=self.eps, **self.mode)
             epochs += 1
             device_ms += ms
             end = time.perf_counter() - t0
-            keep = []
-            for (r, s, fp), o in zip(inflight, res):
+            keep = list(waiting)
+            for (r, s, fp), o in zip(run, res):
                 r.outer_iterations += o["n_done"]
                 r.converged, r.status, r.last = o["converged"], o["status"], o["last"]
                 if r.converged or r.status != 0 or r.outer_iterations >= self.max_outer:

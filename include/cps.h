@@ -412,6 +412,14 @@ const char* cps_last_error(const cps_ctx* ctx);
 /* Library version string. */
 const char* cps_version(void);
 
+/* The tile shape this build of the library evaluates (points per tile:
+ * *rows x *cols, one point per thread of a 256-thread CTA).  The shape is a
+ * compile-time constant of the kernels; libcps.so is built with 8 x 32 tiles,
+ * libcps_t16.so with 16 x 16 and libcps_t64.so with 4 x 64, all with this same
+ * ABI.  The shape changes only which points a CTA evaluates together (and so
+ * the grouping of the grid-wide sums), not the per-point arithmetic. */
+cps_status cps_tile_shape(int* rows, int* cols);
+
 #ifdef __cplusplus
 }
 #endif

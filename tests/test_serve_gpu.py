@@ -46,6 +46,18 @@ def test_each_result_is_the_same_alone_and_in_the_mix(precision, mode):
         assert a.dp == r.dp
 
 
+def test_smallest_first_order_gives_the_arrival_order_results():
+    """The in-flight order changes only which epoch a design finishes in,
+    never what it computes."""
+    stream = small_stream(5, seed=5)
+    a = serve.Server(visit=40, keep_fields=True, max_outer=30000, order="arrival").run(stream, real_time=False)
+    b = serve.Server(visit=40, keep_fields=True, max_outer=30000, order="smallest").run(stream, real_time=False)
+    for ra, rb in zip(a.requests, b.requests):
+        assert ra.outer_iterations == rb.outer_iterations and ra.dp == rb.dp
+        for k in ("u", "v", "p"):
+            assert np.array_equal(ra.fields[k], rb.fields[k]), (ra.rid, k)
+
+
 def test_admission_respects_the_memory_budget():
     stream = small_stream(5, seed=7)
     fps = [cps.footprint(d, cps.CPS_MIXED) for _, d in stream]
@@ -68,7 +80,7 @@ def test_latency_statistics():
 
 def test_autotuner_picks_a_candidate_and_batch_solves():
     designs = [geometry.density_field(Nx=nx, seed=nx, sigma=3.0) for nx in (48, 64, 80, 96)]
-    t = batch.autotune(designs, sample=4, visit=10, use_cache=False)
+    t = batch.autotune(designs, sample=4, probe=10, warm=50, visits=(100, 400), use_cache=False)
     assert t.mode in batch.mode_candidates() and all(v > 0 for v in t.cell_updates_per_s.values())
     res, ms = batch.solve_batch(designs, eps=1e-6, max_outer=40000, mode=t.mode, visit=500)
     assert all(r["converged"] for r in res) and ms > 0
