@@ -100,12 +100,12 @@ class Server:
         if order not in ("smallest", "arrival"):
             raise ValueError(f"order must be 'smallest' or 'arrival', not {order!r}")
         self.order = order
-        self.epoch_designs = int(epoch_designs) if epoch_designs > 0 else 2 * concurrent_groups(mode, device)
         self.budget = int(budget_bytes)
         self.visit = visit
         if mode is None:
             mode = {"cluster_ctas": cluster_ctas} if cluster_ctas else batch.default_mode(device)
         self.mode = dict(mode)
+        self.epoch_designs = int(epoch_designs) if epoch_designs > 0 else 2 * concurrent_groups(self.mode, device)
         self.precision = precision
         self.device = device
         self.max_inflight = max_inflight

@@ -14,6 +14,7 @@ def test_concurrent_groups_follow_the_placement():
 
 
 def test_epoch_designs_default_and_override():
+    assert serve.Server().epoch_designs == 4  # default placement: SM-count groups
     assert serve.Server(mode={"group_ctas": 148}).epoch_designs == 4
     assert serve.Server(mode={"group_ctas": 148}, epoch_designs=3).epoch_designs == 3
 
