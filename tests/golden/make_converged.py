@@ -6,7 +6,11 @@ For each design the reference solves from the zero state to its own 1e-6
 stop (max(residU, residV, residMassDof) <= 1e-6) with the design's settings,
 and then, carrying the state (u, v, p), on to the 1e-10 residual with tight
 inner tolerances (TIGHT: PCG pTol 1e-10 with up to 1000 iterations, Jacobi
-momentumTol 1e-10).  With the reference's default inner tolerances the
+momentumTol 1e-10) -- for the density-field designs on to 1e-12 (``eps``
+below): their Brinkman-penalised solids make the outer iteration contract
+slowly (about 14 000 outer iterations per decade of residual on the 500 x 250
+design), so at residual 1e-10 the state still sits about 1e-6 from the fixed
+point in p.  With the reference's default inner tolerances the
 outer residual of these designs does not fall much below 1e-6: the PCG, held
 to an absolute ||r|| < 1e-4, takes one step per outer iteration there, and the
 residual wanders between ~3e-7 and ~4e-6 (the 1e-6 stop is one of its dips,
@@ -25,7 +29,9 @@ Stored per design:
                  core in, core out; flowArea, massFlux, avgStatic, avgDynamic,
                  avgTotal, valid), FP64
   dp_full        full inlet-outlet total-pressure drop of the fixed point
-  n_stop, n_fixed            outer iterations to 1e-6 and then on to 1e-10
+  n_stop, n_fixed            outer iterations to 1e-6 and then on to ``eps``
+  eps            the residual the second stage ran to (1e-10, 1e-12 for the
+                 density-field designs)
   stop_err_u/v/p, stop_err_dp  the reference's own 1e-6 stop state against
                  its fixed point (relative L2 on u, v and fluid-cell p,
                  relative dP): how far any run stopped at 1e-6 sits from the
@@ -36,6 +42,8 @@ Stored per design:
 Run from the repository root where the reference sources are available:
     make -C oracle ref REF=<reference checkout> && python tests/golden/make_converged.py [NAME ...]
 The fixtures are committed; the tests read them without the reference.
+``--save-state DIR`` also writes each design's full FP64 fixed point to
+DIR/<name>_fp64.npz (not committed; a starting point for a deeper stage).
 """
 from __future__ import annotations
 
@@ -72,13 +80,13 @@ def design_of(generator: str, args: dict):
     raise ValueError(generator)
 
 
-# name -> (generator, arguments, stride)
+# name -> (generator, arguments, stride, residual of the second stage)
 CASES = {
-    "network_500x250": ("channel_network", {}, 1),
-    "density_1000x500": ("density_field", {"Nx": 1000}, 2),
-    "density_500x250": ("density_field", {"Nx": 500}, 1),
-    "mix47_258x129": ("batch_mix", {"n": 64, "k": 47}, 1),
-    "served14_137x68": ("served_stream", {"n": 32, "k": 14}, 1),
+    "network_500x250": ("channel_network", {}, 1, EPS_FIXED),
+    "density_1000x500": ("density_field", {"Nx": 1000}, 2, 1e-12),
+    "density_500x250": ("density_field", {"Nx": 500}, 1, 1e-12),
+    "mix47_258x129": ("batch_mix", {"n": 64, "k": 47}, 1, EPS_FIXED),
+    "served14_137x68": ("served_stream", {"n": 32, "k": 14}, 1, EPS_FIXED),
 }
 
 
@@ -100,8 +108,8 @@ def full_dp(planes: np.ndarray) -> float:
     return float(planes[0, 4] - planes[1, 4])
 
 
-def make(name: str, threads: int) -> None:
-    generator, args, stride = CASES[name]
+def make(name: str, threads: int, save_state: str = "") -> None:
+    generator, args, stride, eps = CASES[name]
     d = design_of(generator, args)
     t0 = time.time()
     a = reference.run(d, MAX_OUTER, precision="f64", eps=EPS_STOP, stop_on_conv=True, threads=threads,
@@ -109,12 +117,16 @@ def make(name: str, threads: int) -> None:
     n_stop = len(a["err"])
     print(f"{name}: 1e-6 stop after {n_stop} outer iterations ({time.time() - t0:.0f} s)", flush=True)
     stop = {k: a[k] for k in ("u", "v", "p")}
-    b = reference.run(d.replace(**TIGHT), MAX_OUTER, precision="f64", eps=EPS_FIXED, stop_on_conv=True,
+    b = reference.run(d.replace(**TIGHT), MAX_OUTER, precision="f64", eps=eps, stop_on_conv=True,
                       threads=threads, init=stop, timeout=24 * 3600)
     n_fixed = len(b["err"])
     last = max(b["residU"][-1], b["residV"][-1], b["residMassDof"][-1])
-    if last > EPS_FIXED:
-        raise RuntimeError(f"{name}: the reference did not reach {EPS_FIXED} in {MAX_OUTER} iterations ({last})")
+    if last > eps:
+        raise RuntimeError(f"{name}: the reference did not reach {eps} in {MAX_OUTER} iterations ({last})")
+    if save_state:
+        os.makedirs(save_state, exist_ok=True)
+        np.savez_compressed(os.path.join(save_state, name + "_fp64.npz"), u=b["u"], v=b["v"], p=b["p"],
+                            residual=last, planes=b["planes"])
     mask = fluid_mask_p(d)
     dp_fixed, dp_stop = full_dp(b["planes"]), full_dp(a["planes"])
     s = stride
@@ -126,19 +138,26 @@ def make(name: str, threads: int) -> None:
         planes=b["planes"], dp_full=dp_fixed, dp_stop=dp_stop, n_stop=n_stop, n_fixed=n_fixed,
         stop_err_u=rel(a["u"], b["u"]), stop_err_v=rel(a["v"], b["v"]),
         stop_err_p=rel(a["p"][mask], b["p"][mask]), stop_err_dp=abs(dp_stop - dp_fixed) / abs(dp_fixed),
-        residual_fixed=last, threads=threads, tight=json.dumps(TIGHT), generator=generator, args=json.dumps(args))
+        residual_fixed=last, eps=eps, threads=threads, tight=json.dumps(TIGHT), generator=generator,
+        args=json.dumps(args))
     print(f"{name}: {n_stop} + {n_fixed} outer iterations, dP {dp_fixed:.9g} Pa (at the 1e-6 stop {dp_stop:.9g}), "
           f"{time.time() - t0:.0f} s", flush=True)
 
 
 def main(argv) -> None:
-    """[--threads T] [NAME ...]: OpenMP threads of the reference (default all
-    host cores; give fewer when several designs are generated at once)."""
+    """[--threads T] [--save-state DIR] [NAME ...]: OpenMP threads of the
+    reference (default all host cores; give fewer when several designs are
+    generated at once)."""
     threads = len(os.sched_getaffinity(0))
-    if argv[:1] == ["--threads"]:
-        threads, argv = int(argv[1]), argv[2:]
+    save_state = ""
+    while argv[:1] in (["--threads"], ["--save-state"]):
+        if argv[0] == "--threads":
+            threads = int(argv[1])
+        else:
+            save_state = argv[1]
+        argv = argv[2:]
     for name in (argv or CASES):
-        make(name, threads)
+        make(name, threads, save_state)
 
 
 if __name__ == "__main__":

@@ -10,8 +10,11 @@ Designs: the 500 x 250 channel network, the density-field generator at
 The oracle is the reference's own code (its sources promoted to double):
 from the zero state to its 1e-6 stop with the design's settings, then on to
 the 1e-10 outer residual with tight inner tolerances (the fixtures' ``tight``:
-PCG pTol 1e-10 with up to 1000 iterations, Jacobi momentumTol 1e-10),
-committed by tests/golden/make_converged.py.  With the default inner
+PCG pTol 1e-10 with up to 1000 iterations, Jacobi momentumTol 1e-10), on to
+1e-12 for the density-field designs (whose penalised solids make the outer
+iteration contract slowly enough that at 1e-10 the state is still ~1e-6 from
+the fixed point in p), committed by tests/golden/make_converged.py; the GPU
+runs to the same residual.  With the default inner
 tolerances these designs' outer residual wanders around 1e-6 without
 converging further, so the state at the 1e-6 stop is not a parity quantity
 (the reference differs from itself by ~1e-4 there between thread counts); the
@@ -45,6 +48,12 @@ def fixture(name):
     if not os.path.exists(path):
         pytest.skip(f"fixture {name} not generated (tests/golden/make_converged.py)")
     return np.load(path)
+
+
+def eps_of(z) -> float:
+    """The residual the fixture's second stage ran to (1e-12 for the
+    density-field designs, 1e-10 else)."""
+    return float(z["eps"]) if "eps" in z.files else EPS_FIXED
 
 
 def tight(d, z):
@@ -105,8 +114,8 @@ def test_single_design_reaches_the_reference_fixed_point(name, precision):
         f = s.download()
     with cps.Solver(tight(d, z), precision=precision) as s:
         s.upload_fields(f["u"], f["v"], f["p"])
-        h2 = s.solve(MAX_OUTER, eps=EPS_FIXED)
-        assert len(h2) < MAX_OUTER and max(h2[-1, 0], h2[-1, 1], h2[-1, 3]) <= EPS_FIXED
+        h2 = s.solve(MAX_OUTER, eps=eps_of(z))
+        assert len(h2) < MAX_OUTER and max(h2[-1, 0], h2[-1, 1], h2[-1, 3]) <= eps_of(z)
         assert_fixed_point(d, z, s.download(), s.full_dp())
 
 
