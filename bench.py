@@ -864,8 +864,13 @@ def run_many(args) -> None:
         tuned = batch.autotune(designs, precision, device)
         mode, args.visit, tile_j = tuned.mode, tuned.visit, tuned.tile_j
     else:
-        mode = (batch.default_mode(device) if args.placement in ("default", "auto")
-                else json.loads(args.placement))
+        if args.placement == "auto" and args.workload == "served":
+            # groups sized to each request (8 tiles per CTA): measured best for the
+            # served stream among SM-count groups and sized groups, with either order
+            mode = {"tiles_per_cta": 8}
+        else:
+            mode = (batch.default_mode(device) if args.placement in ("default", "auto")
+                    else json.loads(args.placement))
     n = len(designs)
     clocks = None
     oracle_err = None
@@ -946,8 +951,8 @@ def run_many(args) -> None:
         seq, seq_lat = plain_fp64_sequential(designs, arrivals, device)
         seq_ms = sum(r["ms"] for r in seq)
         srv = serve.Server(mode=mode, precision=precision, device=device, visit=args.visit, max_outer=MAX_OUTER,
-                           keep=set(SERVED_FIXTURES))
-        cfg["order"] = f"{srv.order} first within every epoch"
+                           keep=set(SERVED_FIXTURES), order="smallest", epoch_designs=args.epoch_designs)
+        cfg["order"] = f"the {srv.epoch_designs} smallest in-flight requests advance in each epoch"
         warm = [(0.0, d) for d in designs[: min(4, n)]]
         for _ in range(args.warmup):
             serve.Server(mode=mode, precision=precision, device=device, visit=100, max_outer=100).run(
@@ -1060,9 +1065,11 @@ def main() -> None:
                     help="mix/served: outer iterations per design per launch (default: mix 4096 or the autotuner's; "
                          "served 512)")
     ap.add_argument("--placement", default="auto",
-                    help='mix/served: "auto" (mix: the autotuner picks the placement and the visit length; '
-                         'served: the default placement), "default", or a JSON placement, e.g. '
+                    help='mix/served: "auto" (mix: the autotuner picks the placement, tile shape and visit length; '
+                         'served: groups of 8 tiles per CTA), "default", or a JSON placement, e.g. '
                          '\'{"group_ctas": 148}\' or \'{"tiles_per_cta": 8}\'')
+    ap.add_argument("--epoch-designs", type=int, default=12,
+                    help="served: in-flight requests one epoch advances, smallest first")
     ap.add_argument("--thermal-nx", type=int, default=1000,
                     help="thermal: cells in x of the density-field design (y = x/2); 500 for small profiling captures")
     ap.add_argument("--start-outer", type=int, default=0,

@@ -324,3 +324,24 @@ def served_stream(n: int, rate: float = 20.0, nx_range: Tuple[int, int] = (128, 
                           Ht=float(rng.uniform(200e-6, 600e-6)), twoFiveD=two, name=f"req{k}_{nx}")
         out.append((t, d))
     return out
+
+
+def flow_path_mask(design: Design) -> np.ndarray:
+    """Fluid cells (gamma > 0.5) joined through fluid cells (4-neighbours) to
+    the inlet or the outlet column, on p's index space ((M+1) x (N+1); cell
+    (i-1, j-1) of gamma is p's point (i, j)).
+
+    A fluid pocket enclosed by penalised solid exchanges mass with the rest
+    only through the creeping Brinkman flux, so the pressure level inside it
+    is a mode the SIMPLE iteration barely acts on: two states whose outer
+    residual is below 1e-12 can differ there by ~1e-6 of the pressure scale
+    (measured on the 500 x 250 density design: 613 enclosed fluid cells).
+    Pressure comparisons between solves use this mask."""
+    from scipy import ndimage
+    fluid = design.gamma[:design.M - 1, :design.N - 1] > 0.5
+    lab, _ = ndimage.label(fluid)
+    ends = np.union1d(lab[:, 0], lab[:, -1])
+    path = np.isin(lab, ends[ends > 0])
+    mask = np.zeros((design.M + 1, design.N + 1), dtype=bool)
+    mask[1:design.M, 1:design.N] = path
+    return mask
