@@ -17,8 +17,8 @@ downloaded, every step (wall clock).
 ``error_vs_fp64_oracle``: the solve's u, v, fluid-cell p and full dP against
 the reference's own FP64 fixed point of the same design (committed fixture,
 tests/golden/converged/), at the 1e-6 stop and again after the same solve is
-continued to the 1e-10 residual, beside the reference's own 1e-6 stop state
-against its fixed point.  ``cpu_baseline``: the reference's own build on the
+continued to the fixture's residual (1e-10; 1e-12 for the density-field
+designs), beside the reference's own 1e-6 stop state against its fixed point.  ``cpu_baseline``: the reference's own build on the
 host cores, on a bounded sample of the solve (timed chunks from five states
 along the trajectory), extrapolated with a per-iteration cost model linear in
 the inner iteration counts.  With --precision mixed the line also carries the
@@ -33,8 +33,9 @@ the timed region is bracketed by barriers and the max over ranks is taken.
 in [256, 1024], Ny = Nx/2) solved together by the batched persistent kernel;
 a step is the whole batch.  served: --requests Poisson arrivals (20/s) of
 density-field designs (Nx in [128, 2048]) through the serving loop (HBM
-admission, continuous batching); latency is wall clock from arrival to
-convergence.  Both lines carry the plain FP64 single-design path on the same
+admission, continuous batching, groups sized to each request, the 12 smallest
+in-flight requests advanced per epoch of 512 outer iterations); latency is
+wall clock from arrival to convergence.  Both lines carry the plain FP64 single-design path on the same
 designs, one after another, as the comparison, and the relative dP
 difference of every design against it.
 
@@ -129,9 +130,15 @@ def oracle_fixture(name):
     return np.load(path) if name and os.path.exists(path) else None
 
 
-def fluid_mask_p(design) -> np.ndarray:
+def fluid_mask_p(design, fields=None) -> np.ndarray:
+    """Fluid cells (gamma > 0.5) on p's index space; with a state, only those
+    whose pressure it determines (geometry.pressure_determined_mask: cells
+    enclosed by faces at the velocity clamp keep an arbitrary pressure)."""
+    from coldplate_solver_b200 import geometry
     mask = np.zeros((design.M + 1, design.N + 1), dtype=bool)
     mask[1:design.M, 1:design.N] = design.gamma[:design.M - 1, :design.N - 1] > 0.5
+    if fields is not None:
+        mask &= geometry.pressure_determined_mask(design, fields["u"], fields["v"])
     return mask
 
 
@@ -143,7 +150,7 @@ def errors_vs_fixture(design, fields, dp: float, fx) -> dict:
     def rel(a, b):
         nb = float(np.linalg.norm(b))
         return float(np.linalg.norm(a - b)) / nb if nb > 0 else float(np.linalg.norm(a - b))
-    mask = fluid_mask_p(design)[::st, ::st]
+    mask = fluid_mask_p(design, fields)[::st, ::st]
     out = {k: rel(fields[k][::st, ::st], fx[k].astype(np.float64)) for k in ("u", "v")}
     out["p"] = rel(fields["p"][::st, ::st][mask], fx["p"].astype(np.float64)[mask])
     out["dP"] = abs(dp - float(fx["dp_full"])) / abs(float(fx["dp_full"]))
@@ -166,16 +173,27 @@ def oracle_error_block(solver, design, fx, fixture: str, eps_fixed: float = 1e-1
         eps_fixed = float(fx["eps"])  # the residual the fixture's second stage ran to
     with cps.Solver(design.replace(**tight), precision=solver.precision, device=solver.device) as s2:
         s2.upload_fields(f["u"], f["v"], f["p"])
-        h = s2.solve(max_outer, eps=eps_fixed)
+        # in chunks; mixed precision stops at its own residual floor (~1e-10),
+        # when a chunk no longer halves the best residual
+        n, best = 0, np.inf
+        while n < max_outer:
+            h = s2.solve(min(20000, max_outer - n), eps=eps_fixed)
+            n += len(h)
+            r = float(np.min(np.maximum(np.maximum(h[:, 0], h[:, 1]), h[:, 3])))
+            done = r <= eps_fixed or r > 0.5 * best
+            best = min(best, r)
+            if done:
+                break
         at_fixed = errors_vs_fixture(design, s2.download(), s2.full_dp(), fx)
     return {"at_1e-6_stop": at_stop,
-            "at_fixed_point": dict(at_fixed, residual=eps_fixed, outer_iterations_after_stop=int(len(h)),
-                                   inner_tolerances=tight),
+            "at_fixed_point": dict(at_fixed, residual_target=eps_fixed, residual_reached=best,
+                                   outer_iterations_after_stop=int(n), inner_tolerances=tight),
             "reference_own_1e-6_stop": {"u": float(fx["stop_err_u"]), "v": float(fx["stop_err_v"]),
                                         "p": float(fx["stop_err_p"]), "dP": float(fx["stop_err_dp"])},
             "oracle": "the reference's own FP64 solve (its sources promoted to double): to its 1e-6 stop, then "
                       f"with tight inner tolerances to the {eps_fixed:g} residual; tests/golden/converged/{fixture}.npz",
-            "note": "relative L2 on u, v and fluid-cell p, relative full dP; a run stopped at 1e-6 sits about as "
+            "note": "relative L2 on u, v and fluid-cell p (where the state determines p), relative full dP; a run "
+                    "stopped at 1e-6 sits about as "
                     "far from the fixed point as the reference's own 1e-6 stop does (the residual wanders near "
                     "1e-6 with the default inner tolerances)"}
 

@@ -51,3 +51,22 @@ def test_served_stream_arrivals():
     t = [a for a, _ in s]
     assert all(b > a for a, b in zip(t, t[1:]))
     assert all(0.05 <= d.inletVelocity <= 0.3 for _, d in s)
+
+
+def test_pressure_determined_mask_leaves_out_cells_behind_clamped_faces():
+    """p points cut off from the outlet by faces at the velocity clamp
+    (3 max(|U|, 0.1), iterations.cpp:104) are not determined by a state."""
+    d = g.straight_channel(M=10, N=20)
+    u = np.zeros((d.M + 1, d.N))
+    v = np.zeros((d.M, d.N + 1))
+    assert g.pressure_determined_mask(d, u, v).all()
+    vmax = 3.0 * max(abs(d.inletVelocity), 0.1)
+    i, j = 5, 8  # the four faces of p(5, 8) at the clamp
+    u[i, j - 1] = vmax
+    u[i, j] = -vmax
+    v[i - 1, j] = vmax
+    v[i, j] = vmax
+    m = g.pressure_determined_mask(d, u, v)
+    assert not m[i, j] and m.sum() == m.size - 1
+    u[i, j] = 0.999 * vmax  # one face below the clamp joins it again
+    assert g.pressure_determined_mask(d, u, v).all()
