@@ -378,7 +378,20 @@ bool fill_maps(PFN_cuTensorMapEncodeTiled_v12000 fn, const cps::DesignView& v, c
   using LA = cps::LayoutA;
   using LC = cps::LayoutC<T>;
   using LD = cps::LayoutD<T>;
+  using LB = cps::LayoutB<T>;
   const int R = M + 1;  // rows 0..M
+  const long long ps = v.planeStride;
+  for (int q = 0; q < 5; ++q)
+    if (!encode_map<T, typename LB::WC>(fn, m + cps::kTmCU_B + q, w.cU + q * ps, P, R) ||
+        !encode_map<T, typename LB::WC>(fn, m + cps::kTmCV_B + q, w.cV + q * ps, P, R))
+      return false;
+  if (!encode_map<T, typename LB::WC>(fn, m + cps::kTmBU_B, w.bU, P, R) ||
+      !encode_map<T, typename LB::WC>(fn, m + cps::kTmBV_B, w.bV, P, R) ||
+      !encode_map<T, typename LB::WX>(fn, m + cps::kTmXU0_B, w.xU0, P, R) ||
+      !encode_map<T, typename LB::WX>(fn, m + cps::kTmXU1_B, w.xU1, P, R) ||
+      !encode_map<T, typename LB::WX>(fn, m + cps::kTmXV0_B, w.xV0, P, R) ||
+      !encode_map<T, typename LB::WX>(fn, m + cps::kTmXV1_B, w.xV1, P, R))
+    return false;
   return encode_map<double, LA::WU>(fn, m + cps::kTmU_A, v.u, P, R) &&
          encode_map<double, LA::WU>(fn, m + cps::kTmV_A, v.v, P, R) &&
          encode_map<double, LA::WP>(fn, m + cps::kTmP_A, v.p, P, R) &&
@@ -772,6 +785,12 @@ cps_status cps_create(const cps_desc* d, cps_ctx** out) {
   if (d->precision == CPS_MIXED) bind_inner<float>(c, v.f32); else bind_inner<double>(c, v.f64);
   set_step_inputs(c, 0.0);
   v.tm = build_tensor_maps(c) ? c->dtmaps : nullptr;
+  {
+    // CPS_STAGE_SWEEPS=0 in the environment: the Jacobi sweeps load straight
+    // from global memory even with tensor maps (for comparisons)
+    const char* sw = std::getenv("CPS_STAGE_SWEEPS");
+    v.stageSweeps = (sw && std::strcmp(sw, "0") == 0) ? 0 : 1;
+  }
 
   if (!upload_plane(c, v.alpha, d->alpha, d->M, d->N, d->layout) ||
       !upload_plane(c, v.gamma, d->gamma, d->M, d->N, d->layout))

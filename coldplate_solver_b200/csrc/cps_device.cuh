@@ -101,11 +101,15 @@ struct alignas(64) TensorMap {
 };
 
 // The tensor maps of a design, one per (plane, window shape) the staged
-// phases copy: phase A (and a re-assembling sweep 2), phase C, phase D.
+// phases copy: phase A (and a re-assembling sweep 2), phase C, phase D, and
+// the Jacobi sweeps of phase B (five coefficient planes, the source and the
+// two iterate buffers of each component).
 enum TmaMap : int {
   kTmU_A, kTmV_A, kTmP_A, kTmAlpha_A,
   kTmXU0_C, kTmXU1_C, kTmU_C, kTmDE_C, kTmXV0_C, kTmXV1_C, kTmV_C, kTmDN_C, kTmG_C,
   kTmPX_D, kTmP_D, kTmDE_D, kTmUS_D, kTmDN_D, kTmVS_D, kTmG_D,
+  kTmCU_B, kTmBU_B = kTmCU_B + 5, kTmXU0_B, kTmXU1_B,
+  kTmCV_B, kTmBV_B = kTmCV_B + 5, kTmXV0_B, kTmXV1_B,
   kTmCount
 };
 
@@ -168,6 +172,9 @@ struct DesignView {
   // kTmCount tensor maps of this design's planes (TmaMap), or null: the staged
   // phases then copy element by element
   const TensorMap* tm;
+  // with tensor maps: 1 stages the Jacobi sweeps' tiles too (phase B), 0 loads
+  // them straight from global memory (no tensor maps: always the latter)
+  int stageSweeps;
 };
 
 // The CFL controllers' state while a design runs; every CTA keeps a copy in
@@ -1112,9 +1119,55 @@ __device__ __forceinline__ void explicit_point(const DesignView& d, const Layout
 
 // ---------------------------------------------------------------------------
 // Phase B: Jacobi sweep k >= 2 at one unknown (jacobi_solver.cpp:49-57),
-// arithmetic in FP64 on the stored values; loads straight from global memory
-// (staging the twelve planes of a tile costs more than it saves).
+// arithmetic in FP64 on the stored values.  With tensor maps a tile's five
+// coefficient windows, its source window and its iterate window (halo 1) are
+// staged by TMA (sweep_point_staged; 7 copies per active component, issued by
+// one thread); element by element the fourteen windows cost more than they
+// save, so without tensor maps the sweep loads straight from global memory
+// (sweep_point).  Both evaluate the same expressions in the same order.
 // ---------------------------------------------------------------------------
+template <typename T>
+struct LayoutB {
+  using WC = Staged<T, 0, kTileI, 0, kTileJ>;            // a coefficient plane or the source: the tile
+  using WX = Staged<T, -1, kTileI + 2, -1, kTileJ + 2>;  // the iterate and its 1-point halo
+  static constexpr size_t kComp = 6 * WC::kBytes + WX::kBytes;
+  static constexpr size_t kBytes = 2 * kComp;
+  int i0, j0;
+  WC cu[5], bu, cv[5], bv;  // cu[k]: plane k of cU (aE, aW, aN, aS, aP), bu: bU
+  WX xu, xv;
+  __device__ __forceinline__ LayoutB(char* b, int i0_, int j0_) : i0(i0_), j0(j0_) {
+    Carver c{b};
+#pragma unroll
+    for (int k = 0; k < 5; ++k) cu[k] = c.take<WC>(i0, j0);
+    bu = c.take<WC>(i0, j0);
+    xu = c.take<WX>(i0, j0);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) cv[k] = c.take<WC>(i0, j0);
+    bv = c.take<WC>(i0, j0);
+    xv = c.take<WX>(i0, j0);
+  }
+};
+
+template <bool IsU, typename T>
+__device__ __forceinline__ double sweep_point_staged(const DesignView& d, const LayoutB<T>& L, int i, int j,
+                                                     T* __restrict__ xout) {
+  const int M = d.M, N = d.N, P = d.P;
+  const int iHi = IsU ? M - 1 : M - 2, jHi = IsU ? N - 2 : N - 1;
+  const auto* c = IsU ? L.cu : L.cv;
+  const auto& X = IsU ? L.xu : L.xv;
+  double Ax = 0.0;
+  if (i - 1 >= 1) Ax += (double)c[3](i, j) * (double)X(i - 1, j);
+  if (j - 1 >= 1) Ax += (double)c[1](i, j) * (double)X(i, j - 1);
+  const double aP = (double)c[4](i, j);
+  const double x0 = (double)X(i, j);
+  Ax += aP * x0;
+  if (j + 1 <= jHi) Ax += (double)c[0](i, j) * (double)X(i, j + 1);
+  if (i + 1 <= iHi) Ax += (double)c[2](i, j) * (double)X(i + 1, j);
+  const double r = (double)(IsU ? L.bu : L.bv)(i, j) - Ax;
+  xout[(size_t)i * P + j] = (T)(x0 + r / aP);
+  return r * r;
+}
+
 template <bool IsU, typename T>
 __device__ __forceinline__ double sweep_point(const DesignView& d, int i, int j, const T* __restrict__ xin,
                                               T* __restrict__ xout) {
@@ -2092,7 +2145,9 @@ constexpr size_t tile_smem_bytes() {
   constexpr size_t a = kStageDepth * LayoutA::kBytes;
   constexpr size_t c = kStageDepth * LayoutC<T>::kBytes + LayoutC<T>::kExtraBytes;
   constexpr size_t dd = kStageDepth * LayoutD<T>::kBytes;
-  constexpr size_t m = a > c ? a : c;
+  constexpr size_t bb = kStageDepth * LayoutB<T>::kBytes;
+  constexpr size_t m0 = a > c ? a : c;
+  constexpr size_t m = m0 > bb ? m0 : bb;
   constexpr size_t t = m > dd ? m : dd;
   constexpr size_t q = CPS_SMEM_PCG ? sizeof(PcgSmem<T, SmemTiles<T>::value>) : 0;  // the PCG reuses the buffers
   return t > q ? t : q;
@@ -2190,6 +2245,43 @@ __device__ int outer_iteration(const DesignView& d, Group& g, double* smem, char
             if (av && i <= M - 2)
               s[1] += storeV ? sweep_point<false, T>(d, i, j, xinV, xoutV)
                              : sweep2_point<false, T, Pseudo>(d, L, i, j, cfl, xinV, xoutV, store);
+          });
+    } else if (d.tm && d.stageSweeps) {
+      using LB = LayoutB<T>;
+      const long long ps = d.planeStride;
+      const int mapXU = (k & 1) ? kTmXU0_B : kTmXU1_B, mapXV = (k & 1) ? kTmXV0_B : kTmXV1_B;
+      okB = for_each_tile<LB>(
+          d, g, tbuf,
+          [au, av, mapXU, mapXV](const LB& L, const TensorMap* tm, unsigned long long* bar) {
+            if (au) {
+#pragma unroll
+              for (int q = 0; q < 5; ++q) L.cu[q].tma(tm + kTmCU_B + q, bar);
+              L.bu.tma(tm + kTmBU_B, bar);
+              L.xu.tma(tm + mapXU, bar);
+            }
+            if (av) {
+#pragma unroll
+              for (int q = 0; q < 5; ++q) L.cv[q].tma(tm + kTmCV_B + q, bar);
+              L.bv.tma(tm + kTmBV_B, bar);
+              L.xv.tma(tm + mapXV, bar);
+            }
+          },
+          [&](const LB& L) {
+            if (au) {
+              for (int q = 0; q < 5; ++q) L.cu[q].elems(w.cU + q * ps, P, M);
+              L.bu.elems(w.bU, P, M);
+              L.xu.elems(xinU, P, M);
+            }
+            if (av) {
+              for (int q = 0; q < 5; ++q) L.cv[q].elems(w.cV + q * ps, P, M);
+              L.bv.elems(w.bV, P, M);
+              L.xv.elems(xinV, P, M);
+            }
+          },
+          [&](const LB& L, int i, int j, bool inside) {
+            if (!inside) return;
+            if (au && j <= N - 2) s[0] += sweep_point_staged<true, T>(d, L, i, j, xoutU);
+            if (av && i <= M - 2) s[1] += sweep_point_staged<false, T>(d, L, i, j, xoutV);
           });
     } else {
       for_each_point(d, g.rank, g.nblk, [&](int i, int j) {
