@@ -52,10 +52,12 @@
 // ahead: one TMA 2-D tile copy per window (cp.async.bulk.tensor, completing
 // on the stage buffer's mbarrier; this GPU's own memory only, no multicast),
 // or element-wise cp.async for designs without tensor maps.  C then evaluates
-// u*, v* and z0 once per tile over the halo instead of once per neighbour.  B,
-// P1 and P2 read global memory directly.  Per-point expressions and
-// per-thread summation order are the same either way, so the results do not
-// depend on staging.
+// u*, v* and z0 once per tile over the halo instead of once per neighbour.
+// The Jacobi sweeps of B are staged by TMA as well when the design has tensor
+// maps (and read global memory directly otherwise); P1 and P2 keep their
+// state in registers or shared memory when it fits, else read global memory
+// directly.  Per-point expressions and per-thread summation order are the
+// same either way, so the results do not depend on staging.
 #pragma once
 #include <cuda_runtime.h>
 #include <cooperative_groups.h>
