@@ -786,10 +786,12 @@ cps_status cps_create(const cps_desc* d, cps_ctx** out) {
   set_step_inputs(c, 0.0);
   v.tm = build_tensor_maps(c) ? c->dtmaps : nullptr;
   {
-    // CPS_STAGE_SWEEPS=0 in the environment: the Jacobi sweeps load straight
-    // from global memory even with tensor maps (for comparisons)
+    // The Jacobi sweeps load straight from global memory: staging their tiles
+    // by TMA gave the same bits but measured 0-1.5 % slower per outer
+    // iteration (the sweeps are not bound by their loads' latency).
+    // CPS_STAGE_SWEEPS=1 in the environment stages them (for comparisons).
     const char* sw = std::getenv("CPS_STAGE_SWEEPS");
-    v.stageSweeps = (sw && std::strcmp(sw, "0") == 0) ? 0 : 1;
+    v.stageSweeps = (sw && std::strcmp(sw, "1") == 0) ? 1 : 0;
   }
 
   if (!upload_plane(c, v.alpha, d->alpha, d->M, d->N, d->layout) ||

@@ -53,8 +53,8 @@
 // on the stage buffer's mbarrier; this GPU's own memory only, no multicast),
 // or element-wise cp.async for designs without tensor maps.  C then evaluates
 // u*, v* and z0 once per tile over the halo instead of once per neighbour.
-// The Jacobi sweeps of B are staged by TMA as well when the design has tensor
-// maps (and read global memory directly otherwise); P1 and P2 keep their
+// The Jacobi sweeps of B read global memory directly (a TMA-staged form is
+// kept behind CPS_STAGE_SWEEPS=1; it measured no faster); P1 and P2 keep their
 // state in registers or shared memory when it fits, else read global memory
 // directly.  Per-point expressions and per-thread summation order are the
 // same either way, so the results do not depend on staging.
@@ -174,8 +174,8 @@ struct DesignView {
   // kTmCount tensor maps of this design's planes (TmaMap), or null: the staged
   // phases then copy element by element
   const TensorMap* tm;
-  // with tensor maps: 1 stages the Jacobi sweeps' tiles too (phase B), 0 loads
-  // them straight from global memory (no tensor maps: always the latter)
+  // with tensor maps: 1 stages the Jacobi sweeps' tiles too (phase B), 0 (the
+  // default) loads them straight from global memory (no tensor maps: always)
   int stageSweeps;
 };
 
@@ -1121,12 +1121,14 @@ __device__ __forceinline__ void explicit_point(const DesignView& d, const Layout
 
 // ---------------------------------------------------------------------------
 // Phase B: Jacobi sweep k >= 2 at one unknown (jacobi_solver.cpp:49-57),
-// arithmetic in FP64 on the stored values.  With tensor maps a tile's five
+// arithmetic in FP64 on the stored values, loaded straight from global memory
+// (sweep_point).  With tensor maps and DesignView::stageSweeps a tile's five
 // coefficient windows, its source window and its iterate window (halo 1) are
-// staged by TMA (sweep_point_staged; 7 copies per active component, issued by
-// one thread); element by element the fourteen windows cost more than they
-// save, so without tensor maps the sweep loads straight from global memory
-// (sweep_point).  Both evaluate the same expressions in the same order.
+// staged by TMA instead (sweep_point_staged; 7 copies per active component,
+// issued by one thread): the same expressions in the same order, the same
+// bits, but not faster on B200 (the sweeps are not bound by their loads'
+// latency), so it is off by default; element by element the fourteen
+// windows cost more than they save.
 // ---------------------------------------------------------------------------
 template <typename T>
 struct LayoutB {

@@ -1,9 +1,9 @@
 """The ways a phase gets its tile's inputs give the same bits: TMA 2-D tile
-copies (phases A, C, D and the Jacobi sweeps of phase B), element-wise
-cp.async copies (CPS_STAGING=elements), and, for the sweeps, direct loads
-from global memory (CPS_STAGE_SWEEPS=0).  Every form evaluates the same
-expressions on the same values in the same order, so the fields, residuals
-and inner iteration counts of a run agree exactly.  The choice is read when
+copies (phases A, C, D; the Jacobi sweeps of phase B too with
+CPS_STAGE_SWEEPS=1), element-wise cp.async copies (CPS_STAGING=elements),
+and, for the sweeps by default, direct loads from global memory.  Every form
+evaluates the same expressions on the same values in the same order, so the
+fields, residuals and inner iteration counts of a run agree exactly.  The choice is read when
 a context is created."""
 import os
 
@@ -14,7 +14,7 @@ from coldplate_solver_b200 import cps, geometry
 
 pytestmark = pytest.mark.gpu
 
-FORMS = {"tma": {}, "sweeps_direct": {"CPS_STAGE_SWEEPS": "0"}, "elements": {"CPS_STAGING": "elements"}}
+FORMS = {"tma": {}, "sweeps_tma": {"CPS_STAGE_SWEEPS": "1"}, "elements": {"CPS_STAGING": "elements"}}
 
 
 def run(design, precision, env, n):
@@ -42,7 +42,7 @@ def test_staging_forms_give_the_same_bits(name, precision):
     out = {f: run(d, precision, env, 40) for f, env in FORMS.items()}
     h0, f0 = out["tma"]
     assert h0[:, 6].max() >= 2 or h0[:, 7].max() >= 2  # the runs include phase B sweeps
-    for form in ("sweeps_direct", "elements"):
+    for form in ("sweeps_tma", "elements"):
         h, f = out[form]
         assert np.array_equal(h, h0), form
         for k in ("u", "v", "p", "pStar", "uStar", "vStar", "dE", "dN"):
