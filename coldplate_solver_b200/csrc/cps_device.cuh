@@ -517,12 +517,14 @@ struct GridGroup {
   // Publish this CTA's K values, synchronise, and combine all CTAs' values in
   // a fixed order.  Result valid in every thread of every CTA.
   //   CTA value: warp trees (shfl_xor), then the 8 warps in order.
-  //   Grid value: lane l of warp 0 folds CTAs l, l+32, ... in order, then a
-  //   warp tree.  The ring holds value k of CTA b at [k * nblk + b].
-  // Two __syncthreads per reduction: the first orders every thread's tile
-  // writes before thread 0's release (cumulativity) and hands the warp values
-  // to thread 0; the second hands the result (and thread 0's acquire, through
-  // __syncwarp in warp 0) to the whole CTA.
+  //   Grid value: lane l folds CTAs l, l+32, ... in order, then a warp tree
+  //   (warp 0 for a single value; warp k for value k when there are several).
+  //   The ring holds value k of CTA b at [k * nblk + b].
+  // Two __syncthreads per single-value reduction: the first orders every
+  // thread's tile writes before thread 0's release (cumulativity) and hands
+  // the warp values to thread 0; the second hands the result (and thread 0's
+  // acquire, through __syncwarp in warp 0) to the whole CTA.  Reductions of
+  // 2..8 values take three (see below).
   template <int K, unsigned MaxMask>
   __device__ bool sync_reduce(double (&v)[K], double* smem) {
     static_assert(K <= kRedWidth, "ring slots hold kRedWidth values per CTA");
@@ -552,6 +554,56 @@ struct GridGroup {
     }
     ++epoch;
     __syncthreads();
+    if constexpr (K >= 2 && K <= kThreads / 32) {
+      // Value k folded by warp k, all K at once: the same order per value as
+      // below (CTAs lane, lane + 32, ... then a warp tree), but one L2 round
+      // trip for the whole reduction instead of one per batch of 16/K CTAs
+      // per lane.  A third __syncthreads hands thread 0's acquire to the
+      // folding warps.
+      if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          double a = smem[k * 8 + 0];
+#pragma unroll
+          for (int w = 1; w < 8; ++w) a = ((MaxMask >> k) & 1u) ? maxd(a, smem[k * 8 + w]) : a + smem[k * 8 + w];
+          slot[(size_t)k * nblk + rank] = a;
+        }
+        s_ok = arrive_and_wait();
+      }
+      __syncthreads();
+      const int ok = s_ok;
+      if (warp < K) {
+        const bool isMax = ((MaxMask >> warp) & 1u) != 0;
+        const double* src = slot + (size_t)warp * nblk;
+        double acc = 0.0;
+        if (ok) {
+          constexpr int kB = 16;
+          for (unsigned b0 = lane; b0 < nblk; b0 += 32u * kB) {
+            double x[kB];
+#pragma unroll
+            for (int j = 0; j < kB; ++j) {
+              const unsigned b = b0 + 32u * j;
+              x[j] = b < nblk ? __ldcg(src + b) : 0.0;
+            }
+#pragma unroll
+            for (int j = 0; j < kB; ++j) {
+              if (b0 + 32u * j >= nblk) break;
+              acc = isMax ? maxd(acc, x[j]) : acc + x[j];
+            }
+          }
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) {
+            const double o = __shfl_xor_sync(0xffffffffu, acc, off);
+            acc = isMax ? maxd(acc, o) : acc + o;
+          }
+        }
+        if (lane == 0) s_res[warp] = acc;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < K; ++k) v[k] = s_res[k];
+      return ok != 0;
+    }
     if (warp == 0) {
       int ok = 1;
       if (lane == 0) {
