@@ -1073,7 +1073,7 @@ def main() -> None:
                     help="thermal CPU baseline: seconds after which the port's solve is extrapolated")
     ap.add_argument("--ref-threads", type=int, default=0,
                     help="reference arm: OpenMP threads of the reference (default: every host core)")
-    ap.add_argument("--ref-time-cap", type=float, default=480.0,
+    ap.add_argument("--ref-time-cap", type=float, default=180.0,
                     help="reference arm: seconds after which an unfinished solve is extrapolated")
     ap.add_argument("--ref-design-cap", type=float, default=45.0,
                     help="reference arm, mix: seconds per design after which its solve is extrapolated")
