@@ -1439,9 +1439,10 @@ __device__ int pcg_resident(const DesignView& d, Group& g, double* smem, double 
 //   P2 forms p_k = z + beta p_{k-1} at its own point with P1's expression,
 //   updates x, r, z and stores p_k and z to global memory for the other tiles.
 // FP64 forms the diagonal from the four conductances the way phase C did (the
-// stored conductances are phase C's summands, added in its order), and adds
-// alpha p to x in global memory with red.add (one rounding of x + (alpha p),
-// as P2's x + alpha p without a fused multiply-add).  The points, their order
+// stored conductances are phase C's summands, added in its order), and keeps x
+// at the thread's points in registers (x + alpha p, one rounding, as P2
+// forms it), storing it every iteration so that the last store precedes the
+// last grid barrier and phase D reads the final x.  The points, their order
 // and every sum are those of pcg_two_reductions, so the iterates are the same
 // bits.
 // ---------------------------------------------------------------------------
@@ -1515,6 +1516,9 @@ __device__ int pcg_smem(const DesignView& d, Group& g, double* smem, char* tbuf,
   cp_async_wait<0>();
   __syncthreads();
   double rz = rz0, beta = 0.0;
+  double xr[R];  // FP64: x at the thread's points (phase C's x0 = 0)
+#pragma unroll
+  for (int k = 0; k < R; ++k) xr[k] = 0.0;
   int it = 0;
   for (; it < d.maxPIter; ++it) {
     const double bt = beta;
@@ -1581,7 +1585,9 @@ __device__ int pcg_smem(const DesignView& d, Group& g, double* smem, char* tbuf,
     if (fabs(pAp) < 1e-20) break;
     const double alpha = rz / pAp;
     double s2[2] = {0.0, 0.0};  // |r|^2, r.z
-    for (int k = 0; k < nk; ++k) {
+#pragma unroll
+    for (int k = 0; k < R; ++k) {  // unrolled: xr[k] stays in a register
+      if (k >= nk) break;
       int i, j;
       if (!point(k, i, j)) continue;
       const size_t o = (size_t)i * P + j;
@@ -1593,7 +1599,8 @@ __device__ int pcg_smem(const DesignView& d, Group& g, double* smem, char* tbuf,
         S.x[k][th] = xn;
         w.px[o] = xn;
       } else {
-        atomicAdd(reinterpret_cast<double*>(w.px) + o, alpha * (double)pc);  // x += alpha p (red.add)
+        xr[k] = xr[k] + alpha * (double)pc;  // x += alpha p (pressure_solver.cpp:164)
+        w.px[o] = xr[k];
       }
       const T rt = (T)((double)S.r[k][th] - alpha * (double)S.ap[k][th]);
       S.r[k][th] = rt;
