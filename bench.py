@@ -1047,9 +1047,9 @@ def run_many(args) -> None:
 # workload (`bench.py --steps 2 --warmup 3 --no-cpu-baseline`, 14 launches,
 # FP64); profiles/cps_grid_kernel_network_500x250_fp64.txt has the command.
 # Density 1000 x 500: two launches of the full workload (the first, early launch
-# of a solve and the next, late one), 587.9 and 587.3 GB
+# of a solve and the next, late one), 596.4 and 595.9 GB
 # (profiles/cps_grid_kernel_density_1000x500_fp64.txt has the command).
-MEASURED_TRAFFIC = {("network", "fp64"): 1.249e9, ("density", "fp64"): 5.876e11}
+MEASURED_TRAFFIC = {("network", "fp64"): 1.249e9, ("density", "fp64"): 5.962e11}
 
 # Outer iterations of a converged FP64 solve of each workload (1e-6 outer
 # residual): straight and network by the bit-exact FP64 oracle (the

@@ -1435,9 +1435,10 @@ __device__ int pcg_resident(const DesignView& d, Group& g, double* smem, double 
 // iteration then reads global memory only for the neighbours that lie in
 // another tile (the ring around each tile: z and p_{k-1}, copied with
 // cp.async for all tiles at once, each thread into halo slots only it reads).
-//   P1 reads p_{k-1} and z and writes only Ap, so no thread waits for another;
-//   P2 forms p_k = z + beta p_{k-1} at its own point with P1's expression,
-//   updates x, r, z and stores p_k and z to global memory for the other tiles.
+//   P1 forms p_k = z + beta p_{k-1} once at each of the CTA's points, in
+//   place, then (after a CTA barrier) Ap from it, and from z and p_{k-1} at the
+//   halo with the same expression; P2 updates x, r, z and stores p_k and z to
+//   global memory for the other tiles.
 // FP64 forms the diagonal from the four conductances the way phase C did (the
 // stored conductances are phase C's summands, added in its order), and keeps x
 // at the thread's points in registers (x + alpha p, one rounding, as P2
@@ -1550,30 +1551,37 @@ __device__ int pcg_smem(const DesignView& d, Group& g, double* smem, char* tbuf,
         }
       }
       cp_async_commit();
-      cp_async_wait<0>();  // each thread reads only the halo slots it copied
+      // p_it at the CTA's own points, formed once in place (the stencil below
+      // and P2 read it; the value of forming it at every use)
       for (int k = 0; k < nk; ++k) {
         int i, j;
         if (!point(k, i, j)) continue;
-        const double pc0 = pk(S.z[k][th], S.p[k][th]);
+        S.p[k][th] = (T)pk(S.z[k][th], S.p[k][th]);
+      }
+      cp_async_wait<0>();  // each thread reads only the halo slots it copied
+      __syncthreads();     // and its tile's p_it after every thread has formed its own
+      for (int k = 0; k < nk; ++k) {
+        int i, j;
+        if (!point(k, i, j)) continue;
+        const double pc0 = (double)S.p[k][th];
         double Ap = 0.0;
         if (i > 1) {
-          if (ty > 0) Ap += -(double)S.cN[k][th - kTileJ] * pk(S.z[k][th - kTileJ], S.p[k][th - kTileJ]);
+          if (ty > 0) Ap += -(double)S.cN[k][th - kTileJ] * (double)S.p[k][th - kTileJ];
           else Ap += -(double)S.cSH[k][tx] * pk(S.zH[k][tx], S.pH[k][tx]);
         }
         if (j > 1) {
-          if (tx > 0) Ap += -(double)S.cE[k][th - 1] * pk(S.z[k][th - 1], S.p[k][th - 1]);
+          if (tx > 0) Ap += -(double)S.cE[k][th - 1] * (double)S.p[k][th - 1];
           else Ap += -(double)S.cWH[k][ty] * pk(S.zH[k][2 * kTileJ + ty], S.pH[k][2 * kTileJ + ty]);
         }
         Ap += diag(k, i, j) * pc0;
         if (j + 1 <= N - 2) {
           const int q = 2 * kTileJ + kTileI + ty;
-          Ap += -(double)S.cE[k][th] *
-                (tx < kTileJ - 1 ? pk(S.z[k][th + 1], S.p[k][th + 1]) : pk(S.zH[k][q], S.pH[k][q]));
+          Ap += -(double)S.cE[k][th] * (tx < kTileJ - 1 ? (double)S.p[k][th + 1] : pk(S.zH[k][q], S.pH[k][q]));
         }
         if (i < M - 1) {
           const int q = kTileJ + tx;
           Ap += -(double)S.cN[k][th] *
-                (ty < kTileI - 1 ? pk(S.z[k][th + kTileJ], S.p[k][th + kTileJ]) : pk(S.zH[k][q], S.pH[k][q]));
+                (ty < kTileI - 1 ? (double)S.p[k][th + kTileJ] : pk(S.zH[k][q], S.pH[k][q]));
         }
         const T apt = (T)Ap;
         S.ap[k][th] = apt;
@@ -1591,8 +1599,7 @@ __device__ int pcg_smem(const DesignView& d, Group& g, double* smem, char* tbuf,
       int i, j;
       if (!point(k, i, j)) continue;
       const size_t o = (size_t)i * P + j;
-      const T pc = it > 0 ? (T)pk(S.z[k][th], S.p[k][th]) : S.p[k][th];  // p_it, as P1 formed it
-      S.p[k][th] = pc;
+      const T pc = S.p[k][th];  // p_it (P1 formed it in place; iteration 0: p0 = z0)
       pg[o] = pc;
       if constexpr (kMixed) {
         const T xn = (T)((double)S.x[k][th] + alpha * (double)pc);
