@@ -157,7 +157,7 @@ def errors_vs_fixture(design, fields, dp: float, fx) -> dict:
     return out
 
 
-def oracle_error_block(solver, design, fx, fixture: str, eps_fixed: float = 1e-10, max_outer: int = 200000) -> dict:
+def oracle_error_block(solver, design, fx, fixture: str, eps_fixed: float = 1e-10, max_outer: int = 400000) -> dict:
     """error_vs_fp64_oracle of a solver left at its 1e-6 stop: its fields
     against the reference's FP64 fixed point; then the same state continued
     to the fixture's residual (1e-10; 1e-12 for the density-field designs)
