@@ -90,3 +90,28 @@ def test_design_loop_mode_equals_separate_runs():
         assert np.array_equal(loop[f"{k}2"], rb[k])
         assert np.array_equal(loop[f"{k}3"], ra[k])
     assert np.array_equal(loop["pIters1"], ra["pIters"]) and np.array_equal(loop["pIters2"], rb["pIters"])
+
+
+def test_bench_lines_have_their_fixtures():
+    """Every workload whose bench line states its error against the
+    reference's FP64 fixed point has that fixture committed, for the very
+    design the bench solves (the single designs by workload name, mix design
+    47 and served request 14 by index)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(os.path.dirname(HERE), "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    for workload, name in bench.ORACLE_FIXTURES.items():
+        z = np.load(os.path.join(CONVERGED, name + ".npz"))
+        d, _ = bench.workload(workload)
+        dz = design_of(z)
+        assert (d.M, d.N) == (dz.M, dz.N) == (int(z["M"]), int(z["N"])), workload
+        assert np.array_equal(d.alpha, dz.alpha) and np.array_equal(d.gamma, dz.gamma), workload
+    mix = geometry.batch_mix(64)
+    for k, name in bench.MIX_FIXTURES.items():
+        dz = design_of(np.load(os.path.join(CONVERGED, name + ".npz")))
+        assert np.array_equal(mix[k].alpha, dz.alpha), name
+    stream = geometry.served_stream(32)
+    for k, name in bench.SERVED_FIXTURES.items():
+        dz = design_of(np.load(os.path.join(CONVERGED, name + ".npz")))
+        assert np.array_equal(stream[k][1].alpha, dz.alpha), name
