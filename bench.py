@@ -1054,8 +1054,9 @@ MEASURED_TRAFFIC = {("network", "fp64"): 1.249e9, ("density", "fp64"): 5.962e11}
 # Outer iterations of a converged FP64 solve of each workload (1e-6 outer
 # residual): straight and network by the bit-exact FP64 oracle (the
 # reference's own arithmetic, one thread), density by the reference's own
-# FP64 build on 7 OpenMP threads (940 s).
-REFERENCE_ITERS = {"straight": 5564, "network": 9814, "density": 18176}
+# FP64 build on 7 OpenMP threads: the first stage of its converged fixture
+# (tests/golden/converged/density_1000x500.npz, n_stop; 435 s).
+REFERENCE_ITERS = {"straight": 5564, "network": 9814, "density": 15420}
 
 
 def main() -> None:

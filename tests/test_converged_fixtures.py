@@ -107,6 +107,9 @@ def test_bench_lines_have_their_fixtures():
         dz = design_of(z)
         assert (d.M, d.N) == (dz.M, dz.N) == (int(z["M"]), int(z["N"])), workload
         assert np.array_equal(d.alpha, dz.alpha) and np.array_equal(d.gamma, dz.gamma), workload
+    # the reference arm extrapolates the 1000 x 500 solve to the reference's own stop count
+    z = np.load(os.path.join(CONVERGED, bench.ORACLE_FIXTURES["density"] + ".npz"))
+    assert bench.REFERENCE_ITERS["density"] == int(z["n_stop"])
     mix = geometry.batch_mix(64)
     for k, name in bench.MIX_FIXTURES.items():
         dz = design_of(np.load(os.path.join(CONVERGED, name + ".npz")))
